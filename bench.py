@@ -1,0 +1,327 @@
+"""Benchmark: Mcell-steps/s of the FP64 per-stage RHS + LDDRK4 path.
+
+Workload: 384^3 octant blast wave in isotropic turbulence (symmetry planes at
+x=y=z=0, non-reflecting outflow + sponge at the far faces), two-species
+"_mf" physics with Y = 1, FP64.  One step = Compute_CFL + Compute_Tstep +
+LDDRK4 (10 RHS stages, src/main_mf.f:137-143).  Inputs are seeded synthetic
+fields (see shock_turbulence_b200/initial.py); there is no public dataset.
+
+Multi-GPU: replicas only (one independent case per rank, no collective in
+the data path); value = cells * steps of all ranks / max rank time.
+
+--impl reference times the CPU oracle (plain-C restatement of the reference
+path; the Fortran reference cannot be compiled in this image) on the host
+cores, on a bounded sample grid of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s (FP64 RHS+LDDRK4 step, 10 RK stages/step)"
+UNIT = "Mcell-steps/s"
+
+
+def make_params(n, device=0):
+    from shock_turbulence_b200 import default_params
+    # config: Re = 100 with the molecular viscous term added (re > 0),
+    # Pr = 0.7, artificial viscosity on, CFL 0.5, bulk coefficient scale 1.75
+    return default_params(n, re=100.0, re1=100.0, re2=100.0, pr=0.7, hyper_param=1, cfl_cal=0.5,
+                          c_beta_scale=1.75, device=device)
+
+
+def make_state(p, seed):
+    from shock_turbulence_b200.initial import blast_in_turbulence
+    return blast_in_turbulence(p, k0=8.0, mach_t=0.1, p_ratio=100.0, radius_cells=4.0, seed=seed)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu_id)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_smi_id(dev):
+    import torch
+    props = torch.cuda.get_device_properties(dev)
+    uid = getattr(props, "uuid", None)
+    if uid is not None:
+        s = str(uid)
+        return s if s.startswith("GPU-") else "GPU-" + s
+    return dev
+
+
+# ---------------------------------------------------------------- CPU oracle
+def oracle_rate(n, steps, warm, threads):
+    """Mcell-steps/s of the CPU oracle on an n^3 sample (host cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    oracle_py.build()
+    oracle_py.set_threads(threads)
+    p = make_params(n)
+    Q, Y = make_state(p, seed=1)
+    o = oracle_py.Oracle(p)
+    o.set_state(Q, Y)
+    o.compute_gamma(Y)
+    o.compute_hyper(Q, Y)
+    t, s = 0.0, 0
+    for _ in range(warm):
+        t, s = o.step(t, s)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t, s = o.step(t, s)
+    el = time.perf_counter() - t0
+    return n ** 3 * steps / el / 1e6, el
+
+
+def traffic_per_launch(kernel, n):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
+    to an n^3 grid (traffic grows with the cells a launch processes)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and not line.startswith("#"):
+            ncap, b = int(parts[1]), float(parts[2])
+            return b * (n ** 3) / (ncap ** 3)
+    return None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n = args.cpu_n
+    rate, el = oracle_rate(n, args.steps, args.warmup, threads)
+    sample = (f"CPU oracle (C restatement of the reference path), {n}^3 sample of the same workload, "
+              f"{args.warmup} warm-up + {args.steps} timed steps, {threads} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded blast-in-turbulence)",
+        "config": {"workload": f"blast wave in isotropic turbulence, octant, sample {n}^3 of 384^3",
+                   "grid": n, "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=384, help="grid points per direction")
+    ap.add_argument("--cpu-n", type=int, default=64, help="grid of the CPU-oracle sample")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if (args.impl == "b200" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    from shock_turbulence_b200 import Solver
+    torch.cuda.set_device(local)
+    p = make_params(args.n, device=local)
+    Q, Y = make_state(p, seed=1 + rank)
+    s = Solver(p)
+    stream = torch.cuda.current_stream()
+    s._check(s.lib.st_set_stream(s._h, stream.cuda_stream), "st_set_stream")
+    s.set_state(Q, Y)
+    s.Compute_gamma(Y)
+    s.Compute_hyper(Q, Y)
+    t, st = 0.0, 0
+    for _ in range(args.warmup):
+        t, st = s.step(t, st)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-timed region (inputs resident in HBM) ----
+    clocks = ClockSampler(gpu_smi_id(local))
+    import ctypes
+    c0 = ctypes.c_longlong()
+    s.lib.st_launch_count(s._h, ctypes.byref(c0))
+    s.lib.st_profile(s._h, 1)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        t, st = s.step(t, st)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    s.lib.st_profile(s._h, 0)
+    c1 = ctypes.c_longlong()
+    s.lib.st_launch_count(s._h, ctypes.byref(c1))
+    buf = ctypes.create_string_buffer(1 << 16)
+    s._check(s.lib.st_profile_report(s._h, buf, len(buf)), "st_profile_report")
+    prof = json.loads(buf.value.decode())
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    cells = args.n ** 3
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    mon = s.monitors()
+    finite = bool(math.isfinite(mon[0]) and math.isfinite(mon[5]))
+
+    # ---- end-to-end through the public API with host buffers ----
+    import numpy as np
+    Qh = torch.from_numpy(np.ascontiguousarray(s.get_state()[0])).pin_memory()
+    Yh = torch.from_numpy(np.ascontiguousarray(s.get_state()[1])).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_steps):
+        s.set_state(Qh, Yh)          # H2D of the step's inputs (pinned host)
+        t, st = s.step(t, st)
+        s.get_state(Qh, Yh)          # D2H of the step's result
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = f0.elapsed_time(f1)
+    if dist is not None:
+        tt = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
+    e2e = world * cells * args.e2e_steps / (ms_e2e / 1e3) / 1e6
+    io_bytes = 6 * cells * 8
+
+    # ---- roofline of the dominant kernel ----
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    dom = max((k for k in prof if prof[k]["bytes"] > 0), key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
+    step_ms_all = sum(v["ms"] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": traffic_per_launch(dom, args.n),
+                "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
+                "avg_launch_ms": d["ms"] / d["launches"],
+                "share_of_kernel_time": d["ms"] / step_ms_all if step_ms_all else None,
+                "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                                "GB/s": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["bytes"] and v["ms"] else None}
+                            for k, v in prof.items()}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, el = oracle_rate(args.cpu_n, 2, 1, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 2 timed steps "
+                         f"({el:.1f} s), {threads} OpenMP threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded solenoidal turbulence + Gaussian blast)",
+            "config": {"workload": f"blast wave in isotropic turbulence, {args.n}^3 octant, FP64, two-species _mf "
+                                   "physics (Y=1), Re=100 viscous term on, artificial viscosity on, CFL 0.5",
+                       "grid": args.n, "cells": cells, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (one field is %.0f MB)" % (cells * 8 / 1e6),
+                       "finite": finite},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
+                    "steps": args.e2e_steps},
+            "gpu_launches": int(c1.value - c0.value),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * st_b200.h - C ABI of the B200 (sm_100a) implementation of the per-stage
+ * right-hand side and LDDRK4 stage update of the compact-difference
+ * compressible Navier-Stokes shock-turbulence solver (two-species "_mf"
+ * family: symmetry planes at x=y=z=0, one-sided closures, non-reflecting
+ * outflow and sponge at the far faces).
+ *
+ * Conventions shared by every entry point
+ *  - Arrays use the reference layout: Fortran F(My,Mz,Mx[,nvar]), i.e. y is
+ *    the unit-stride index, then z, then x, then the variable index.  The
+ *    conserved variables are ordered [rho*u, rho*v, rho*w, rho, rho*E].
+ *  - Every array argument may be a host pointer or a device pointer; the
+ *    library inspects each pointer (cudaPointerGetAttributes) and copies
+ *    host data through device staging buffers.  Device pointers must belong
+ *    to the context's device.
+ *  - Every function returns 0 on success or a negative ST_E* code; nothing
+ *    aborts the process.  st_last_error() gives a message for the last
+ *    failure on a context.
+ *  - The hidden state that the reference keeps in COMMON blocks
+ *    (/RKWORK/ Q,dQ,QW; /SPECIES/ Y,drYi,rYW; /THERMO/ gamma_eff; /GRAD/;
+ *    /HYPER/; /TIME_RK/ Tstep) lives on the device inside the context.
+ *  - A context is not thread-safe; it owns one CUDA stream.
+ *
+ * Reference citations are path:line within the reference project.
+ */
+#ifndef ST_B200_H
+#define ST_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define ST_OK            0
+#define ST_E_ARG        -1  /* bad argument (null pointer, bad size, ...)  */
+#define ST_E_NOMEM      -2  /* device or host allocation failed            */
+#define ST_E_CUDA       -3  /* a CUDA runtime call failed                  */
+#define ST_E_UNSUPPORTED -4 /* grid size or mode not supported             */
+#define ST_E_NONFINITE  -5  /* non-finite value detected in the state      */
+#define ST_E_NODEVICE   -6  /* no CUDA device / extension not usable       */
+
+/* ---- run-time parameters --------------------------------------------- */
+/* Carries what the reference fixes at compile time in src/header:5-10
+ * (grid) and reads from srm.input.1 in src/define_nonperiodic_mf.f:17-84. */
+typedef struct st_params {
+    int    nx, ny, nz;          /* grid points (Mx=Nx, My=Ny, Mz=Nz: one GPU) */
+    double x_leng, y_leng, z_leng;   /* domain lengths (period_x, ...)       */
+    double x_start, y_start, z_start;
+    double re;                  /* COMMON Re.  The _mf build never assigns it,
+                                   so the molecular viscous/conductive term is
+                                   computed but not added (src/rhsv_sym_mf.f:
+                                   1420-1424).  re > 0 adds it.               */
+    double re1, re2, pr, sc;
+    double gamma1, gamma2, epsilon, vis_exp, bulk_ratio, t_ratio;
+    int    hyper_param;         /* 1: artificial viscosity/diffusivity on     */
+    int    rk_mode;             /* 0: second LDDRK4 loop with the unassigned
+                                      (zero) alpha2/beta2 of the reference build
+                                      (src/header:247-296);
+                                   1: second loop reuses alpha1/beta1          */
+    double cfl_cal;             /* target CFL (Compute_Tstep)                 */
+    double c_beta_scale;        /* multiplies the dynamic bulk-viscosity
+                                   coefficient; 1 reproduces the reference
+                                   (src/hyper_dynamic_sym_mf.f:145-147)       */
+    int    device;              /* CUDA device ordinal                        */
+} st_params;
+
+typedef struct st_ctx st_ctx;
+
+/* ---- context --------------------------------------------------------- */
+/* Replaces Setup_Grid (src/grid.f:15-112), Setup_Derivatives_Sym/_Asym
+ * (src/derivCDopt6_sym_tri.f:9-373, src/derivCDopt6_asym_tri.f:9-375) and
+ * Init_Filters_sym/_asym (src/filters_sym.f:9-383, src/filters_asym.f:9-385):
+ * builds the constant LU factors once per direction and allocates the
+ * device mirrors of the COMMON blocks. */
+int  st_create(const st_params *p, st_ctx **out);
+int  st_destroy(st_ctx *c);
+const char *st_last_error(const st_ctx *c);
+const char *st_status_string(int status);
+/* Fills p with the reference input values (init/srm.input.1:19-34) on an
+ * n^3 unit-spacing grid. */
+void st_default_params(st_params *p, int nx, int ny, int nz);
+
+/* Resident state: /RKWORK/ Q(My,Mz,Mx,5) and /SPECIES/ Y(My,Mz,Mx).
+ * st_set_state also clears QW, rYW, dQ, drYi (the reference zeroes QW and
+ * rYW at the start of each LDDRK4 loop; dQ/drYi start as zero COMMON). */
+int  st_set_state(st_ctx *c, const double *Q, const double *Y);
+int  st_get_state(st_ctx *c, double *Q, double *Y);
+int  st_set_tstep(st_ctx *c, double tstep);
+int  st_get_tstep(st_ctx *c, double *tstep);
+/* Copies a named COMMON array out of the context: "gamma_eff", "dux_dx",
+ * "duy_dx", "duz_dx", "dux_dy", "duy_dy", "duz_dy", "dux_dz", "duy_dz",
+ * "duz_dz", "dTdx", "dTdy", "dTdz", "beta_hyper", "visc_hyper", "k_hyper",
+ * "D_hyper", "dQ" (5 fields), "QW" (5), "drYi", "rYW". */
+int  st_get_common(st_ctx *c, const char *name, double *out);
+int  st_set_common(st_ctx *c, const char *name, const double *in);
+
+/* ---- line solvers ------------------------------------------------------ */
+/* tridiagonal(A1,B1,C1,R,n,lot,nper,ncom), src/tridiagonal.f90:1-49; serial
+ * paths :197-287.  Arrays (lot,n), lot fastest; R is overwritten.  nper=1
+ * selects the periodic (bordered) solve.  General (per-line) coefficients. */
+int  st_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C,
+                    double *R, int n, int lot, int nper);
+/* pentadiagonal(A1..E1,R,n,lot,nper,ncom), src/pentadiagonal.f90:1-52;
+ * serial paths :319-504. */
+int  st_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C,
+                      const double *D, const double *E, double *R,
+                      int n, int lot, int nper);
+
+/* ---- compact derivatives ------------------------------------------------ */
+/* DFDX_sym(F,dF,iadd,cadd) src/derivCDopt6_sym_tri.f:409-535, DFDY_sym :672,
+ * DFDZ_sym :932; _asym variants src/derivCDopt6_asym_tri.f:412,670,930.
+ * iadd=0: dF = cadd*dF/dx ; iadd=1: dF += cadd*dF/dx. */
+int  st_dfdx_sym (st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdy_sym (st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdz_sym (st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdx_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdy_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdz_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+/* D2FDX2_sym(F,dF,d2F,iadd) src/derivCDopt6_sym_tri.f:538-669, D2FDY2_sym
+ * :801, D2FDZ2_sym :1062; _asym src/derivCDopt6_asym_tri.f:540,798,1061.
+ * d2F = d2F/dx2; if iadd=1 also dF = dF/dx (overwritten). */
+int  st_d2fdx2_sym (st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdy2_sym (st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdz2_sym (st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdx2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdy2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdz2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+
+/* ---- filters -------------------------------------------------------------- */
+/* Compact_Filter(F,F0,N) src/filters_sym.f:398-432 (variable 1 filtered with
+ * the x asym filter, 2 with y asym, 3 with z asym, all others sym; X then Y
+ * then Z).  F0 may alias F. */
+int  st_compact_filter(st_ctx *c, const double *F, double *F0, int nvar);
+/* Compact_Filter_{X,Y,Z}_sym src/filters_sym.f:436-634,637-835,838-1034 and
+ * _asym src/filters_asym.f:388-583,586-782,783-975.  F0 may alias F. */
+int  st_compact_filter_x_sym (st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_y_sym (st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_z_sym (st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_x_asym(st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_y_asym(st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_z_asym(st_ctx *c, const double *F, double *F0);
+/* Gaussian_Filter(F,Fg,N) src/filters_sym.f:1046-1071 and its X/Y/Z passes
+ * :1076-1554 (coefficients rounded to float32, src/LES_header:153-157). */
+int  st_gaussian_filter  (st_ctx *c, const double *F, double *Fg, int nvar);
+int  st_gaussian_filter_x(st_ctx *c, const double *F, double *Fg);
+int  st_gaussian_filter_y(st_ctx *c, const double *F, double *Fg);
+int  st_gaussian_filter_z(st_ctx *c, const double *F, double *Fg);
+
+/* ---- physics operators ------------------------------------------------------ */
+/* Compute_gamma(Y) src/lddrk4_nonperiodic_mf.f:342-372 -> /THERMO/. */
+int  st_compute_gamma(st_ctx *c, const double *Y);
+/* RHS(Q,Qrhs,Y) src/rhsv_sym_mf.f:9-26 (RHS_x :37-481, RHS_yz :492-1428).
+ * Overwrites Qrhs, writes /GRAD/, and (like the reference) rewrites the
+ * momenta of Q as (m/rho)*rho. */
+int  st_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y);
+/* Compute_hyper(Q,Y) src/hyper_dynamic_sym_mf.f:166-334 -> /HYPER/. */
+int  st_compute_hyper(st_ctx *c, const double *Q, const double *Y);
+/* Hyper_RHS(Q,Qrhs,Y) src/hyper_rhs_sym_mf.f:12-500: Qrhs += artificial
+ * stress/heat-flux divergence (calls Compute_hyper). */
+int  st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y);
+/* Species_RHS(Q,Qrhs,Y,Yrhs) src/species_rhs_sym.f:9-207. */
+int  st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y,
+                    double *Yrhs);
+/* bc_RHS(Q,Qrhs,Y,Yrhs,time) src/bc_mf.f:11-463 (zeroes the normal momentum
+ * of Q on the symmetry planes, overwrites the far-face rows). */
+int  st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs,
+               double time);
+/* Sponge_Forcing(Q,Qrhs,Y,Yrhs) src/sponge_mf.f:7-127. */
+int  st_sponge_forcing(st_ctx *c, const double *Q, double *Qrhs, const double *Y,
+                       double *Yrhs);
+/* Fix_Pressure(Q,Y) pproc/pproc_mf.f:190-233 (uses /THERMO/). */
+int  st_fix_pressure(st_ctx *c, double *Q, const double *Y);
+/* Compute_CFL(Q,cfl_stab,cfl_resv,step) src/lddrk4_nonperiodic_mf.f:7-66. */
+int  st_compute_cfl(st_ctx *c, const double *Q, double *cfl_stab, double *cfl_resv);
+/* Compute_Tstep(Q,Y,cfl_resv,step) src/lddrk4_nonperiodic_mf.f:75-160:
+ * sets the context's Tstep and returns it in *tstep (may be NULL). */
+int  st_compute_tstep(st_ctx *c, const double *Q, const double *Y, double cfl_resv,
+                      int step, double *tstep);
+
+/* ---- time integration on the resident state ------------------------------ */
+/* LDDRK4(time,step) src/lddrk4_nonperiodic_mf.f:428-541 on /RKWORK/ and
+ * /SPECIES/ held by the context (st_set_state), using the context Tstep.
+ * Advances *time by 2*Tstep and *step by 1; the monitoring scalars
+ * (KE, Mom, Mass, Energy, Entropy) are recomputed and can be read with
+ * st_get_monitors. */
+int  st_lddrk4(st_ctx *c, double *time, int *step);
+/* One iteration of the main loop body of src/main_mf.f:137-145 (march_mode
+ * 1): Compute_CFL, Compute_Tstep, LDDRK4.  dt stays on the device. */
+int  st_step(st_ctx *c, double *time, int *step);
+/* Compute_Mom/KE/Mass/Energy/Entropy src/lddrk4_nonperiodic_mf.f:168-327 on
+ * the resident state: out[0..9] = KE, MomX, MomY, MomZ, Mass, Energy,
+ * Entropy, Entropy2, cfl_resv of the last st_step, Tstep. */
+int  st_get_monitors(st_ctx *c, double out[10]);
+/* Synchronises the context stream. */
+int  st_sync(st_ctx *c);
+
+/* ---- streams, instrumentation (no reference counterpart) ------------------ */
+/* Runs the context's work on a caller-owned cudaStream_t (NULL restores the
+ * context's own stream), so callers can order and time it with their own
+ * events; st_get_stream returns the stream in use. */
+int  st_set_stream(st_ctx *c, void *stream);
+int  st_get_stream(st_ctx *c, void **stream);
+/* Per-kernel CUDA-event timing of every launch on the context stream while
+ * enabled; st_profile_report writes a JSON object
+ * {"kernel": {"launches": n, "ms": total, "bytes": algorithmic bytes}} and
+ * clears the records.  st_launch_count returns the number of kernels the
+ * context has launched since creation. */
+int  st_profile(st_ctx *c, int enable);
+int  st_profile_report(st_ctx *c, char *buf, int buflen);
+int  st_launch_count(st_ctx *c, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ST_B200_H */

@@ -1,0 +1,200 @@
+"""ctypes loader for the CPU oracle (TEST INFRASTRUCTURE: the checker).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module.  It mirrors the reference routine names (``DFDX_sym`` ...) on
+numpy arrays in the reference layout F(My,Mz,Mx[,n]); a numpy array of shape
+(Mx, Mz, My) in C order has exactly that memory layout.
+
+Parity status: unpinned by the reference's own tests (none exist, and the
+Fortran reference cannot be built here); see st_oracle.h.
+"""
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liborc_st.so")
+
+sys.path.insert(0, os.path.dirname(_HERE))
+from shock_turbulence_b200.params import StParams, default_params  # noqa: E402
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build(force=False):
+    """Compile the oracle with its Makefile if the library is missing."""
+    if force or not os.path.exists(_LIB):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liborc_st.so"])
+    return _LIB
+
+
+def _load():
+    build()
+    lib = ctypes.CDLL(_LIB)
+    lib.orc_create.restype = ctypes.c_void_p
+    lib.orc_create.argtypes = [ctypes.POINTER(StParams)]
+    lib.orc_destroy.argtypes = [ctypes.c_void_p]
+    lib.orc_compute_tstep.restype = ctypes.c_double
+    lib.orc_get_tstep.restype = ctypes.c_double
+    lib.orc_set_tstep.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.orc_dfd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                            ctypes.c_double]
+    lib.orc_d2fd2.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
+    lib.orc_filter.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]
+    lib.orc_gauss.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+    lib.orc_compact_filter.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+    lib.orc_gaussian_filter.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+    lib.orc_bc_rhs.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double]
+    lib.orc_compute_tstep.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, ctypes.c_int]
+    lib.orc_get_common.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
+    lib.orc_set_common.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
+    lib.orc_tridiagonal.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.orc_pentadiagonal.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int]
+    lib.orc_set_threads.argtypes = [ctypes.c_int]
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous, "oracle needs C-contiguous float64"
+    return a.ctypes.data_as(_dp)
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def tridiagonal(A, B, C, R, nper=0):
+    """tridiagonal(A1,B1,C1,R,n,lot,nper) on arrays of shape (n, lot); R overwritten."""
+    n, lot = R.shape
+    lib().orc_tridiagonal(_p(A), _p(B), _p(C), _p(R), n, lot, nper)
+
+
+def pentadiagonal(A, B, C, D, E, R, nper=0):
+    n, lot = R.shape
+    lib().orc_pentadiagonal(_p(A), _p(B), _p(C), _p(D), _p(E), _p(R), n, lot, nper)
+
+
+class Oracle:
+    """One oracle context: the COMMON blocks of the reference plus its LHS."""
+
+    def __init__(self, params=None, **kw):
+        if params is None:
+            params = default_params(**kw)
+        self.params = params
+        self.shape = (params.nx, params.nz, params.ny)   # (Mx, Mz, My) C order = F(My,Mz,Mx)
+        self._c = lib().orc_create(ctypes.byref(params))
+
+    def __del__(self):
+        if getattr(self, "_c", None):
+            lib().orc_destroy(self._c)
+            self._c = None
+
+    def field(self, n=None):
+        return np.zeros(self.shape if n is None else (n,) + self.shape)
+
+    # --- state ---------------------------------------------------------
+    def set_state(self, Q, Y):
+        lib().orc_set_state(ctypes.c_void_p(self._c), _p(np.ascontiguousarray(Q)),
+                            _p(np.ascontiguousarray(Y)))
+
+    def get_state(self):
+        Q, Y = self.field(5), self.field()
+        lib().orc_get_state(ctypes.c_void_p(self._c), _p(Q), _p(Y))
+        return Q, Y
+
+    def set_tstep(self, t):
+        lib().orc_set_tstep(self._c, float(t))
+
+    def get_tstep(self):
+        return lib().orc_get_tstep(ctypes.c_void_p(self._c))
+
+    def get_common(self, name):
+        n = 5 if name in ("dQ", "QW") else None
+        out = self.field(n)
+        if lib().orc_get_common(self._c, name.encode(), _p(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def set_common(self, name, arr):
+        if lib().orc_set_common(self._c, name.encode(), _p(np.ascontiguousarray(arr))) != 0:
+            raise KeyError(name)
+
+    # --- operators (reference names) -----------------------------------
+    def dfd(self, d, asym, F, dF, iadd, cadd):
+        lib().orc_dfd(self._c, d, asym, _p(F), _p(dF), iadd, float(cadd))
+
+    def d2fd2(self, d, asym, F, dF, d2F, iadd):
+        lib().orc_d2fd2(self._c, d, asym, _p(F), _p(dF), _p(d2F), iadd)
+
+    def filter(self, d, asym, F, F0):
+        lib().orc_filter(self._c, d, asym, _p(F), _p(F0))
+
+    def gauss(self, d, F, Fg):
+        lib().orc_gauss(self._c, d, _p(F), _p(Fg))
+
+    def compact_filter(self, F, F0, nvar):
+        lib().orc_compact_filter(self._c, _p(F), _p(F0), nvar)
+
+    def gaussian_filter(self, F, Fg, nvar):
+        lib().orc_gaussian_filter(self._c, _p(F), _p(Fg), nvar)
+
+    def compute_gamma(self, Y):
+        lib().orc_compute_gamma(ctypes.c_void_p(self._c), _p(Y))
+
+    def rhs(self, Q, Qrhs, Y):
+        lib().orc_rhs(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y))
+
+    def compute_hyper(self, Q, Y):
+        lib().orc_compute_hyper(ctypes.c_void_p(self._c), _p(Q), _p(Y))
+
+    def hyper_rhs(self, Q, Qrhs, Y):
+        lib().orc_hyper_rhs(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y))
+
+    def species_rhs(self, Q, Qrhs, Y, Yrhs):
+        lib().orc_species_rhs(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y), _p(Yrhs))
+
+    def bc_rhs(self, Q, Qrhs, Y, Yrhs, time=0.0):
+        lib().orc_bc_rhs(self._c, _p(Q), _p(Qrhs), _p(Y), _p(Yrhs), float(time))
+
+    def sponge_forcing(self, Q, Qrhs, Y, Yrhs):
+        lib().orc_sponge_forcing(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y), _p(Yrhs))
+
+    def fix_pressure(self, Q, Y):
+        lib().orc_fix_pressure(ctypes.c_void_p(self._c), _p(Q), _p(Y))
+
+    def compute_cfl(self, Q):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        lib().orc_compute_cfl(ctypes.c_void_p(self._c), _p(Q), ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def compute_tstep(self, Q, Y, cfl_resv, step):
+        return lib().orc_compute_tstep(self._c, _p(Q), _p(Y), float(cfl_resv), int(step))
+
+    def lddrk4(self, time=0.0, step=0):
+        t, s = ctypes.c_double(time), ctypes.c_int(step)
+        lib().orc_lddrk4(ctypes.c_void_p(self._c), ctypes.byref(t), ctypes.byref(s))
+        return t.value, s.value
+
+    def step(self, time=0.0, step=0):
+        t, s = ctypes.c_double(time), ctypes.c_int(step)
+        lib().orc_step(ctypes.c_void_p(self._c), ctypes.byref(t), ctypes.byref(s))
+        return t.value, s.value
+
+    def monitors(self):
+        out = np.zeros(10)
+        lib().orc_get_monitors(ctypes.c_void_p(self._c), _p(out))
+        return out

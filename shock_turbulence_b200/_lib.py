@@ -1,0 +1,81 @@
+"""ctypes binding of ``libst_b200.so`` (declarations in include/st_b200.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+from .params import StParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libst_b200.so")
+
+_dp = ctypes.c_void_p          # array arguments are raw addresses (host or device)
+_ctx = ctypes.c_void_p
+
+# name -> argument types (all return int status unless listed in _RESTYPES)
+SIGNATURES = {
+    "st_create": [ctypes.POINTER(StParams), ctypes.POINTER(ctypes.c_void_p)],
+    "st_destroy": [_ctx],
+    "st_last_error": [_ctx],
+    "st_status_string": [ctypes.c_int],
+    "st_default_params": [ctypes.POINTER(StParams), ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "st_set_state": [_ctx, _dp, _dp],
+    "st_get_state": [_ctx, _dp, _dp],
+    "st_set_tstep": [_ctx, ctypes.c_double],
+    "st_get_tstep": [_ctx, ctypes.POINTER(ctypes.c_double)],
+    "st_get_common": [_ctx, ctypes.c_char_p, _dp],
+    "st_set_common": [_ctx, ctypes.c_char_p, _dp],
+    "st_tridiagonal": [_ctx, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "st_pentadiagonal": [_ctx, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "st_compact_filter": [_ctx, _dp, _dp, ctypes.c_int],
+    "st_gaussian_filter": [_ctx, _dp, _dp, ctypes.c_int],
+    "st_compute_gamma": [_ctx, _dp],
+    "st_rhs": [_ctx, _dp, _dp, _dp],
+    "st_compute_hyper": [_ctx, _dp, _dp],
+    "st_hyper_rhs": [_ctx, _dp, _dp, _dp],
+    "st_species_rhs": [_ctx, _dp, _dp, _dp, _dp],
+    "st_bc_rhs": [_ctx, _dp, _dp, _dp, _dp, ctypes.c_double],
+    "st_sponge_forcing": [_ctx, _dp, _dp, _dp, _dp],
+    "st_fix_pressure": [_ctx, _dp, _dp],
+    "st_compute_cfl": [_ctx, _dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+    "st_compute_tstep": [_ctx, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
+    "st_lddrk4": [_ctx, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
+    "st_step": [_ctx, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
+    "st_get_monitors": [_ctx, _dp],
+    "st_sync": [_ctx],
+    "st_set_stream": [_ctx, ctypes.c_void_p],
+    "st_get_stream": [_ctx, ctypes.POINTER(ctypes.c_void_p)],
+    "st_profile": [_ctx, ctypes.c_int],
+    "st_profile_report": [_ctx, ctypes.c_char_p, ctypes.c_int],
+    "st_launch_count": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
+}
+for _d in ("x", "y", "z"):
+    for _s in ("sym", "asym"):
+        SIGNATURES[f"st_df{_d.join(['d', ''])}_{_s}"] = [_ctx, _dp, _dp, ctypes.c_int, ctypes.c_double]
+        SIGNATURES[f"st_d2fd{_d}2_{_s}"] = [_ctx, _dp, _dp, _dp, ctypes.c_int]
+        SIGNATURES[f"st_compact_filter_{_d}_{_s}"] = [_ctx, _dp, _dp]
+    SIGNATURES[f"st_gaussian_filter_{_d}"] = [_ctx, _dp, _dp]
+
+_RESTYPES = {"st_last_error": ctypes.c_char_p, "st_status_string": ctypes.c_char_p,
+             "st_default_params": None}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with shock_turbulence_b200.build.build() "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    _lib = lib
+    return lib

@@ -1,0 +1,208 @@
+"""Host-side mirror of the reference's subroutine interface over the C ABI.
+
+Method names and argument meanings follow the Fortran routines
+(``DFDX_sym(F, dF, iadd, cadd)``, ``RHS(Q, Qrhs, Y)``, ``LDDRK4(time, step)``
+...).  Arrays are numpy float64 arrays or torch float64 tensors (host or
+CUDA) in the reference layout F(My,Mz,Mx[,n]), i.e. C-order shape
+([n,] Mx, Mz, My).  Outputs are written in place, as in the reference.
+Every failure raises :class:`StError`; nothing falls back to the CPU.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import StParams, default_params
+
+
+class StError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+def _addr(a, nelem):
+    """Raw address of a contiguous float64 array with nelem elements."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("arrays must be C-contiguous float64")
+        if a.size != nelem:
+            raise ValueError(f"array has {a.size} elements, expected {nelem}")
+        return a.ctypes.data
+    # torch tensor
+    if getattr(a, "dtype", None) is None or str(a.dtype) != "torch.float64":
+        raise TypeError("tensors must be float64")
+    if not a.is_contiguous():
+        raise TypeError("tensors must be contiguous")
+    if a.numel() != nelem:
+        raise ValueError(f"tensor has {a.numel()} elements, expected {nelem}")
+    return a.data_ptr()
+
+
+class Solver:
+    """One solver context: device mirrors of the reference COMMON blocks."""
+
+    def __init__(self, params=None, **kw):
+        self.lib = _lib.load()
+        self.params = params if params is not None else default_params(**kw)
+        p = self.params
+        self.shape = (p.nx, p.nz, p.ny)
+        self.n3 = p.nx * p.ny * p.nz
+        h = ctypes.c_void_p()
+        st = self.lib.st_create(ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise StError(st, "st_create failed: " + self.lib.st_status_string(st).decode())
+        self._h = h
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, st, what):
+        if st != 0:
+            msg = self.lib.st_last_error(self._h).decode(errors="replace")
+            raise StError(st, f"{what}: {msg}")
+
+    def _a(self, a, nf=1):
+        return _addr(a, nf * self.n3)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.st_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field(self, n=None):
+        return np.zeros(self.shape if n is None else (n,) + self.shape)
+
+    # -- state and COMMON blocks -----------------------------------------
+    def set_state(self, Q, Y):
+        self._check(self.lib.st_set_state(self._h, self._a(Q, 5), self._a(Y)), "st_set_state")
+
+    def get_state(self, Q=None, Y=None):
+        Q = self.field(5) if Q is None else Q
+        Y = self.field() if Y is None else Y
+        self._check(self.lib.st_get_state(self._h, self._a(Q, 5), self._a(Y)), "st_get_state")
+        return Q, Y
+
+    def set_tstep(self, t):
+        self._check(self.lib.st_set_tstep(self._h, float(t)), "st_set_tstep")
+
+    def get_tstep(self):
+        t = ctypes.c_double()
+        self._check(self.lib.st_get_tstep(self._h, ctypes.byref(t)), "st_get_tstep")
+        return t.value
+
+    def get_common(self, name, out=None):
+        nf = 5 if name in ("dQ", "QW") else 1
+        out = self.field(nf if nf > 1 else None) if out is None else out
+        self._check(self.lib.st_get_common(self._h, name.encode(), self._a(out, nf)), "st_get_common")
+        return out
+
+    def set_common(self, name, arr):
+        nf = 5 if name in ("dQ", "QW") else 1
+        self._check(self.lib.st_set_common(self._h, name.encode(), self._a(arr, nf)), "st_set_common")
+
+    # -- line solvers (src/tridiagonal.f90, src/pentadiagonal.f90) ----------
+    def tridiagonal(self, A, B, C, R, n, lot, nper=0):
+        N = n * lot
+        self._check(self.lib.st_tridiagonal(self._h, _addr(A, N), _addr(B, N), _addr(C, N), _addr(R, N),
+                                            n, lot, nper), "tridiagonal")
+
+    def pentadiagonal(self, A, B, C, D, E, R, n, lot, nper=0):
+        N = n * lot
+        self._check(self.lib.st_pentadiagonal(self._h, _addr(A, N), _addr(B, N), _addr(C, N), _addr(D, N),
+                                              _addr(E, N), _addr(R, N), n, lot, nper), "pentadiagonal")
+
+    # -- physics (reference names) -----------------------------------------
+    def Compute_gamma(self, Y):
+        self._check(self.lib.st_compute_gamma(self._h, self._a(Y)), "Compute_gamma")
+
+    def RHS(self, Q, Qrhs, Y):
+        self._check(self.lib.st_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y)), "RHS")
+
+    def Compute_hyper(self, Q, Y):
+        self._check(self.lib.st_compute_hyper(self._h, self._a(Q, 5), self._a(Y)), "Compute_hyper")
+
+    def Hyper_RHS(self, Q, Qrhs, Y):
+        self._check(self.lib.st_hyper_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y)), "Hyper_RHS")
+
+    def Species_RHS(self, Q, Qrhs, Y, Yrhs):
+        self._check(self.lib.st_species_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y),
+                                            self._a(Yrhs)), "Species_RHS")
+
+    def bc_RHS(self, Q, Qrhs, Y, Yrhs, time=0.0):
+        self._check(self.lib.st_bc_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y), self._a(Yrhs),
+                                       float(time)), "bc_RHS")
+
+    def Sponge_Forcing(self, Q, Qrhs, Y, Yrhs):
+        self._check(self.lib.st_sponge_forcing(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y),
+                                               self._a(Yrhs)), "Sponge_Forcing")
+
+    def Fix_Pressure(self, Q, Y):
+        self._check(self.lib.st_fix_pressure(self._h, self._a(Q, 5), self._a(Y)), "Fix_Pressure")
+
+    def Compact_Filter(self, F, F0, N):
+        self._check(self.lib.st_compact_filter(self._h, self._a(F, N), self._a(F0, N), N), "Compact_Filter")
+
+    def Gaussian_Filter(self, F, Fg, N):
+        self._check(self.lib.st_gaussian_filter(self._h, self._a(F, N), self._a(Fg, N), N), "Gaussian_Filter")
+
+    def Compute_CFL(self, Q):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.st_compute_cfl(self._h, self._a(Q, 5), ctypes.byref(a), ctypes.byref(b)),
+                    "Compute_CFL")
+        return a.value, b.value
+
+    def Compute_Tstep(self, Q, Y, cfl_resv, step):
+        t = ctypes.c_double()
+        self._check(self.lib.st_compute_tstep(self._h, self._a(Q, 5), self._a(Y), float(cfl_resv), int(step),
+                                              ctypes.byref(t)), "Compute_Tstep")
+        return t.value
+
+    def LDDRK4(self, time, step):
+        """LDDRK4(time, step) on the resident state; returns (time, step)."""
+        t, s = ctypes.c_double(time), ctypes.c_int(step)
+        self._check(self.lib.st_lddrk4(self._h, ctypes.byref(t), ctypes.byref(s)), "LDDRK4")
+        return t.value, s.value
+
+    def step(self, time, step):
+        """Compute_CFL + Compute_Tstep + LDDRK4 (src/main_mf.f:137-143)."""
+        t, s = ctypes.c_double(time), ctypes.c_int(step)
+        self._check(self.lib.st_step(self._h, ctypes.byref(t), ctypes.byref(s)), "step")
+        return t.value, s.value
+
+    def monitors(self):
+        out = np.zeros(10)
+        self._check(self.lib.st_get_monitors(self._h, out.ctypes.data), "st_get_monitors")
+        return out
+
+    def sync(self):
+        self._check(self.lib.st_sync(self._h), "st_sync")
+
+
+def _make_line_op(cname, kind):
+    if kind == "d1":
+        def op(self, F, dF, iadd, cadd):
+            self._check(getattr(self.lib, cname)(self._h, self._a(F), self._a(dF), int(iadd), float(cadd)), cname)
+    elif kind == "d2":
+        def op(self, F, dF, d2F, iadd):
+            dptr = self._a(dF) if (iadd or dF is not None) else None
+            self._check(getattr(self.lib, cname)(self._h, self._a(F), dptr, self._a(d2F), int(iadd)), cname)
+    else:
+        def op(self, F, F0):
+            self._check(getattr(self.lib, cname)(self._h, self._a(F), self._a(F0)), cname)
+    op.__name__ = cname
+    return op
+
+
+for _d in ("X", "Y", "Z"):
+    for _s in ("sym", "asym"):
+        setattr(Solver, f"DFD{_d}_{_s}", _make_line_op(f"st_dfd{_d.lower()}_{_s}", "d1"))
+        setattr(Solver, f"D2FD{_d}2_{_s}", _make_line_op(f"st_d2fd{_d.lower()}2_{_s}", "d2"))
+        setattr(Solver, f"Compact_Filter_{_d}_{_s}", _make_line_op(f"st_compact_filter_{_d.lower()}_{_s}", "f"))
+    setattr(Solver, f"Gaussian_Filter_{_d}", _make_line_op(f"st_gaussian_filter_{_d.lower()}", "f"))
+
+__all__ = ["Solver", "StError", "StParams", "default_params"]

@@ -1,0 +1,679 @@
+// st_api.cpp - C ABI (include/st_b200.h): context life cycle, COMMON-block
+// mirrors, host/device argument staging and the reference-named entry points.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include "st_internal.h"
+
+namespace st {
+
+int fail(st_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+struct OomError : std::runtime_error {
+    OomError() : std::runtime_error("device scratch allocation failed") {}
+};
+
+double *scratch(st_ctx *c, int nf) {
+    for (auto &e : c->pool)
+        if (!e.used && e.nf == nf) { e.used = true; return e.p; }
+    void *p = nullptr;
+    if (cudaMalloc(&p, (size_t)nf * c->dm.n3 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        c->pool_oom = true;
+        throw OomError();
+    }
+    c->pool.push_back({(double *)p, nf, true});
+    return (double *)p;
+}
+
+int prof_start(st_ctx *c, const char *name, double bytes) {
+    c->launches++;
+    if (!c->prof) return -1;
+    cudaEvent_t ev[2];
+    for (int q = 0; q < 2; q++) {
+        if (!c->evpool.empty()) { ev[q] = c->evpool.back(); c->evpool.pop_back(); }
+        else if (cudaEventCreate(&ev[q]) != cudaSuccess) { cudaGetLastError(); return -1; }
+    }
+    cudaEventRecord(ev[0], c->stream);
+    c->prec.push_back({name, bytes, ev[0], ev[1]});
+    return (int)c->prec.size() - 1;
+}
+
+void prof_stop(st_ctx *c, int idx) {
+    if (idx >= 0) cudaEventRecord(c->prec[idx].b, c->stream);
+}
+
+void release(st_ctx *c, double *p) {
+    for (auto &e : c->pool)
+        if (e.p == p) { e.used = false; return; }
+}
+
+// ---- argument staging ------------------------------------------------------
+// Each array argument is either used in place (device memory of the context's
+// device) or staged through a pooled device buffer (host memory).
+class Args {
+  public:
+    explicit Args(st_ctx *c) : c_(c) {}
+    ~Args() { for (auto &a : v_) if (a.staged) release(c_, a.dev); }
+    // returns the device pointer to use for p (nf fields of N^3)
+    double *map(const double *p, int nf, bool in, bool out) {
+        for (auto &a : v_)
+            if (a.host == p) { a.in |= in; a.out |= out; return a.dev; }
+        Arg a{p, nullptr, nf, in, out, false};
+        cudaPointerAttributes at{};
+        bool dev = false;
+        if (cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+            (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged))
+            dev = at.device == c_->dev;
+        cudaGetLastError();
+        if (dev) {
+            a.dev = const_cast<double *>(p);
+        } else {
+            a.dev = scratch(c_, nf);
+            a.staged = true;
+            if (in && cudaMemcpyAsync(a.dev, p, bytes(nf), cudaMemcpyHostToDevice, c_->stream) != cudaSuccess)
+                err_ = true;
+        }
+        v_.push_back(a);
+        return a.dev;
+    }
+    // late input flag: an argument that is both read and written
+    int finish() {
+        for (auto &a : v_)
+            if (a.staged && a.out)
+                if (cudaMemcpyAsync(const_cast<double *>(a.host), a.dev, bytes(a.nf), cudaMemcpyDeviceToHost,
+                                    c_->stream) != cudaSuccess)
+                    err_ = true;
+        cudaError_t e = cudaStreamSynchronize(c_->stream);
+        if (err_ || e != cudaSuccess)
+            return fail(c_, ST_E_CUDA, std::string("argument transfer: ") + cudaGetErrorString(
+                                                                                 e != cudaSuccess ? e : cudaErrorInvalidValue));
+        return ST_OK;
+    }
+
+  private:
+    struct Arg { const double *host; double *dev; int nf; bool in, out, staged; };
+    size_t bytes(int nf) const { return (size_t)nf * c_->dm.n3 * sizeof(double); }
+    st_ctx *c_;
+    std::vector<Arg> v_;
+    bool err_ = false;
+};
+
+
+}  // namespace st
+
+using namespace st;
+
+#define API_BEGIN(c)                                                            \
+    if (!(c)) return ST_E_ARG;                                                  \
+    if (cudaSetDevice((c)->dev) != cudaSuccess) return fail(c, ST_E_CUDA, "cudaSetDevice"); \
+    try {
+#define API_END(c)                                                              \
+    } catch (const OomError &) {                                                \
+        return fail(c, ST_E_NOMEM, "device scratch allocation failed");        \
+    } catch (const std::bad_alloc &) {                                          \
+        return fail(c, ST_E_NOMEM, "host allocation failed");                  \
+    }
+
+extern "C" {
+
+const char *st_status_string(int s) {
+    switch (s) {
+        case ST_OK: return "ok";
+        case ST_E_ARG: return "bad argument";
+        case ST_E_NOMEM: return "out of memory";
+        case ST_E_CUDA: return "CUDA error";
+        case ST_E_UNSUPPORTED: return "unsupported size or mode";
+        case ST_E_NONFINITE: return "non-finite value in the state";
+        case ST_E_NODEVICE: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char *st_last_error(const st_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+void st_default_params(st_params *p, int nx, int ny, int nz) {
+    std::memset(p, 0, sizeof(*p));
+    p->nx = nx; p->ny = ny; p->nz = nz;
+    p->x_leng = p->y_leng = p->z_leng = 2.0 * M_PI;
+    p->re = 0.0;
+    p->re1 = 100.0; p->re2 = 100.0; p->pr = 0.7; p->sc = 1.0;
+    p->gamma1 = 1.4; p->gamma2 = 1.09; p->epsilon = 0.198265856; p->vis_exp = 0.76;
+    p->bulk_ratio = 0.0; p->t_ratio = 1.0;
+    p->hyper_param = 1; p->rk_mode = 0; p->cfl_cal = 0.5; p->c_beta_scale = 1.0; p->device = 0;
+}
+
+int st_create(const st_params *p, st_ctx **out) {
+    if (!p || !out) return ST_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return ST_E_NODEVICE; }
+    if (p->device < 0 || p->device >= ndev) return ST_E_ARG;
+    const int n[3] = {p->nx, p->ny, p->nz};
+    for (int d = 0; d < 3; d++)
+        if (n[d] % kSeg != 0 || n[d] < kSeg || n[d] > kSeg * kMaxS) return ST_E_UNSUPPORTED;
+    st_ctx *c = new (std::nothrow) st_ctx();
+    if (!c) return ST_E_NOMEM;
+    c->p = *p;
+    c->dev = p->device;
+    c->dm.n[0] = p->nx; c->dm.n[1] = p->ny; c->dm.n[2] = p->nz;
+    c->dm.n3 = (size_t)p->nx * p->ny * p->nz;
+    auto bail = [&](int code, const char *m) { c->err = m; st_destroy(c); return code; };
+    if (cudaSetDevice(c->dev) != cudaSuccess) return bail(ST_E_CUDA, "cudaSetDevice");
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(ST_E_CUDA, "cudaStreamCreate");
+    c->stream = c->own_stream;
+    // Setup_Grid src/grid.f:15-112 (uniform grids, Uniform_X :116-128)
+    const double leng[3] = {p->x_leng, p->y_leng, p->z_leng}, start[3] = {p->x_start, p->y_start, p->z_start};
+    double D[3];
+    for (int d = 0; d < 3; d++) {
+        c->s1[d] = 1.0 / leng[d];
+        c->s2[d] = c->s1[d] * c->s1[d];
+        double g1 = start[d] + leng[d] * (double)(0) / (double)(n[d] - 1);
+        double g2 = start[d] + leng[d] * (double)(1) / (double)(n[d] - 1);
+        D[d] = g2 - g1;
+    }
+    c->DX = D[0]; c->DY = D[1]; c->DZ = D[2];
+    // Define_Param src/define_nonperiodic_mf.f:182-204
+    c->Re1_inv = p->re1 > 0.0 ? 1.0 / p->re1 : 0.0;
+    c->Re2_inv = p->re2 > 0.0 ? 1.0 / p->re2 : 0.0;
+    c->Pr_inv = p->pr > 0.0 ? 1.0 / p->pr : 0.0;
+    c->Sc_inv = p->sc > 0.0 ? 1.0 / p->sc : 0.0;
+    fill_consts(c->k);
+    if (build_tables(c) != ST_OK) return bail(ST_E_NOMEM, "tables");
+    const size_t b = c->dm.n3 * sizeof(double);
+    auto al = [&](double **q, int nf) { return cudaMalloc((void **)q, nf * b) == cudaSuccess &&
+                                              cudaMemset(*q, 0, nf * b) == cudaSuccess; };
+    bool ok = al(&c->Q, 5) && al(&c->dQ, 5) && al(&c->QW, 5) && al(&c->Y, 1) && al(&c->drYi, 1) &&
+              al(&c->rYW, 1) && al(&c->gamma_eff, 1);
+    for (int g = 0; g < 12 && ok; g++) ok = al(&c->grad[g], 1);
+    for (int h = 0; h < 4 && ok; h++) ok = al(&c->hyp[h], 1);
+    for (int h = 0; h < 3 && ok; h++) ok = al(&c->dYd[h], 1);
+    ok = ok && cudaMalloc((void **)&c->dscal, 16 * sizeof(double)) == cudaSuccess &&
+         cudaMemset(c->dscal, 0, 16 * sizeof(double)) == cudaSuccess &&
+         cudaMallocHost((void **)&c->hpinned, 16 * sizeof(double)) == cudaSuccess;
+    if (!ok) { cudaGetLastError(); return bail(ST_E_NOMEM, "device allocation of the COMMON blocks failed"); }
+    *out = c;
+    return ST_OK;
+}
+
+int st_destroy(st_ctx *c) {
+    if (!c) return ST_E_ARG;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &r : c->prec) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : c->evpool) cudaEventDestroy(e);
+    free_tables(c);
+    double *arrs[] = {c->Q, c->dQ, c->QW, c->Y, c->drYi, c->rYW, c->gamma_eff, c->dscal};
+    for (double *a : arrs) if (a) cudaFree(a);
+    for (double *a : c->grad) if (a) cudaFree(a);
+    for (double *a : c->hyp) if (a) cudaFree(a);
+    for (double *a : c->dYd) if (a) cudaFree(a);
+    for (auto &e : c->pool) cudaFree(e.p);
+    if (c->hpinned) cudaFreeHost(c->hpinned);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return ST_OK;
+}
+
+int st_sync(st_ctx *c) {
+    API_BEGIN(c)
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+// ---- state -------------------------------------------------------------------
+int st_set_state(st_ctx *c, const double *Q, const double *Y) {
+    if (!Q || !Y) return ST_E_ARG;
+    API_BEGIN(c)
+    const size_t b = c->dm.n3 * 8;
+    ST_CUDA(c, cudaMemcpyAsync(c->Q, Q, 5 * b, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaMemcpyAsync(c->Y, Y, b, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaMemsetAsync(c->QW, 0, 5 * b, c->stream));
+    ST_CUDA(c, cudaMemsetAsync(c->dQ, 0, 5 * b, c->stream));
+    ST_CUDA(c, cudaMemsetAsync(c->rYW, 0, b, c->stream));
+    ST_CUDA(c, cudaMemsetAsync(c->drYi, 0, b, c->stream));
+    ST_CUDA(c, cudaMemsetAsync(c->dscal + 7, 0, sizeof(double), c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_get_state(st_ctx *c, double *Q, double *Y) {
+    API_BEGIN(c)
+    const size_t b = c->dm.n3 * 8;
+    if (Q) ST_CUDA(c, cudaMemcpyAsync(Q, c->Q, 5 * b, cudaMemcpyDefault, c->stream));
+    if (Y) ST_CUDA(c, cudaMemcpyAsync(Y, c->Y, b, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_set_tstep(st_ctx *c, double t) {
+    API_BEGIN(c)
+    c->Tstep = t;
+    c->hpinned[6] = t;
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + 6, c->hpinned + 6, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_get_tstep(st_ctx *c, double *t) {
+    if (!t) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_CUDA(c, cudaMemcpyAsync(c->hpinned + 6, c->dscal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->Tstep = c->hpinned[6];
+    *t = c->Tstep;
+    return ST_OK;
+    API_END(c)
+}
+
+static double *common_ptr(st_ctx *c, const char *name, int *nf) {
+    static const char *gn[12] = {"dux_dx", "duy_dx", "duz_dx", "dux_dy", "duy_dy", "duz_dy",
+                                 "dux_dz", "duy_dz", "duz_dz", "dTdx", "dTdy", "dTdz"};
+    static const char *hn[4] = {"beta_hyper", "visc_hyper", "k_hyper", "D_hyper"};
+    *nf = 1;
+    for (int q = 0; q < 12; q++) if (!std::strcmp(name, gn[q])) return c->grad[q];
+    for (int q = 0; q < 4; q++) if (!std::strcmp(name, hn[q])) return c->hyp[q];
+    if (!std::strcmp(name, "gamma_eff")) return c->gamma_eff;
+    if (!std::strcmp(name, "drYi")) return c->drYi;
+    if (!std::strcmp(name, "rYW")) return c->rYW;
+    *nf = 5;
+    if (!std::strcmp(name, "dQ")) return c->dQ;
+    if (!std::strcmp(name, "QW")) return c->QW;
+    return nullptr;
+}
+
+int st_get_common(st_ctx *c, const char *name, double *out) {
+    if (!name || !out) return ST_E_ARG;
+    API_BEGIN(c)
+    int nf;
+    double *p = common_ptr(c, name, &nf);
+    if (!p) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    ST_CUDA(c, cudaMemcpyAsync(out, p, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_set_common(st_ctx *c, const char *name, const double *in) {
+    if (!name || !in) return ST_E_ARG;
+    API_BEGIN(c)
+    int nf;
+    double *p = common_ptr(c, name, &nf);
+    if (!p) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    ST_CUDA(c, cudaMemcpyAsync(p, in, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+// ---- line solvers --------------------------------------------------------------
+int st_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C, double *R, int n, int lot,
+                   int nper) {
+    if (!A || !B || !C || !R || n < 1 || lot < 1) return ST_E_ARG;
+    API_BEGIN(c)
+    const size_t N = (size_t)n * lot, bytes = N * 8;
+    double *buf = nullptr;
+    ST_CUDA(c, cudaMalloc((void **)&buf, 4 * bytes));
+    double *dA = buf, *dB = buf + N, *dC = buf + 2 * N, *dR = buf + 3 * N;
+    const double *src[4] = {A, B, C, R};
+    double *dst[4] = {dA, dB, dC, dR};
+    for (int q = 0; q < 4; q++) cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyDefault, c->stream);
+    int rc = dev_tridiagonal(c, dA, dB, dC, dR, n, lot, nper);
+    if (rc == ST_OK) cudaMemcpyAsync(R, dR, bytes, cudaMemcpyDefault, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (rc != ST_OK) return rc;
+    if (e != cudaSuccess) return fail(c, ST_E_CUDA, cudaGetErrorString(e));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C, const double *D,
+                     const double *E, double *R, int n, int lot, int nper) {
+    if (!A || !B || !C || !D || !E || !R || n < 1 || lot < 1) return ST_E_ARG;
+    API_BEGIN(c)
+    const size_t N = (size_t)n * lot, bytes = N * 8;
+    double *buf = nullptr;
+    ST_CUDA(c, cudaMalloc((void **)&buf, 6 * bytes));
+    const double *src[6] = {A, B, C, D, E, R};
+    for (int q = 0; q < 6; q++) cudaMemcpyAsync(buf + q * N, src[q], bytes, cudaMemcpyDefault, c->stream);
+    int rc = dev_pentadiagonal(c, buf, buf + N, buf + 2 * N, buf + 3 * N, buf + 4 * N, buf + 5 * N, n, lot, nper);
+    if (rc == ST_OK) cudaMemcpyAsync(R, buf + 5 * N, bytes, cudaMemcpyDefault, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (rc != ST_OK) return rc;
+    if (e != cudaSuccess) return fail(c, ST_E_CUDA, cudaGetErrorString(e));
+    return ST_OK;
+    API_END(c)
+}
+
+// ---- derivatives and filters ------------------------------------------------
+static int do_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
+    if (!F || !dF || (iadd != 0 && iadd != 1)) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    double *dFd = a.map(dF, 1, iadd == 1, true);
+    const double *Fd = a.map(F, 1, true, false);
+    ST_TRY(dev_dfd(c, dir, asym, Fd, dFd, iadd, cadd));
+    return a.finish();
+    API_END(c)
+}
+static int do_d2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
+    if (!F || !d2F || (iadd && !dF)) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Fd = a.map(F, 1, true, false);
+    double *d2 = a.map(d2F, 1, false, true);
+    double *d1 = iadd ? a.map(dF, 1, false, true) : nullptr;
+    ST_TRY(dev_d2fd2(c, dir, asym, Fd, d1, d2, iadd));
+    return a.finish();
+    API_END(c)
+}
+static int do_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
+    if (!F || !F0) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Fd = a.map(F, 1, true, false);
+    double *Od = a.map(F0, 1, false, true);
+    ST_TRY(dev_filter(c, dir, asym, Fd, Od));
+    return a.finish();
+    API_END(c)
+}
+static int do_gauss(st_ctx *c, int dir, const double *F, double *Fg) {
+    if (!F || !Fg) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Fd = a.map(F, 1, true, false);
+    double *Od = a.map(Fg, 1, false, true);
+    if (Fd == Od) {
+        Scratch t(c);
+        ST_TRY(dev_gauss(c, dir, Fd, t));
+        ST_CUDA(c, cudaMemcpyAsync(Od, t, c->dm.n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        ST_TRY(dev_gauss(c, dir, Fd, Od));
+    }
+    return a.finish();
+    API_END(c)
+}
+
+int st_dfdx_sym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 0, 0, F, dF, iadd, cadd); }
+int st_dfdy_sym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 1, 0, F, dF, iadd, cadd); }
+int st_dfdz_sym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 2, 0, F, dF, iadd, cadd); }
+int st_dfdx_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 0, 1, F, dF, iadd, cadd); }
+int st_dfdy_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 1, 1, F, dF, iadd, cadd); }
+int st_dfdz_asym(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 2, 1, F, dF, iadd, cadd); }
+int st_d2fdx2_sym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 0, 0, F, dF, d2F, iadd); }
+int st_d2fdy2_sym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 1, 0, F, dF, d2F, iadd); }
+int st_d2fdz2_sym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 2, 0, F, dF, d2F, iadd); }
+int st_d2fdx2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 0, 1, F, dF, d2F, iadd); }
+int st_d2fdy2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 1, 1, F, dF, d2F, iadd); }
+int st_d2fdz2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 2, 1, F, dF, d2F, iadd); }
+int st_compact_filter_x_sym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 0, 0, F, F0); }
+int st_compact_filter_y_sym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 1, 0, F, F0); }
+int st_compact_filter_z_sym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 2, 0, F, F0); }
+int st_compact_filter_x_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 0, 1, F, F0); }
+int st_compact_filter_y_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 1, 1, F, F0); }
+int st_compact_filter_z_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 2, 1, F, F0); }
+int st_gaussian_filter_x(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 0, F, Fg); }
+int st_gaussian_filter_y(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 1, F, Fg); }
+int st_gaussian_filter_z(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 2, F, Fg); }
+
+int st_compact_filter(st_ctx *c, const double *F, double *F0, int nvar) {
+    if (!F || !F0 || nvar < 1) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Fd = a.map(F, nvar, true, false);
+    double *Od = a.map(F0, nvar, false, true);
+    ST_TRY(dev_compact_filter(c, Fd, Od, nvar));
+    return a.finish();
+    API_END(c)
+}
+
+int st_gaussian_filter(st_ctx *c, const double *F, double *Fg, int nvar) {
+    if (!F || !Fg || nvar < 1) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Fd = a.map(F, nvar, true, false);
+    double *Od = a.map(Fg, nvar, false, true);
+    if (Fd == Od) return fail(c, ST_E_ARG, "Gaussian_Filter output may not alias its input");
+    ST_TRY(dev_gaussian_filter(c, Fd, Od, nvar));
+    return a.finish();
+    API_END(c)
+}
+
+// ---- physics operators ---------------------------------------------------------
+int st_compute_gamma(st_ctx *c, const double *Y) {
+    if (!Y) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    ST_TRY(dev_compute_gamma(c, a.map(Y, 1, true, false)));
+    return a.finish();
+    API_END(c)
+}
+
+int st_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
+    if (!Q || !Qrhs || !Y) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    double *Qd = a.map(Q, 5, true, true);
+    double *Rd = a.map(Qrhs, 5, false, true);
+    const double *Yd = a.map(Y, 1, true, false);
+    ST_TRY(dev_rhs(c, Qd, Rd, Yd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
+    if (!Q || !Y) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    const double *Yd = a.map(Y, 1, true, false);
+    ST_TRY(dev_compute_hyper(c, Qd, Yd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
+    if (!Q || !Qrhs || !Y) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    double *Rd = a.map(Qrhs, 5, true, true);
+    const double *Yd = a.map(Y, 1, true, false);
+    ST_TRY(dev_hyper_rhs(c, Qd, Rd, Yd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    double *Rd = a.map(Qrhs, 5, true, true);
+    const double *Yd = a.map(Y, 1, true, false);
+    double *YRd = a.map(Yrhs, 1, true, true);
+    ST_TRY(dev_species_rhs(c, Qd, Rd, Yd, YRd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs, double time) {
+    (void)time;
+    if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    double *Qd = a.map(Q, 5, true, true);
+    double *Rd = a.map(Qrhs, 5, true, true);
+    const double *Yd = a.map(Y, 1, true, false);
+    double *YRd = a.map(Yrhs, 1, true, true);
+    ST_TRY(dev_bc_rhs(c, Qd, Rd, Yd, YRd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_sponge_forcing(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    double *Rd = a.map(Qrhs, 5, true, true);
+    const double *Yd = a.map(Y, 1, true, false);
+    double *YRd = a.map(Yrhs, 1, true, true);
+    ST_TRY(dev_sponge(c, Qd, Rd, Yd, YRd));
+    return a.finish();
+    API_END(c)
+}
+
+int st_fix_pressure(st_ctx *c, double *Q, const double *Y) {
+    (void)Y;
+    if (!Q) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    ST_TRY(dev_fix_pressure(c, a.map(Q, 5, true, true)));
+    return a.finish();
+    API_END(c)
+}
+
+int st_compute_cfl(st_ctx *c, const double *Q, double *cfl_stab, double *cfl_resv) {
+    if (!Q) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    ST_TRY(dev_compute_cfl(c, Qd, true, cfl_stab, cfl_resv));
+    return a.finish();
+    API_END(c)
+}
+
+int st_compute_tstep(st_ctx *c, const double *Q, const double *Y, double cfl_resv, int step, double *tstep) {
+    if (!Q || !Y) return ST_E_ARG;
+    API_BEGIN(c)
+    Args a(c);
+    const double *Qd = a.map(Q, 5, true, false);
+    const double *Yd = a.map(Y, 1, true, false);
+    ST_TRY(dev_compute_tstep(c, Qd, Yd, step, false, cfl_resv));
+    ST_CUDA(c, cudaMemcpyAsync(c->hpinned + 6, c->dscal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ST_TRY(a.finish());
+    c->Tstep = c->hpinned[6];
+    if (tstep) *tstep = c->Tstep;
+    return ST_OK;
+    API_END(c)
+}
+
+// ---- time integration ------------------------------------------------------------
+static int read_time(st_ctx *c, double *time) {
+    ST_CUDA(c, cudaMemcpyAsync(c->hpinned + 7, c->dscal + 7, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (time) *time = c->hpinned[7];
+    return ST_OK;
+}
+
+int st_lddrk4(st_ctx *c, double *time, int *step) {
+    if (!time || !step) return ST_E_ARG;
+    API_BEGIN(c)
+    c->hpinned[7] = *time;
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + 7, c->hpinned + 7, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ST_TRY(dev_lddrk4(c, true));
+    ST_TRY(dev_monitors(c));
+    ST_TRY(read_time(c, time));
+    *step = *step + 1;
+    return ST_OK;
+    API_END(c)
+}
+
+int st_step(st_ctx *c, double *time, int *step) {
+    if (!time || !step) return ST_E_ARG;
+    API_BEGIN(c)
+    c->hpinned[7] = *time;
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + 7, c->hpinned + 7, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ST_TRY(dev_compute_cfl(c, c->Q, false, nullptr, nullptr));
+    ST_TRY(dev_compute_tstep(c, c->Q, c->Y, *step, true, 0.0));
+    ST_TRY(dev_lddrk4(c, true));
+    ST_TRY(read_time(c, time));
+    *step = *step + 1;
+    return ST_OK;
+    API_END(c)
+}
+
+int st_set_stream(st_ctx *c, void *stream) {
+    API_BEGIN(c)
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return ST_OK;
+    API_END(c)
+}
+
+int st_get_stream(st_ctx *c, void **stream) {
+    if (!c || !stream) return ST_E_ARG;
+    *stream = (void *)c->stream;
+    return ST_OK;
+}
+
+int st_profile(st_ctx *c, int enable) {
+    if (!c) return ST_E_ARG;
+    c->prof = enable != 0;
+    return ST_OK;
+}
+
+int st_launch_count(st_ctx *c, long long *count) {
+    if (!c || !count) return ST_E_ARG;
+    *count = c->launches;
+    return ST_OK;
+}
+
+int st_profile_report(st_ctx *c, char *buf, int buflen) {
+    if (!buf || buflen < 3) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    struct Agg { long long n = 0; double ms = 0, bytes = 0; };
+    std::vector<std::pair<std::string, Agg>> agg;
+    for (auto &r : c->prec) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        size_t k = 0;
+        while (k < agg.size() && agg[k].first != r.name) k++;
+        if (k == agg.size()) agg.push_back({r.name, Agg()});
+        agg[k].second.n++; agg[k].second.ms += ms; agg[k].second.bytes += r.bytes;
+        c->evpool.push_back(r.a); c->evpool.push_back(r.b);
+    }
+    c->prec.clear();
+    cudaGetLastError();
+    std::string s = "{";
+    char tmp[256];
+    for (size_t k = 0; k < agg.size(); k++) {
+        std::snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"bytes\": %.1f}",
+                      k ? ", " : "", agg[k].first.c_str(), agg[k].second.n, agg[k].second.ms, agg[k].second.bytes);
+        s += tmp;
+    }
+    s += "}";
+    if ((int)s.size() + 1 > buflen) return fail(c, ST_E_ARG, "report buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return ST_OK;
+    API_END(c)
+}
+
+int st_get_monitors(st_ctx *c, double out[10]) {
+    if (!out) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_TRY(dev_monitors(c));
+    ST_CUDA(c, cudaMemcpyAsync(c->hpinned, c->dscal, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::memcpy(out, c->mon, 8 * sizeof(double));
+    out[8] = c->hpinned[1];
+    out[9] = c->hpinned[6];
+    return ST_OK;
+    API_END(c)
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// st_internal.h - private declarations of the B200 solver library.
+//
+// Device layout: every field is an N^3 double array in the reference layout
+// F(My,Mz,Mx) (y fastest); multi-variable arrays are nvar consecutive fields.
+// Lines along y are contiguous, lines along z have stride My and lines along
+// x have stride My*Mz.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "../../include/st_b200.h"
+
+namespace st {
+
+constexpr int kSeg = 32;          // segments per line = lanes of a warp
+constexpr int kScanSteps = 5;     // log2(kSeg)
+constexpr int kMaxS = 16;         // max points per lane (N <= 512)
+
+// Row tables of a constant-coefficient tridiagonal system, factorised as the
+// reference's tridiagonal_serial does (src/tridiagonal.f90:264-287), plus the
+// per-segment carry coefficients of the segmented solve.
+struct TriTab {
+    const double *l;    // forward multiplier of row i (row 0: 0)
+    const double *g;    // response of the forward value of row i to the carry-in
+    const double *up;   // upper diagonal c_i
+    const double *id;   // 1 / (b'_i + tiny)   (last row: 1 / b'_n)
+    const double *h;    // response of x_i to the carry from the right
+    const double *bk;   // [kSeg][kScanSteps] running products, forward scan
+    const double *gk;   // [kSeg][kScanSteps] running products, reverse scan
+};
+
+// Same for the pentadiagonal systems of the compact filter
+// (pentadiagonal_serial, src/pentadiagonal.f90:319-374).
+struct PenTab {
+    const double *p1, *p2;   // forward multipliers of r'_{i-1}, r'_{i-2}
+    const double *g1, *g2;   // forward carry responses (carry = (r'_{a-1}, r'_{a-2}))
+    const double *q1, *q2;   // back-substitution coefficients of x_{i+1}, x_{i+2}
+    const double *id;        // 1 / (C'_i + tiny)
+    const double *h1, *h2;   // backward carry responses (carry = (x_{b+1}, x_{b+2}))
+    const double *mk;        // [kSeg][kScanSteps][4] forward scan 2x2 products
+    const double *nk;        // [kSeg][kScanSteps][4] reverse scan 2x2 products
+};
+
+enum TriKind { K_D1S = 0, K_D1A = 1, K_D2S = 2, K_D2A = 3 };
+enum PenKind { K_FS = 0, K_FA = 1 };
+
+// Scheme constants (src/header:173-204, src/LES_header:107-157).
+struct Consts {
+    double a1, b1, a2, b2, c2, closure1, closure2;
+    double fa0, fa1, fa2, fa3, fa4;        // compact filter RHS
+    double bc1[6], bc2[6], bc3[3], bc4[4]; // Visbal-Gaitonde closures
+    double ga[5];                          // Gaussian coefficients (float32 values)
+};
+
+enum { G_DUX_DX, G_DUY_DX, G_DUZ_DX, G_DUX_DY, G_DUY_DY, G_DUZ_DY,
+       G_DUX_DZ, G_DUY_DZ, G_DUZ_DZ, G_DTDX, G_DTDY, G_DTDZ };
+enum { H_BETA, H_VISC, H_K, H_D };
+
+struct Dims {
+    int n[3];          // Mx, My, Mz
+    size_t n3;
+};
+
+}  // namespace st
+
+struct st_ctx {
+    st_params p;
+    st::Dims dm;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // derived scalars
+    double s1[3], s2[3];
+    double DX, DY, DZ;
+    double Re1_inv, Re2_inv, Pr_inv, Sc_inv;
+    double Tstep = 0.0;
+    double last_cfl_resv = 0.0, last_cfl_stab = 0.0;
+    double mon[10] = {0};
+    st::Consts k;
+    // tables [dir][kind]
+    st::TriTab tri[3][4];
+    st::PenTab pen[3][2];
+    std::vector<void *> table_allocs;
+    // COMMON blocks
+    double *Q = nullptr, *dQ = nullptr, *QW = nullptr;
+    double *Y = nullptr, *drYi = nullptr, *rYW = nullptr, *gamma_eff = nullptr;
+    double *grad[12] = {nullptr};
+    double *hyp[4] = {nullptr};
+    double *dYd[3] = {nullptr};
+    // scratch field pool
+    struct PoolEntry { double *p; int nf; bool used; };
+    std::vector<PoolEntry> pool;
+    bool pool_oom = false;
+    // device scalars (reductions, dt)
+    double *dscal = nullptr;     // [16]
+    double *hpinned = nullptr;   // pinned host mirror [16]
+    // host<->device staging for the per-operator entry points
+    std::vector<double *> stage;
+    cudaStream_t own_stream = nullptr;
+    // instrumentation
+    long long launches = 0;
+    bool prof = false;
+    struct ProfRec { const char *name; double bytes; cudaEvent_t a, b; };
+    std::vector<ProfRec> prec;
+    std::vector<cudaEvent_t> evpool;
+};
+
+namespace st {
+
+// error helpers
+int fail(st_ctx *c, int code, const std::string &msg);
+#define ST_CUDA(c, call)                                                           \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess)                                                     \
+            return ::st::fail((c), ST_E_CUDA, std::string(#call) + ": " +          \
+                                                  cudaGetErrorString(e_));         \
+    } while (0)
+#define ST_TRY(expr)                 \
+    do {                             \
+        int r_ = (expr);             \
+        if (r_ != ST_OK) return r_;  \
+    } while (0)
+
+// launch instrumentation: every kernel launch is bracketed by these
+int prof_start(st_ctx *c, const char *name, double bytes);
+void prof_stop(st_ctx *c, int idx);
+
+// tables
+int build_tables(st_ctx *c);
+void free_tables(st_ctx *c);
+void fill_consts(Consts &k);
+
+// scratch pool
+double *scratch(st_ctx *c, int nfields = 1);   // nfields contiguous N^3 fields
+void release(st_ctx *c, double *p);
+struct Scratch {                                 // RAII helper
+    st_ctx *c; double *p;
+    explicit Scratch(st_ctx *cc, int nf = 1) : c(cc), p(scratch(cc, nf)) {}
+    ~Scratch() { release(c, p); }
+    Scratch(const Scratch &) = delete;
+    Scratch &operator=(const Scratch &) = delete;
+    operator double *() const { return p; }
+};
+
+// line operators on device arrays (st_kernels.cu)
+int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd);
+int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd);
+int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0);
+int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg);
+int dev_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C, double *R,
+                    int n, int lot, int nper);
+int dev_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C,
+                      const double *D, const double *E, double *R, int n, int lot, int nper);
+
+// physics on device arrays (st_physics.cu)
+int dev_compute_gamma(st_ctx *c, const double *Y);
+int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y);
+int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y);
+int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y);
+int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs);
+int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs);
+int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs);
+int dev_fix_pressure(st_ctx *c, double *Q);
+int dev_compact_filter(st_ctx *c, const double *F, double *F0, int nvar);
+int dev_gaussian_filter(st_ctx *c, const double *F, double *Fg, int nvar);
+int dev_compute_cfl(st_ctx *c, const double *Q, bool to_host, double *stab, double *resv);
+int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, bool resv_on_device,
+                      double cfl_resv_host);
+int dev_lddrk4(st_ctx *c, bool dt_on_device);
+int dev_monitors(st_ctx *c);
+
+}  // namespace st

@@ -1,0 +1,276 @@
+// st_tables.cpp - constant LU factors and segmented-solve tables.
+//
+// The reference stores the left-hand sides as 135 full (lot,n) arrays
+// (src/header:64-150, src/LES_header:1-63) and re-factorises them on every
+// call (src/tridiagonal.f90:39, src/pentadiagonal.f90:42).  Every line of a
+// direction has the same left-hand side (the Setup loops assign one value for
+// all lines, src/derivCDopt6_sym_tri.f:41-63), so one factorisation per
+// (direction, scheme, boundary kind) computed with the reference's own
+// operation order gives the same pivots and multipliers.
+//
+// The segmented solve splits each line into kSeg contiguous segments of
+// S = n/kSeg rows.  Each segment runs the Thomas recurrences with a zero
+// carry; the true carries are then obtained by an affine scan over the
+// segments (tables bk/gk, mk/nk) and added back through the per-row carry
+// responses (g, h).  In exact arithmetic this is the Thomas algorithm.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include "st_internal.h"
+
+namespace st {
+
+static const double kTiny = (double)FLT_MIN;   // tiny(1.0), src/tridiagonal.f90:275
+
+void fill_consts(Consts &k) {
+    // FDL3DI sixth-order compact tridiagonal set, src/header:191-204
+    k.a1 = 14.0 / 18.0; k.b1 = 1.0 / 36.0;
+    k.a2 = 12.0 / 11.0; k.b2 = 3.0 / 44.0; k.c2 = 2.0 * (k.a2 + k.b2);
+    k.closure1 = 5.0 / 9.0; k.closure2 = 1.0 / 18.0;              // src/header:173-175
+    // Cook-Cabot eighth-order filter, src/LES_header:107-113
+    k.fa0 = 9.9965e-01; k.fa1 = 0.66652; k.fa2 = 0.16674; k.fa3 = 4.0e-05; k.fa4 = -5.0e-06;
+    const double ab = 0.45, af = 6.6624e-01, bf = 1.6688e-01;   // src/LES_header:118-146
+    k.bc1[0] = 0.0;
+    k.bc1[1] = 15.0 / 16.0; k.bc1[2] = 1.0 / 4.0; k.bc1[3] = -3.0 / 8.0;
+    k.bc1[4] = 1.0 / 4.0; k.bc1[5] = -1.0 / 16.0;
+    k.bc2[0] = (1.0 / 2.0 + ab);
+    k.bc2[1] = (1.0 / 16.0 + (7.0 / 8.0) * ab);
+    k.bc2[2] = (3.0 / 4.0 + (1.0 / 2.0) * ab);
+    k.bc2[3] = (3.0 / 8.0 + (1.0 / 4.0) * ab);
+    k.bc2[4] = (-1.0 / 4.0 + (1.0 / 2.0) * ab);
+    k.bc2[5] = (1.0 / 16.0 - (1.0 / 8.0) * ab);
+    k.bc3[0] = (5.0 / 8.0 + (3.0 / 4.0) * ab);
+    k.bc3[1] = (1.0 / 2.0 + ab) / 2.0;
+    k.bc3[2] = (-1.0 / 8.0 + ab / 4.0) / 2.0;
+    k.bc4[0] = (11.0 / 16.0 + (5.0 / 8.0) * af - (5.0 / 8.0) * bf);
+    k.bc4[1] = (15.0 / 32.0 + (17.0 / 16.0) * af + (15.0 / 16.0) * bf) / 2.0;
+    k.bc4[2] = (-3.0 / 16.0 + (3.0 / 8.0) * af + (13.0 / 8.0) * bf) / 2.0;
+    k.bc4[3] = (1.0 / 32.0 - af / 16.0 + bf / 16.0) / 2.0;
+    // Gaussian filter: implicit REAL parameters, src/LES_header:153-157
+    k.ga[0] = (double)(float)(3565.0 / 10368.0);
+    k.ga[1] = (double)(float)(3091.0 / 12960.0);
+    k.ga[2] = (double)(float)(1997.0 / 25920.0);
+    k.ga[3] = (double)(float)(149.0 / 12960.0);
+    k.ga[4] = (double)(float)(107.0 / 103680.0);
+}
+
+// ---- left-hand sides ------------------------------------------------------
+// Setup_Derivatives_Sym/_Asym (src/derivCDopt6_sym_tri.f:41-372,
+// src/derivCDopt6_asym_tri.f:41-374), one-rank case.
+static void deriv_lhs(int n, int order, int asym, std::vector<double> &a, std::vector<double> &b,
+                      std::vector<double> &c) {
+    const double al1 = 1.0 / 3.0, al2 = 2.0 / 11.0;
+    double al = order == 1 ? al1 : al2;
+    a.assign(n, al); b.assign(n, 1.0); c.assign(n, al);
+    if (order == 1) {
+        a[0] = 0.0; b[0] = 1.0; c[0] = asym ? 2.0 * al1 : 0.0;
+        a[n - 1] = 2.0; b[n - 1] = 1.0; c[n - 1] = 0.0;
+        a[1] = al1; b[1] = 1.0; c[1] = al1;
+        a[n - 2] = 1.0 / 2.0; b[n - 2] = 1.0; c[n - 2] = 1.0 / 6.0;
+    } else {
+        a[0] = 0.0; b[0] = 1.0; c[0] = asym ? 0.0 : 2.0 * al2;
+        a[n - 1] = 1.1e1; b[n - 1] = 1.0; c[n - 1] = 0.0;
+        a[1] = al2; b[1] = 1.0; c[1] = al2;
+        a[n - 2] = -7.0 / 2.0e1; b[n - 2] = 1.0; c[n - 2] = 1.0e-1;
+    }
+}
+
+// Init_Filters_sym/_asym (src/filters_sym.f:44-382, src/filters_asym.f:44-384)
+static void filter_lhs(int n, int asym, std::vector<double> M[5]) {
+    const double af = 6.6624e-01, bf = 1.6688e-01, ab = 0.45;
+    M[0].assign(n, bf); M[1].assign(n, af); M[2].assign(n, 1.0); M[3].assign(n, af); M[4].assign(n, bf);
+    auto row = [&](int r, double A, double B, double C, double D, double E) {
+        M[0][r] = A; M[1][r] = B; M[2][r] = C; M[3][r] = D; M[4][r] = E;
+    };
+    if (asym) row(0, 0, 0, 1, 0, 0); else row(0, 0, 0, 1, 2.0 * af, 2.0 * bf);
+    row(n - 1, 0, 0, 1, 0, 0);
+    if (asym) row(1, 0, af, 1.0 - bf, af, bf); else row(1, 0, af, 1.0 + bf, af, bf);
+    row(n - 2, 0, ab, 1, ab, 0);
+    row(2, bf, af, 1, af, bf);
+    row(n - 3, 0, ab, 1, ab, 0);
+    row(3, bf, af, 1, af, bf);
+    row(n - 4, bf, af, 1, af, bf);
+}
+
+// ---- tables ---------------------------------------------------------------
+struct TriHost {
+    std::vector<double> l, g, up, id, h, bk, gk;
+};
+struct PenHost {
+    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mk, nk;
+};
+
+static TriHost tri_tables(const std::vector<double> &a, const std::vector<double> &b,
+                          const std::vector<double> &c, int n) {
+    TriHost t;
+    std::vector<double> bp(n);
+    t.l.assign(n, 0.0);
+    bp[0] = b[0];
+    for (int i = 1; i < n; i++) {
+        t.l[i] = a[i] / (bp[i - 1] + kTiny);
+        bp[i] = b[i] - c[i - 1] * t.l[i];
+    }
+    t.up = c;
+    t.id.resize(n);
+    for (int i = 0; i < n - 1; i++) t.id[i] = 1.0 / (bp[i] + kTiny);
+    t.id[n - 1] = 1.0 / bp[n - 1];
+    const int S = n / kSeg;
+    t.g.assign(n, 0.0); t.h.assign(n, 0.0);
+    std::vector<double> B(kSeg), G(kSeg);
+    for (int s = 0; s < kSeg; s++) {
+        int a0 = s * S;
+        double pr = 1.0;
+        for (int q = 0; q < S; q++) { pr *= -t.l[a0 + q]; t.g[a0 + q] = pr; }
+        B[s] = t.g[a0 + S - 1];
+        pr = 1.0;
+        for (int q = S - 1; q >= 0; q--) { pr *= -(t.up[a0 + q] * t.id[a0 + q]); t.h[a0 + q] = pr; }
+        G[s] = t.h[a0];
+    }
+    // running products seen by each lane at each Hillis-Steele step
+    t.bk.assign(kSeg * kScanSteps, 0.0); t.gk.assign(kSeg * kScanSteps, 0.0);
+    std::vector<double> cur = B, nxt(kSeg);
+    for (int k = 0; k < kScanSteps; k++) {
+        int off = 1 << k;
+        for (int s = 0; s < kSeg; s++) t.bk[s * kScanSteps + k] = cur[s];
+        for (int s = 0; s < kSeg; s++) nxt[s] = s >= off ? cur[s] * cur[s - off] : cur[s];
+        cur = nxt;
+    }
+    cur = G;
+    for (int k = 0; k < kScanSteps; k++) {
+        int off = 1 << k;
+        for (int s = 0; s < kSeg; s++) t.gk[s * kScanSteps + k] = cur[s];
+        for (int s = 0; s < kSeg; s++) nxt[s] = s + off < kSeg ? cur[s] * cur[s + off] : cur[s];
+        cur = nxt;
+    }
+    return t;
+}
+
+static void mat2mul(const double *A, const double *B, double *C) {  // C = A*B (row-major 2x2)
+    double r[4] = {A[0] * B[0] + A[1] * B[2], A[0] * B[1] + A[1] * B[3],
+                   A[2] * B[0] + A[3] * B[2], A[2] * B[1] + A[3] * B[3]};
+    std::memcpy(C, r, sizeof(r));
+}
+
+static PenHost pen_tables(std::vector<double> M[5], int n) {
+    PenHost t;
+    std::vector<double> A = M[0], B = M[1], C = M[2], D = M[3], E = M[4];
+    std::vector<double> k1(n, 0.0), k2(n, 0.0);
+    for (int i = 0; i <= n - 3; i++) {
+        k1[i] = B[i + 1] / (C[i] + kTiny);
+        C[i + 1] = C[i + 1] - D[i] * k1[i];
+        D[i + 1] = D[i + 1] - E[i] * k1[i];
+        k2[i] = A[i + 2] / (C[i] + kTiny);
+        B[i + 2] = B[i + 2] - D[i] * k2[i];
+        C[i + 2] = C[i + 2] - E[i] * k2[i];
+    }
+    double k3 = B[n - 1] / (C[n - 2] + kTiny);
+    C[n - 1] = C[n - 1] - D[n - 2] * k3;
+    t.p1.assign(n, 0.0); t.p2.assign(n, 0.0);
+    t.p1[1] = k1[0];
+    for (int i = 2; i <= n - 2; i++) { t.p1[i] = k1[i - 1]; t.p2[i] = k2[i - 2]; }
+    t.p1[n - 1] = k3; t.p2[n - 1] = k2[n - 3];
+    t.q1.assign(n, 0.0); t.q2.assign(n, 0.0); t.id.resize(n);
+    for (int i = 0; i <= n - 2; i++) t.q1[i] = D[i];
+    for (int i = 0; i <= n - 3; i++) t.q2[i] = E[i];
+    for (int i = 0; i < n; i++) t.id[i] = 1.0 / (C[i] + kTiny);
+    const int S = n / kSeg;
+    t.g1.assign(n, 0.0); t.g2.assign(n, 0.0); t.h1.assign(n, 0.0); t.h2.assign(n, 0.0);
+    std::vector<double> Mseg(kSeg * 4), Nseg(kSeg * 4);
+    for (int s = 0; s < kSeg; s++) {
+        int a0 = s * S;
+        for (int which = 0; which < 2; which++) {
+            // forward homogeneous response to (r'_{a-1}, r'_{a-2}) = e_which
+            double hm1 = which == 0 ? 1.0 : 0.0, hm2 = which == 0 ? 0.0 : 1.0;
+            for (int q = 0; q < S; q++) {
+                int i = a0 + q;
+                double v = (0.0 - t.p2[i] * hm2) - t.p1[i] * hm1;
+                (which == 0 ? t.g1 : t.g2)[i] = v;
+                hm2 = hm1; hm1 = v;
+            }
+            // backward homogeneous response to (x_{b+1}, x_{b+2}) = e_which
+            double kp1 = which == 0 ? 1.0 : 0.0, kp2 = which == 0 ? 0.0 : 1.0;
+            for (int q = S - 1; q >= 0; q--) {
+                int i = a0 + q;
+                double v = ((0.0 - t.q1[i] * kp1) - t.q2[i] * kp2) * t.id[i];
+                (which == 0 ? t.h1 : t.h2)[i] = v;
+                kp2 = kp1; kp1 = v;
+            }
+        }
+        double *m = &Mseg[s * 4], *nn = &Nseg[s * 4];
+        int e = a0 + S - 1;
+        if (S >= 2) {
+            m[0] = t.g1[e]; m[1] = t.g2[e]; m[2] = t.g1[e - 1]; m[3] = t.g2[e - 1];
+            nn[0] = t.h1[a0]; nn[1] = t.h2[a0]; nn[2] = t.h1[a0 + 1]; nn[3] = t.h2[a0 + 1];
+        } else {
+            m[0] = t.g1[e]; m[1] = t.g2[e]; m[2] = 1.0; m[3] = 0.0;
+            nn[0] = t.h1[a0]; nn[1] = t.h2[a0]; nn[2] = 1.0; nn[3] = 0.0;
+        }
+    }
+    t.mk.assign(kSeg * kScanSteps * 4, 0.0); t.nk.assign(kSeg * kScanSteps * 4, 0.0);
+    std::vector<double> cur = Mseg, nxt(kSeg * 4);
+    for (int k = 0; k < kScanSteps; k++) {
+        int off = 1 << k;
+        for (int s = 0; s < kSeg; s++) std::memcpy(&t.mk[(s * kScanSteps + k) * 4], &cur[s * 4], 32);
+        for (int s = 0; s < kSeg; s++) {
+            if (s >= off) mat2mul(&cur[s * 4], &cur[(s - off) * 4], &nxt[s * 4]);
+            else std::memcpy(&nxt[s * 4], &cur[s * 4], 32);
+        }
+        cur = nxt;
+    }
+    cur = Nseg;
+    for (int k = 0; k < kScanSteps; k++) {
+        int off = 1 << k;
+        for (int s = 0; s < kSeg; s++) std::memcpy(&t.nk[(s * kScanSteps + k) * 4], &cur[s * 4], 32);
+        for (int s = 0; s < kSeg; s++) {
+            if (s + off < kSeg) mat2mul(&cur[s * 4], &cur[(s + off) * 4], &nxt[s * 4]);
+            else std::memcpy(&nxt[s * 4], &cur[s * 4], 32);
+        }
+        cur = nxt;
+    }
+    return t;
+}
+
+static const double *upload(st_ctx *c, const std::vector<double> &v, int *err) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, v.size() * sizeof(double)) != cudaSuccess) { *err = 1; return nullptr; }
+    c->table_allocs.push_back(p);
+    if (cudaMemcpy(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        *err = 1;
+    return (const double *)p;
+}
+
+int build_tables(st_ctx *c) {
+    int err = 0;
+    for (int d = 0; d < 3; d++) {
+        int n = c->dm.n[d];
+        for (int kind = 0; kind < 4; kind++) {
+            std::vector<double> a, b, cc;
+            deriv_lhs(n, kind < 2 ? 1 : 2, kind & 1, a, b, cc);
+            TriHost h = tri_tables(a, b, cc, n);
+            TriTab &t = c->tri[d][kind];
+            t.l = upload(c, h.l, &err); t.g = upload(c, h.g, &err); t.up = upload(c, h.up, &err);
+            t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
+            t.bk = upload(c, h.bk, &err); t.gk = upload(c, h.gk, &err);
+        }
+        for (int kind = 0; kind < 2; kind++) {
+            std::vector<double> M[5];
+            filter_lhs(n, kind, M);
+            PenHost h = pen_tables(M, n);
+            PenTab &t = c->pen[d][kind];
+            t.p1 = upload(c, h.p1, &err); t.p2 = upload(c, h.p2, &err);
+            t.g1 = upload(c, h.g1, &err); t.g2 = upload(c, h.g2, &err);
+            t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
+            t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
+            t.mk = upload(c, h.mk, &err); t.nk = upload(c, h.nk, &err);
+        }
+    }
+    if (err) return fail(c, ST_E_NOMEM, "could not allocate or upload the LU tables");
+    return ST_OK;
+}
+
+void free_tables(st_ctx *c) {
+    for (void *p : c->table_allocs) cudaFree(p);
+    c->table_allocs.clear();
+}
+
+}  // namespace st

@@ -1,0 +1,101 @@
+"""Synthetic initial conditions and the reference restart-file format.
+
+The reference has no turbulence generator (its init/ programs build a
+converging shock with a perturbed interface), so the seeded generator below
+stands in for the benchmark inputs: a solenoidal random-phase velocity field
+with spectrum E(k) ~ k^4 exp(-2 (k/k0)^2), plus an optional Gaussian pressure
+deposit at the symmetry corner (the template of Add_Shock_Expanding,
+src/shock.f:1-86, moved to the origin of the octant domain).
+
+Thermodynamic background: rho = 1, p = 1/gamma (sound speed 1), so the rms
+velocity per component is M_t / sqrt(3) for a turbulent Mach number M_t.
+
+Restart files follow Write_Restart / Read_Restart (src/out_mf.f:453-662):
+four int32 sizes (Ny, Nz, Nx, 6), float64 time, int32 step, then
+Q(Ny,Nz,Nx,6) in Fortran order (5 conserved variables and Y), native byte
+order.
+"""
+import numpy as np
+
+
+def solenoidal_velocity(shape, k0, urms, seed):
+    """Random-phase solenoidal field on a periodic grid of the given C-order
+    shape (Mx, Mz, My); returns (u, v, w) with per-component rms ``urms``.
+    Wavenumbers are counted in units of the box fundamental."""
+    rng = np.random.default_rng(seed)
+    nx, nz, ny = shape
+    kx = np.fft.fftfreq(nx) * nx
+    kz = np.fft.fftfreq(nz) * nz
+    ky = np.fft.rfftfreq(ny) * ny
+    KX, KZ, KY = np.meshgrid(kx, kz, ky, indexing="ij")
+    k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    k = np.sqrt(k2)
+    kk = np.where(k > 0, k, 1.0)
+    spec = kk ** 4 * np.exp(-2.0 * (kk / k0) ** 2)
+    amp = np.where(k > 0, np.sqrt(spec / (4.0 * np.pi * kk ** 2)), 0.0)
+    comps = []
+    for _ in range(3):
+        ph = rng.uniform(0.0, 2.0 * np.pi, size=k.shape)
+        mag = rng.normal(size=k.shape)
+        comps.append(amp * mag * np.exp(1j * ph))
+    # project out the component along k (divergence-free)
+    dot = (comps[0] * KX + comps[1] * KY + comps[2] * KZ) / np.where(k2 > 0, k2, 1.0)
+    uh = [comps[0] - dot * KX, comps[1] - dot * KY, comps[2] - dot * KZ]
+    fields = [np.fft.irfftn(c, s=(nx, nz, ny), axes=(0, 1, 2)) for c in uh]
+    u, v, w = fields
+    rms = np.sqrt((u ** 2 + v ** 2 + w ** 2).mean() / 3.0)
+    scale = urms / rms if rms > 0 else 0.0
+    return u * scale, v * scale, w * scale
+
+
+def blast_in_turbulence(params, k0=8.0, mach_t=0.1, p_ratio=100.0, radius_cells=4.0, seed=1,
+                        y_field=None):
+    """Conserved state Q (5, Mx, Mz, My) and mass fraction Y for an
+    expanding blast (Gaussian energy deposit at the x=y=z=0 corner) in
+    isotropic turbulence.  ``p_ratio`` <= 1 gives turbulence alone."""
+    shape = (params.nx, params.nz, params.ny)
+    g = params.gamma1
+    urms = mach_t / np.sqrt(3.0)
+    u, v, w = solenoidal_velocity(shape, k0, urms, seed)
+    rho = np.ones(shape)
+    p0 = 1.0 / g
+    dx = params.x_leng / (params.nx - 1)
+    x = params.x_start + dx * np.arange(params.nx)
+    y = params.y_start + params.y_leng / (params.ny - 1) * np.arange(params.ny)
+    z = params.z_start + params.z_leng / (params.nz - 1) * np.arange(params.nz)
+    r2 = x[:, None, None] ** 2 + z[None, :, None] ** 2 + y[None, None, :] ** 2
+    p = p0 * (1.0 + (p_ratio - 1.0) * np.exp(-r2 / (radius_cells * dx) ** 2)) if p_ratio > 1.0 \
+        else np.full(shape, p0)
+    Y = np.ones(shape) if y_field is None else np.asarray(y_field, dtype=np.float64)
+    # gamma_eff of the mixture (Compute_gamma, src/lddrk4_nonperiodic_mf.f:342-372)
+    g1, g2, eps = params.gamma1, params.gamma2, params.epsilon
+    geff = ((Y * g1 / (g1 - 1.0)) + (eps * (1.0 - Y) * g2 / (g2 - 1.0))) / \
+           ((Y / (g1 - 1.0)) + (eps * (1.0 - Y) / (g2 - 1.0)))
+    Q = np.empty((5,) + shape)
+    Q[0], Q[1], Q[2], Q[3] = rho * u, rho * v, rho * w, rho
+    Q[4] = p / (geff - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return np.ascontiguousarray(Q), np.ascontiguousarray(Y)
+
+
+def write_restart(path, Q, Y, time, step):
+    """Write_Restart layout (src/out_mf.f:469-551)."""
+    nx, nz, ny = Y.shape
+    with open(path, "wb") as f:
+        np.array([ny, nz, nx, 6], dtype=np.int32).tofile(f)
+        np.array([time], dtype=np.float64).tofile(f)
+        np.array([step], dtype=np.int32).tofile(f)
+        data = np.concatenate([np.asarray(Q).reshape(5, -1), np.asarray(Y).reshape(1, -1)])
+        data.astype(np.float64).tofile(f)
+
+
+def read_restart(path):
+    """Read_Restart layout (src/out_mf.f:563-662): returns (Q, Y, time, step)."""
+    with open(path, "rb") as f:
+        ny, nz, nx, nv = np.fromfile(f, dtype=np.int32, count=4)
+        time = float(np.fromfile(f, dtype=np.float64, count=1)[0])
+        step = int(np.fromfile(f, dtype=np.int32, count=1)[0])
+        data = np.fromfile(f, dtype=np.float64, count=int(nv) * nx * ny * nz)
+    if int(nv) != 6:
+        raise ValueError(f"restart file holds {nv} variables, expected 6")
+    data = data.reshape(6, nx, nz, ny)
+    return np.ascontiguousarray(data[:5]), np.ascontiguousarray(data[5]), time, step
