@@ -156,13 +156,14 @@ int st_create(const st_params *p, st_ctx **out) {
     if (p->device < 0 || p->device >= ndev) return ST_E_ARG;
     const int n[3] = {p->nx, p->ny, p->nz};
     for (int d = 0; d < 3; d++)
-        if (n[d] % kSeg != 0 || n[d] < kSeg || n[d] > kSeg * kMaxS) return ST_E_UNSUPPORTED;
+        if (n[d] % kLanes != 0 || n[d] < kLanes || choose_seg(n[d]) == 0) return ST_E_UNSUPPORTED;
     st_ctx *c = new (std::nothrow) st_ctx();
     if (!c) return ST_E_NOMEM;
     c->p = *p;
     c->dev = p->device;
     c->dm.n[0] = p->nx; c->dm.n[1] = p->ny; c->dm.n[2] = p->nz;
     c->dm.n3 = (size_t)p->nx * p->ny * p->nz;
+    for (int d = 0; d < 3; d++) c->seg[d] = choose_seg(n[d]);
     auto bail = [&](int code, const char *m) { c->err = m; st_destroy(c); return code; };
     if (cudaSetDevice(c->dev) != cudaSuccess) return bail(ST_E_CUDA, "cudaSetDevice");
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)

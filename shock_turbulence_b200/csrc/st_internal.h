@@ -14,33 +14,39 @@
 
 namespace st {
 
-constexpr int kSeg = 32;          // segments per line = lanes of a warp
-constexpr int kScanSteps = 5;     // log2(kSeg)
-constexpr int kMaxS = 16;         // max points per lane (N <= 512)
+constexpr int kMaxSeg = 32;       // max segments per line (warps per CTA)
+constexpr int kLanes = 32;        // lines per CTA (lanes of a warp)
+
+// A line of n rows is split into P = n/S segments of S rows; warp s of a CTA
+// owns segment s of 32 neighbouring lines (lane = line).  Supported S.
+int choose_seg(int n);
 
 // Row tables of a constant-coefficient tridiagonal system, factorised as the
 // reference's tridiagonal_serial does (src/tridiagonal.f90:264-287), plus the
-// per-segment carry coefficients of the segmented solve.
+// carry tables of the segmented solve.
 struct TriTab {
     const double *l;    // forward multiplier of row i (row 0: 0)
     const double *g;    // response of the forward value of row i to the carry-in
     const double *up;   // upper diagonal c_i
     const double *id;   // 1 / (b'_i + tiny)   (last row: 1 / b'_n)
     const double *h;    // response of x_i to the carry from the right
-    const double *bk;   // [kSeg][kScanSteps] running products, forward scan
-    const double *gk;   // [kSeg][kScanSteps] running products, reverse scan
+    const double *wf;   // [P][P]: carry into segment s = sum_{s'<s} wf[s'][s] * A_{s'}
+    const double *wb;   // [P][P]: carry into segment s = sum_{s'>s} wb[s'][s] * B_{s'}
+    int kf, kb;         // segments back/ahead whose carry weight is >= 1e-20
 };
 
 // Same for the pentadiagonal systems of the compact filter
-// (pentadiagonal_serial, src/pentadiagonal.f90:319-374).
+// (pentadiagonal_serial, src/pentadiagonal.f90:319-374); carries are
+// 2-vectors and the carry tables hold 2x2 matrices.
 struct PenTab {
     const double *p1, *p2;   // forward multipliers of r'_{i-1}, r'_{i-2}
     const double *g1, *g2;   // forward carry responses (carry = (r'_{a-1}, r'_{a-2}))
     const double *q1, *q2;   // back-substitution coefficients of x_{i+1}, x_{i+2}
     const double *id;        // 1 / (C'_i + tiny)
     const double *h1, *h2;   // backward carry responses (carry = (x_{b+1}, x_{b+2}))
-    const double *mk;        // [kSeg][kScanSteps][4] forward scan 2x2 products
-    const double *nk;        // [kSeg][kScanSteps][4] reverse scan 2x2 products
+    const double *mf;        // [P][P][4]
+    const double *mb;        // [P][P][4]
+    int kf, kb;              // segments back/ahead whose carry weight is >= 1e-20
 };
 
 enum TriKind { K_D1S = 0, K_D1A = 1, K_D2S = 2, K_D2A = 3 };
@@ -68,6 +74,7 @@ struct Dims {
 struct st_ctx {
     st_params p;
     st::Dims dm;
+    int seg[3];        // rows per segment along x, y, z
     int dev = 0;
     cudaStream_t stream = nullptr;
     std::string err;

@@ -5,13 +5,11 @@
 
 namespace st {
 
-constexpr int kW = 4;   // lines (warps) per CTA
-
 struct LineArgs {
     const double *F;
     double *O1, *O2;
-    LineMap m;
-    size_t nlines;
+    LineGeo geo;
+    int S, P;
     double fac1, fac2;
     int asym, iadd;
     TriTab t1, t2;
@@ -19,114 +17,144 @@ struct LineArgs {
     Consts K;
 };
 
-// DF*_sym/_asym: O1 (=|+=) cadd * dF/ds
-template <int S>
-__global__ void __launch_bounds__(kW * 32) k_dfd(LineArgs a) {
-    __shared__ double sm[kW * LineGeom<S>::kStride];
-    const size_t L0 = (size_t)blockIdx.x * kW;
-    tile_load<S, kW>(sm, a.F, a.m, L0);
-    __syncthreads();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *line = sm + w * LineGeom<S>::kStride;
-    double r[S];
-    rhs_d1<S>(r, line, lane, a.m.n, a.asym, a.fac1, a.K);
-    tri_solve<S>(r, a.t1, lane);
-    __syncwarp();
-    seg_to_line<S>(line, lane, r);
-    __syncthreads();
-    tile_store<S, kW>(sm, a.O1, a.m, L0, a.iadd);
-}
+// Every line kernel is instantiated for x/z lines (YT = false: direct
+// coalesced row accesses) and for y lines (YT = true: staged through a
+// shared [32][n+1] tile).
+#define LINE_PROLOGUE                                                                  \
+    __shared__ CarryBuf cb;                                                            \
+    extern __shared__ double tile[];                                                   \
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5, n = a.geo.n, row0 = s * S; \
+    const ColMap m = a.geo.map(blockIdx.x);                                            \
+    const RowReader rd = YT ? RowReader{tile + lane * (n + 1), 1}                      \
+                            : RowReader{a.F + m.base + (size_t)lane * m.lstride, m.rstride};
 
-// D2F*2_sym/_asym: O2 = d2F/ds2; if iadd, O1 = dF/ds (cadd = 1)
-template <int S>
-__global__ void __launch_bounds__(kW * 32) k_d2fd2(LineArgs a) {
-    __shared__ double sm[kW * LineGeom<S>::kStride];
-    const size_t L0 = (size_t)blockIdx.x * kW;
-    tile_load<S, kW>(sm, a.F, a.m, L0);
-    __syncthreads();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *line = sm + w * LineGeom<S>::kStride;
-    double r2[S], r1[S];
-    rhs_d2<S>(r2, line, lane, a.m.n, a.asym, a.fac2, a.K);
-    if (a.iadd) rhs_d1<S>(r1, line, lane, a.m.n, a.asym, a.fac1, a.K);
-    tri_solve<S>(r2, a.t2, lane);
-    if (a.iadd) tri_solve<S>(r1, a.t1, lane);
-    __syncwarp();
-    seg_to_line<S>(line, lane, r2);
-    __syncthreads();
-    tile_store<S, kW>(sm, a.O2, a.m, L0, 0);
-    if (a.iadd) {
+template <int S, int H, bool YT>
+__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const double *F,
+                                         const ColMap &m, int lane, int a, int n) {
+    if (YT) ytile_rows<S, H>(v, tile, lane, a, n);
+    else load_rows<S, H>(v, F, m, lane, a, n);
+}
+template <int S, bool YT, int N>
+__device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, double *O, const ColMap &m,
+                                         int lane, int a, int n, int add) {
+    if (YT) {
+        __syncthreads();                 // every thread has finished reading the tile
+        ytile_put<S>(tile, v, lane, a, n);
         __syncthreads();
-        seg_to_line<S>(line, lane, r1);
-        __syncthreads();
-        tile_store<S, kW>(sm, a.O1, a.m, L0, 0);
+        ytile_store(tile, O, m.base, n, add);
+    } else {
+        store_rows<S>(v, O, m, lane, a, add);
     }
 }
 
-// Compact_Filter_*_sym/_asym: O1 = filtered F (O1 may alias F)
-template <int S>
-__global__ void __launch_bounds__(kW * 32) k_filter(LineArgs a) {
-    __shared__ double sm[kW * LineGeom<S>::kStride];
-    const size_t L0 = (size_t)blockIdx.x * kW;
-    tile_load<S, kW>(sm, a.F, a.m, L0);
-    __syncthreads();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *line = sm + w * LineGeom<S>::kStride;
-    double r[S];
-    rhs_filter<S>(r, line, lane, a.m.n, a.asym, a.K);
-    pen_solve<S>(r, a.p, lane);
-    __syncwarp();
-    seg_to_line<S>(line, lane, r);
-    __syncthreads();
-    tile_store<S, kW>(sm, a.O1, a.m, L0, 0);
+// DF*_sym/_asym: O1 (=|+=) cadd * dF/ds
+template <int S, bool YT>
+__global__ void __launch_bounds__(1024) k_dfd(LineArgs a) {
+    LINE_PROLOGUE
+    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 4];
+    get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+    rhs_d1<S, 2>(v, row0, n, a.asym, a.fac1, a.K, rd);
+    tri_solve<S>(v, a.t1, s, a.P, lane, cb);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd);
 }
 
-// Gaussian_Filter_X/Y/Z: O1 = explicit 9-point Gaussian of F
-template <int S>
-__global__ void __launch_bounds__(kW * 32) k_gauss(LineArgs a) {
-    __shared__ double sm[kW * LineGeom<S>::kStride];
-    const size_t L0 = (size_t)blockIdx.x * kW;
-    tile_load<S, kW>(sm, a.F, a.m, L0);
-    __syncthreads();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *line = sm + w * LineGeom<S>::kStride;
-    double r[S];
-    rhs_gauss<S>(r, line, lane, a.m.n, a.K);
-    __syncthreads();
-    seg_to_line<S>(line, lane, r);
-    __syncthreads();
-    tile_store<S, kW>(sm, a.O1, a.m, L0, 0);
+// D2F*2_sym/_asym: O2 = d2F/ds2; if iadd, O1 = dF/ds (cadd = 1).  The first
+// derivative re-reads the rows (the CTA's lines are still in L2).
+template <int S, bool YT>
+__global__ void __launch_bounds__(1024) k_d2fd2(LineArgs a) {
+    LINE_PROLOGUE
+    {
+        if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+        double v[S + 4];
+        get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+        rhs_d2<S, 2>(v, row0, n, a.asym, a.fac2, a.K, rd);
+        tri_solve<S>(v, a.t2, s, a.P, lane, cb);
+        put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0);
+    }
+    if (a.iadd) {
+        __syncthreads();   // carry buffers and tile are reused
+        if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+        double v[S + 4];
+        get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+        rhs_d1<S, 2>(v, row0, n, a.asym, a.fac1, a.K, rd);
+        tri_solve<S>(v, a.t1, s, a.P, lane, cb);
+        put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+    }
+}
+
+// Compact_Filter_*_sym/_asym: O1 = filtered F.  O1 may alias F: every read of
+// F (including the boundary re-reads) happens before the solve's first
+// barrier and every write after its last one.
+template <int S, bool YT>
+__global__ void __launch_bounds__(1024) k_filter(LineArgs a) {
+    LINE_PROLOGUE
+    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 8];
+    get_rows<S, 4, YT>(v, tile, a.F, m, lane, row0, n);
+    rhs_filter<S, 4>(v, row0, n, a.asym, a.K, rd);
+    pen_solve<S>(v, a.p, s, a.P, lane, cb);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+}
+
+// Gaussian_Filter_X/Y/Z: O1 = explicit 9-point Gaussian of F (O1 != F)
+template <int S, bool YT>
+__global__ void __launch_bounds__(1024) k_gauss(LineArgs a) {
+    LINE_PROLOGUE
+    (void)cb;
+    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 8];
+    get_rows<S, 4, YT>(v, tile, a.F, m, lane, row0, n);
+    rhs_gauss<S, 4>(v, row0, n, a.K, rd);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
 }
 
 enum OpKind { OP_D1, OP_D2, OP_FILTER, OP_GAUSS };
 
-template <int S>
-static void launch_S(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t s) {
-    dim3 grid((unsigned)(a.nlines / kW)), block(kW * 32);
+// opt in to the dynamic shared memory a kernel needs on top of its static
+// carry buffers (the default cap is 48 KB in total); once per kernel and size
+template <auto Kern>
+static void set_smem(size_t bytes) {
+    static size_t done = 0;   // one counter per kernel instantiation
+    if (bytes > done) {
+        cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        done = bytes;
+    }
+}
+
+template <int S, bool YT>
+static void launch_SY(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
+    const size_t nlines = c->dm.n3 / (size_t)a.geo.n;
+    dim3 grid((unsigned)(nlines / kLanes)), block(kLanes * a.P);
+    const size_t smem = YT ? (size_t)kLanes * (a.geo.n + 1) * sizeof(double) : 0;
     // algorithmic bytes: every input and output field touched once
-    const double n3 = (double)a.nlines * a.m.n;
+    const double n3 = (double)c->dm.n3;
     double b = 16.0;
     if (op == OP_D1 && a.iadd) b = 24.0;
     if (op == OP_D2 && a.iadd) b = 24.0;
     static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
     int pi = prof_start(c, names[op], b * n3);
     switch (op) {
-        case OP_D1: k_dfd<S><<<grid, block, 0, s>>>(a); break;
-        case OP_D2: k_d2fd2<S><<<grid, block, 0, s>>>(a); break;
-        case OP_FILTER: k_filter<S><<<grid, block, 0, s>>>(a); break;
-        case OP_GAUSS: k_gauss<S><<<grid, block, 0, s>>>(a); break;
+        case OP_D1: set_smem<k_dfd<S, YT>>(smem); k_dfd<S, YT><<<grid, block, smem, st>>>(a); break;
+        case OP_D2: set_smem<k_d2fd2<S, YT>>(smem); k_d2fd2<S, YT><<<grid, block, smem, st>>>(a); break;
+        case OP_FILTER: set_smem<k_filter<S, YT>>(smem); k_filter<S, YT><<<grid, block, smem, st>>>(a); break;
+        case OP_GAUSS: set_smem<k_gauss<S, YT>>(smem); k_gauss<S, YT><<<grid, block, smem, st>>>(a); break;
     }
     prof_stop(c, pi);
 }
 
+template <int S>
+static void launch_S(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
+    if (a.geo.dir == 1) launch_SY<S, true>(c, op, a, st);
+    else launch_SY<S, false>(c, op, a, st);
+}
+
 static int launch_line(st_ctx *c, OpKind op, const LineArgs &a) {
-    const int S = a.m.n / kSeg;
-    switch (S) {
+    switch (a.S) {
 #define CASE(s_) case s_: launch_S<s_>(c, op, a, c->stream); break;
-        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
-        CASE(9) CASE(10) CASE(11) CASE(12) CASE(13) CASE(14) CASE(15) CASE(16)
+        CASE(2) CASE(3) CASE(4) CASE(6) CASE(8) CASE(12) CASE(16)
 #undef CASE
-        default: return fail(c, ST_E_UNSUPPORTED, "line length must be 32*S with 1<=S<=16");
+        default: return fail(c, ST_E_UNSUPPORTED, "unsupported line segmentation");
     }
     ST_CUDA(c, cudaGetLastError());
     return ST_OK;
@@ -134,11 +162,12 @@ static int launch_line(st_ctx *c, OpKind op, const LineArgs &a) {
 
 static LineArgs make_args(st_ctx *c, int dir) {
     LineArgs a{};
-    a.m.dir = dir;
-    a.m.n = c->dm.n[dir];
-    a.m.My = c->dm.n[1];
-    a.m.Mz = c->dm.n[2];
-    a.nlines = c->dm.n3 / (size_t)a.m.n;
+    a.geo.dir = dir;
+    a.geo.n = c->dm.n[dir];
+    a.geo.My = c->dm.n[1];
+    a.geo.Mz = c->dm.n[2];
+    a.S = c->seg[dir];
+    a.P = a.geo.n / a.S;
     a.K = c->k;
     return a;
 }
@@ -146,7 +175,7 @@ static LineArgs make_args(st_ctx *c, int dir) {
 int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
     LineArgs a = make_args(c, dir);
     a.F = F; a.O1 = dF; a.asym = asym; a.iadd = iadd;
-    a.fac1 = cadd * c->s1[dir] * (double)(a.m.n - 1);           // src/derivCDopt6_sym_tri.f:424
+    a.fac1 = cadd * c->s1[dir] * (double)(a.geo.n - 1);           // src/derivCDopt6_sym_tri.f:424
     a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
     return launch_line(c, OP_D1, a);
 }
@@ -154,8 +183,8 @@ int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd,
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
     LineArgs a = make_args(c, dir);
     a.F = F; a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;
-    a.fac1 = 1.0 * c->s1[dir] * (double)(a.m.n - 1);
-    a.fac2 = ((double)((a.m.n - 1) * (a.m.n - 1))) * c->s2[dir];   // src/derivCDopt6_sym_tri.f:554
+    a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
+    a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];   // src/derivCDopt6_sym_tri.f:554
     a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
     a.t2 = c->tri[dir][asym ? K_D2A : K_D2S];
     return launch_line(c, OP_D2, a);

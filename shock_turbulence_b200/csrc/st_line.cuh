@@ -1,67 +1,102 @@
 // st_line.cuh - device building blocks of the line operators.
 //
-// Work decomposition: one warp owns one grid line of n = 32*S points; lane s
-// owns the contiguous rows [s*S, s*S+S) in registers.  Lines are staged in
-// shared memory with one padding double after every segment, so that the 32
-// lanes reading "their" row t hit 32 different banks (row stride S+1).
+// Work decomposition ("columns"): a CTA owns 32 neighbouring lines of one
+// direction; lane l of every warp works on line l and warp s on the rows
+// [s*S, s*S+S) of those lines, held in registers.  Consequences:
+//  - for x and z lines the 32 lanes touch 32 adjacent doubles of every row,
+//    so every global access is one coalesced 256-byte transaction;
+//  - all lanes of a warp are on the same row, so the LU-table reads are
+//    warp-uniform (one broadcast);
+//  - boundary rows belong to the first and last warp only (no divergence);
+//  - segments exchange their end values through shared memory once per
+//    recurrence direction; the carry into each segment is a fixed linear
+//    combination of those values (tables wf/wb, mf/mb).
 #pragma once
 #include "st_internal.h"
 
 namespace st {
 
-constexpr unsigned kFull = 0xffffffffu;
-
-// shared-memory geometry of one staged line
-template <int S>
-struct LineGeom {
-    static constexpr int kPadL = 8 * (S + 1);          // room for out-of-line stencil reads
-    static constexpr int kBody = kSeg * (S + 1);
-    static constexpr int kStride = kPadL + kBody + 8 * (S + 1) + 1;   // odd stride
-    __device__ static int pos(int row) { return kPadL + (row / S) * (S + 1) + (row % S); }
+// element (lane, row) of a CTA's 32 lines is base + lane*lstride + row*rstride
+struct ColMap {
+    size_t base, lstride, rstride;
+};
+struct LineGeo {
+    int dir, n, My, Mz;
+    __device__ __forceinline__ ColMap map(unsigned blk) const {
+        ColMap m;
+        const size_t sMy = My, sMz = Mz, jb = My / kLanes;
+        if (dir == 0) {            // lines (j,k): 32 consecutive j at one k
+            m.base = (blk % jb) * kLanes + sMy * (blk / jb); m.lstride = 1; m.rstride = sMy * sMz;
+        } else if (dir == 1) {     // lines (k,i): 32 consecutive lines, each contiguous
+            m.base = sMy * (size_t)blk * kLanes; m.lstride = sMy; m.rstride = 1;
+        } else {                   // lines (j,i): 32 consecutive j at one i
+            m.base = (blk % jb) * kLanes + sMy * sMz * (blk / jb); m.lstride = 1; m.rstride = sMy;
+        }
+        return m;
+    }
 };
 
-// value of row (lane*S + u) of a staged line; u is a compile-time constant
-// after unrolling, so the segment jump folds to a constant offset.
-template <int S>
-__device__ __forceinline__ double ldrow(const double *line, int lane, int u) {
-    const int q = (u >= 0) ? u / S : -((-u + S - 1) / S);
-    const int off = u - q * S;
-    return line[LineGeom<S>::kPadL + (lane + q) * (S + 1) + off];
+// rows a-H .. a+S+H-1 of this lane's line into v (rows clamped into the
+// line; clamped values are never used by the stencils)
+template <int S, int H>
+__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const double *__restrict__ F,
+                                          const ColMap &m, int lane, int a, int n) {
+    const double *p = F + m.base + (size_t)lane * m.lstride;
+#pragma unroll
+    for (int q = 0; q < S + 2 * H; q++) {
+        int row = a - H + q;
+        row = row < 0 ? 0 : (row > n - 1 ? n - 1 : row);
+        v[q] = __ldg(p + (size_t)row * m.rstride);
+    }
 }
+
+template <int S, int N>
+__device__ __forceinline__ void store_rows(const double (&r)[N], double *__restrict__ O, const ColMap &m,
+                                           int lane, int a, int add) {
+    double *p = O + m.base + (size_t)lane * m.lstride + (size_t)a * m.rstride;
+    if (add) {
+        double prev[S];
+#pragma unroll
+        for (int t = 0; t < S; t++) prev[t] = p[(size_t)t * m.rstride];
+#pragma unroll
+        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = prev[t] + r[t];
+    } else {
+#pragma unroll
+        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = r[t];
+    }
+}
+
+// shared buffers for the segment end values of one solve
+struct CarryBuf {
+    double a[kMaxSeg][kLanes][2];
+    double b[kMaxSeg][kLanes][2];
+};
 
 // ---- segmented constant-coefficient tridiagonal solve --------------------
 // Forward elimination r'_i = r_i - l_i r'_{i-1} and back substitution
 // x_i = (r'_i - c_i x_{i+1}) / (b'_i + tiny) of tridiagonal_serial
-// (src/tridiagonal.f90:274-284), run per segment with zero carries, then
-// corrected by the carries that a warp scan of the segment maps produces.
-template <int S>
-__device__ __forceinline__ void tri_solve(double (&r)[S], const TriTab &T, int lane) {
-    const int a = lane * S;
+// (src/tridiagonal.f90:274-284) per segment with zero carries, then the
+// carry corrections.  Caller guarantees cb is free (synchronised).
+template <int S, int N>
+__device__ __forceinline__ void tri_solve(double (&r)[N], const TriTab &T, int s, int P, int lane,
+                                          CarryBuf &cb) {
+    const int a = s * S;
 #pragma unroll
     for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * __ldg(T.l + a + t);
-    double A = r[S - 1];
-#pragma unroll
-    for (int k = 0; k < kScanSteps; k++) {
-        const int off = 1 << k;
-        double o = __shfl_up_sync(kFull, A, off);
-        if (lane >= off) A = fma(__ldg(T.bk + lane * kScanSteps + k), o, A);
-    }
-    double cin = __shfl_up_sync(kFull, A, 1);
-    if (lane == 0) cin = 0.0;
+    cb.a[s][lane][0] = r[S - 1];
+    __syncthreads();
+    double cin = 0.0;
+    for (int sp = max(0, s - T.kf); sp < s; sp++) cin = fma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g + a + t), cin, r[t]);
     r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
 #pragma unroll
     for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
-    double F = r[0];
-#pragma unroll
-    for (int k = 0; k < kScanSteps; k++) {
-        const int off = 1 << k;
-        double o = __shfl_down_sync(kFull, F, off);
-        if (lane + off < kSeg) F = fma(__ldg(T.gk + lane * kScanSteps + k), o, F);
-    }
-    double ein = __shfl_down_sync(kFull, F, 1);
-    if (lane == kSeg - 1) ein = 0.0;
+    cb.b[s][lane][0] = r[0];
+    __syncthreads();
+    double ein = 0.0;
+    for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
+        ein = fma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.h + a + t), ein, r[t]);
 }
@@ -70,31 +105,27 @@ __device__ __forceinline__ void tri_solve(double (&r)[S], const TriTab &T, int l
 // Elimination order of pentadiagonal_serial (src/pentadiagonal.f90:340-372):
 // r'_i = (r_i - k2 r'_{i-2}) - k1 r'_{i-1};  x_i = ((r'_i - D'_i x_{i+1})
 // - E_i x_{i+2}) / (C'_i + tiny).  Carries are 2-vectors.
-template <int S>
-__device__ __forceinline__ void pen_solve(double (&r)[S], const PenTab &T, int lane) {
-    const int a = lane * S;
+template <int S, int N>
+__device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s, int P, int lane,
+                                          CarryBuf &cb) {
+    const int a = s * S;
 #pragma unroll
     for (int t = 1; t < S; t++) {
         double v = r[t];
-        if (t >= 2) v = v - __ldg(T.p2 + a + t) * r[t - 2];
+        if (t >= 2) v = v - __ldg(T.p2 + a + t) * r[t >= 2 ? t - 2 : 0];
         v = v - __ldg(T.p1 + a + t) * r[t - 1];
         r[t] = v;
     }
-    double A1 = r[S - 1], A2 = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
-#pragma unroll
-    for (int k = 0; k < kScanSteps; k++) {
-        const int off = 1 << k;
-        double o1 = __shfl_up_sync(kFull, A1, off);
-        double o2 = __shfl_up_sync(kFull, A2, off);
-        if (lane >= off) {
-            const double *m = T.mk + (lane * kScanSteps + k) * 4;
-            double n1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, A1));
-            double n2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, A2));
-            A1 = n1; A2 = n2;
-        }
+    cb.a[s][lane][0] = r[S - 1];
+    cb.a[s][lane][1] = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
+    __syncthreads();
+    double c1 = 0.0, c2 = 0.0;
+    for (int sp = max(0, s - T.kf); sp < s; sp++) {
+        const double *m = T.mf + ((size_t)sp * P + s) * 4;
+        double a1 = cb.a[sp][lane][0], a2 = cb.a[sp][lane][1];
+        c1 = fma(__ldg(m + 0), a1, fma(__ldg(m + 1), a2, c1));
+        c2 = fma(__ldg(m + 2), a1, fma(__ldg(m + 3), a2, c2));
     }
-    double c1 = __shfl_up_sync(kFull, A1, 1), c2 = __shfl_up_sync(kFull, A2, 1);
-    if (lane == 0) { c1 = 0.0; c2 = 0.0; }
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g1 + a + t), c1, fma(__ldg(T.g2 + a + t), c2, r[t]));
 #pragma unroll
@@ -104,86 +135,147 @@ __device__ __forceinline__ void pen_solve(double (&r)[S], const PenTab &T, int l
         if (t + 2 < S) v = v - __ldg(T.q2 + a + t) * r[t + 2 < S ? t + 2 : t];
         r[t] = v * __ldg(T.id + a + t);
     }
-    double B1 = r[0], B2 = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
-#pragma unroll
-    for (int k = 0; k < kScanSteps; k++) {
-        const int off = 1 << k;
-        double o1 = __shfl_down_sync(kFull, B1, off);
-        double o2 = __shfl_down_sync(kFull, B2, off);
-        if (lane + off < kSeg) {
-            const double *m = T.nk + (lane * kScanSteps + k) * 4;
-            double n1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, B1));
-            double n2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, B2));
-            B1 = n1; B2 = n2;
-        }
+    cb.b[s][lane][0] = r[0];
+    cb.b[s][lane][1] = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
+    __syncthreads();
+    double e1 = 0.0, e2 = 0.0;
+    for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++) {
+        const double *m = T.mb + ((size_t)sp * P + s) * 4;
+        double b1 = cb.b[sp][lane][0], b2 = cb.b[sp][lane][1];
+        e1 = fma(__ldg(m + 0), b1, fma(__ldg(m + 1), b2, e1));
+        e2 = fma(__ldg(m + 2), b1, fma(__ldg(m + 3), b2, e2));
     }
-    double e1 = __shfl_down_sync(kFull, B1, 1), e2 = __shfl_down_sync(kFull, B2, 1);
-    if (lane == kSeg - 1) { e1 = 0.0; e2 = 0.0; }
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.h1 + a + t), e1, fma(__ldg(T.h2 + a + t), e2, r[t]));
 }
 
 // ---- explicit right-hand sides ------------------------------------------
-// Rows follow the reference formulas term by term (Fortran evaluates
-// left to right); f(k) is the value k rows away from row i.
+// v holds rows a-H .. a+S+H-1 on entry; the RHS of row a+t is written into
+// v[t] (in place, ascending t: row a+t only needs v[t..t+2H]).  Rows follow
+// the reference formulas term by term (Fortran evaluates left to right).
+// Boundary rows belong to the first/last segment only: those warps re-read
+// the few rows they need from global memory (warp-uniform branch).
+struct RowReader {
+    const double *p;          // global or shared memory
+    size_t rstride;
+    __device__ __forceinline__ double operator()(int row) const { return p[(size_t)row * rstride]; }
+};
+
+// ---- y lines: staging through shared memory ------------------------------
+// The 32 lines of a y CTA are one contiguous block of 32*n doubles.  They
+// are copied with 16-byte coalesced accesses into a [32][n+1] tile (odd
+// stride: lane l reading row r of line l hits bank (l*(n+1)+r) mod 32, all
+// distinct), so that each thread reads its segment conflict-free.
+__device__ __forceinline__ void ytile_load(double *tile, const double *__restrict__ F, size_t base, int n) {
+    const double2 *src = reinterpret_cast<const double2 *>(F + base);
+    const int half = kLanes * n / 2;
+    for (int q = threadIdx.x; q < half; q += blockDim.x) {
+        double2 d = __ldg(src + q);
+        int e = 2 * q, line = e / n, row = e - line * n;
+        tile[line * (n + 1) + row] = d.x;
+        tile[line * (n + 1) + row + 1] = d.y;
+    }
+}
+__device__ __forceinline__ void ytile_store(const double *tile, double *__restrict__ O, size_t base, int n,
+                                            int add) {
+    double2 *dst = reinterpret_cast<double2 *>(O + base);
+    const int half = kLanes * n / 2;
+    for (int q = threadIdx.x; q < half; q += blockDim.x) {
+        int e = 2 * q, line = e / n, row = e - line * n;
+        double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
+        if (add) {
+            double2 o = dst[q];
+            d.x = o.x + d.x;
+            d.y = o.y + d.y;
+        }
+        dst[q] = d;
+    }
+}
+template <int S, int H>
+__device__ __forceinline__ void ytile_rows(double (&v)[S + 2 * H], const double *tile, int lane, int a, int n) {
+    const double *p = tile + lane * (n + 1);
+#pragma unroll
+    for (int q = 0; q < S + 2 * H; q++) {
+        int row = a - H + q;
+        row = row < 0 ? 0 : (row > n - 1 ? n - 1 : row);
+        v[q] = p[row];
+    }
+}
+template <int S, int N>
+__device__ __forceinline__ void ytile_put(double *tile, const double (&r)[N], int lane, int a, int n) {
+    double *p = tile + lane * (n + 1) + a;
+#pragma unroll
+    for (int t = 0; t < S; t++) p[t] = r[t];
+}
 
 // DFDX_sym/_asym RHS, src/derivCDopt6_sym_tri.f:458-514,
-// src/derivCDopt6_asym_tri.f:461-516
-template <int S>
-__device__ __forceinline__ void rhs_d1(double (&r)[S], const double *line, int lane, int n, int asym,
-                                       double fac, const Consts &K) {
+// src/derivCDopt6_asym_tri.f:461-516  (H = 2)
+template <int S, int H>
+__device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
+                                       const Consts &K, const RowReader &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
-        auto f = [&](int k) { return ldrow<S>(line, lane, t + k); };
-        const int i = lane * S + t;
-        double w = fac * (K.b1 * (f(2) - f(-2)) + K.a1 * (f(1) - f(-1)));
-        if (i < 2 || i >= n - 2) {
-            if (i == 0) w = asym ? fac * (K.b1 * (f(2) + f(2)) + K.a1 * (f(1) + f(1))) : 0.0;
-            else if (i == 1) w = asym ? fac * (K.b1 * (f(2) + f(0)) + K.a1 * (f(1) - f(-1)))
-                                      : fac * (K.b1 * (f(2) - f(0)) + K.a1 * (f(1) - f(-1)));
+        auto f = [&](int k) { return v[t + k + H]; };
+        v[t] = fac * (K.b1 * (f(2) - f(-2)) + K.a1 * (f(1) - f(-1)));
+    }
+    if (a < 2 || a + S > n - 2) {
+#pragma unroll
+        for (int t = 0; t < S; t++) {
+            const int i = a + t;
+            auto f = [&](int k) { return F(i + k); };
+            if (i == 0) v[t] = asym ? fac * (K.b1 * (f(2) + f(2)) + K.a1 * (f(1) + f(1))) : 0.0;
+            else if (i == 1) v[t] = asym ? fac * (K.b1 * (f(2) + f(0)) + K.a1 * (f(1) - f(-1)))
+                                         : fac * (K.b1 * (f(2) - f(0)) + K.a1 * (f(1) - f(-1)));
             else if (i == n - 2)
-                w = fac * (K.closure1 * f(1) + 5.0e-1 * f(0) - f(-1) - K.closure2 * f(-2));
-            else w = fac * (2.5 * f(0) - 2.0 * f(-1) - 5.0e-1 * f(-2));
+                v[t] = fac * (K.closure1 * f(1) + 5.0e-1 * f(0) - f(-1) - K.closure2 * f(-2));
+            else if (i == n - 1) v[t] = fac * (2.5 * f(0) - 2.0 * f(-1) - 5.0e-1 * f(-2));
         }
-        r[t] = w;
     }
 }
 
 // D2FDX2_sym/_asym RHS, src/derivCDopt6_sym_tri.f:587-645,
-// src/derivCDopt6_asym_tri.f:588-643
-template <int S>
-__device__ __forceinline__ void rhs_d2(double (&r)[S], const double *line, int lane, int n, int asym,
-                                       double fac, const Consts &K) {
+// src/derivCDopt6_asym_tri.f:588-643  (H = 2)
+template <int S, int H>
+__device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
+                                       const Consts &K, const RowReader &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
-        auto f = [&](int k) { return ldrow<S>(line, lane, t + k); };
-        const int i = lane * S + t;
-        double w = fac * (K.b2 * (f(2) + f(-2)) + K.a2 * (f(1) + f(-1)) - K.c2 * f(0));
-        if (i < 2 || i >= n - 2) {
-            if (i == 0) w = asym ? 0.0 : fac * (K.b2 * 2.0 * (f(2) - f(0)) + K.a2 * 2.0 * (f(1) - f(0)));
+        auto f = [&](int k) { return v[t + k + H]; };
+        v[t] = fac * (K.b2 * (f(2) + f(-2)) + K.a2 * (f(1) + f(-1)) - K.c2 * f(0));
+    }
+    if (a < 2 || a + S > n - 2) {
+#pragma unroll
+        for (int t = 0; t < S; t++) {
+            const int i = a + t;
+            auto f = [&](int k) { return F(i + k); };
+            if (i == 0) v[t] = asym ? 0.0 : fac * (K.b2 * 2.0 * (f(2) - f(0)) + K.a2 * 2.0 * (f(1) - f(0)));
             else if (i == 1)
-                w = asym ? fac * (K.b2 * (f(2) - 3.0 * f(0)) + K.a2 * (f(1) - 2.0 * f(0)))
-                         : fac * (K.b2 * (f(2) - 2.0 * f(0) + f(0)) + K.a2 * (f(1) - 2.0 * f(0) + f(-1)));
+                v[t] = asym ? fac * (K.b2 * (f(2) - 3.0 * f(0)) + K.a2 * (f(1) - 2.0 * f(0)))
+                            : fac * (K.b2 * (f(2) - 2.0 * f(0) + f(0)) + K.a2 * (f(1) - 2.0 * f(0) + f(-1)));
             else if (i == n - 2)
-                w = fac * (1.2375 * f(1) - 3.0 * f(0) + 2.325 * f(-1) - 6.0e-1 * f(-2) + 3.75e-2 * f(-3));
-            else w = fac * (1.3e1 * f(0) - 2.7e1 * f(-1) + 1.5e1 * f(-2) - f(-3));
+                v[t] = fac * (1.2375 * f(1) - 3.0 * f(0) + 2.325 * f(-1) - 6.0e-1 * f(-2) + 3.75e-2 * f(-3));
+            else if (i == n - 1) v[t] = fac * (1.3e1 * f(0) - 2.7e1 * f(-1) + 1.5e1 * f(-2) - f(-3));
         }
-        r[t] = w;
     }
 }
 
 // Compact_Filter_X_sym/_asym RHS, src/filters_sym.f:483-616,
-// src/filters_asym.f:435-565
-template <int S>
-__device__ __forceinline__ void rhs_filter(double (&r)[S], const double *line, int lane, int n, int asym,
-                                           const Consts &K) {
+// src/filters_asym.f:435-565  (H = 4)
+template <int S, int H>
+__device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n, int asym, const Consts &K,
+                                           const RowReader &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
-        auto f = [&](int k) { return ldrow<S>(line, lane, t + k); };
-        const int i = lane * S + t;
-        double w = K.fa4 * (f(4) + f(-4)) + K.fa3 * (f(3) + f(-3)) + K.fa2 * (f(2) + f(-2)) +
-                   K.fa1 * (f(1) + f(-1)) + K.fa0 * f(0);
-        if (i < 4 || i >= n - 4) {
+        auto f = [&](int k) { return v[t + k + H]; };
+        v[t] = K.fa4 * (f(4) + f(-4)) + K.fa3 * (f(3) + f(-3)) + K.fa2 * (f(2) + f(-2)) +
+               K.fa1 * (f(1) + f(-1)) + K.fa0 * f(0);
+    }
+    if (a < 4 || a + S > n - 4) {
+#pragma unroll
+        for (int t = 0; t < S; t++) {
+            const int i = a + t;
+            auto f = [&](int k) { return F(i + k); };
+            double w = v[t];
             if (!asym) {
                 if (i == 0) w = K.fa4 * (2.0 * f(4)) + K.fa3 * (2.0 * f(3)) + K.fa2 * (2.0 * f(2)) +
                                 K.fa1 * (2.0 * f(1)) + K.fa0 * f(0);
@@ -210,87 +302,39 @@ __device__ __forceinline__ void rhs_filter(double (&r)[S], const double *line, i
                                      K.bc3[2] * f(2);
             else if (i == n - 4) w = K.bc4[3] * f(-3) + K.bc4[2] * f(-2) + K.bc4[1] * f(-1) + K.bc4[0] * f(0) +
                                      K.bc4[1] * f(1) + K.bc4[2] * f(2) + K.bc4[3] * f(3);
+            v[t] = w;
         }
-        r[t] = w;
     }
 }
 
 // Gaussian_Filter_X, src/filters_sym.f:1119-1212: explicit, symmetric low end,
-// last four points copied
-template <int S>
-__device__ __forceinline__ void rhs_gauss(double (&r)[S], const double *line, int lane, int n,
-                                          const Consts &K) {
+// last four points copied  (H = 4)
+template <int S, int H>
+__device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, const Consts &K,
+                                          const RowReader &F) {
     const double *g = K.ga;
 #pragma unroll
     for (int t = 0; t < S; t++) {
-        auto f = [&](int k) { return ldrow<S>(line, lane, t + k); };
-        const int i = lane * S + t;
-        double w = g[4] * (f(4) + f(-4)) + g[3] * (f(3) + f(-3)) + g[2] * (f(2) + f(-2)) +
-                   g[1] * (f(1) + f(-1)) + g[0] * f(0);
-        if (i < 4 || i >= n - 4) {
-            if (i == 0) w = g[4] * (2.0 * f(4)) + g[3] * (2.0 * f(3)) + g[2] * (2.0 * f(2)) +
-                            g[1] * (2.0 * f(1)) + g[0] * f(0);
-            else if (i == 1) w = g[4] * (f(2) + f(4)) + g[3] * (f(1) + f(3)) + g[2] * (f(0) + f(2)) +
-                                 g[1] * (f(-1) + f(1)) + g[0] * f(0);
-            else if (i == 2) w = g[4] * (f(0) + f(4)) + g[3] * (f(-1) + f(3)) + g[2] * (f(-2) + f(2)) +
-                                 g[1] * (f(-1) + f(1)) + g[0] * f(0);
-            else if (i == 3) w = g[4] * (f(-2) + f(4)) + g[3] * (f(-3) + f(3)) + g[2] * (f(-2) + f(2)) +
-                                 g[1] * (f(-1) + f(1)) + g[0] * f(0);
-            if (i >= n - 4) w = f(0);
-        }
-        r[t] = w;
+        auto f = [&](int k) { return v[t + k + H]; };
+        v[t] = g[4] * (f(4) + f(-4)) + g[3] * (f(3) + f(-3)) + g[2] * (f(2) + f(-2)) + g[1] * (f(1) + f(-1)) +
+               g[0] * f(0);
     }
-}
-
-// ---- line tiles -----------------------------------------------------------
-// A CTA of W warps stages W lines of direction d.  Lines are numbered so
-// that W consecutive lines are W consecutive addresses (x, z) or W
-// consecutive contiguous lines (y):
-//   x: L = j + My*k,  element (L,i) at L + My*Mz*i
-//   y: L = k + Mz*i,  element (L,j) at My*L + j
-//   z: L = j + My*i,  element (L,k) at (L%My) + My*Mz*(L/My) + My*k
-struct LineMap {
-    int dir, n, My, Mz;
-    __device__ __forceinline__ size_t addr(size_t L, int row) const {
-        if (dir == 0) return L + (size_t)My * Mz * row;
-        if (dir == 1) return (size_t)My * L + row;
-        return (L % My) + (size_t)My * Mz * (L / My) + (size_t)My * row;
-    }
-};
-
-// cooperative coalesced load of W lines into padded shared memory
-template <int S, int W>
-__device__ __forceinline__ void tile_load(double *sm, const double *__restrict__ F, const LineMap &m,
-                                          size_t L0) {
-    const int n = kSeg * S;
-    for (int idx = threadIdx.x; idx < W * n; idx += blockDim.x) {
-        int w, row;
-        if (m.dir == 1) { w = idx / n; row = idx - w * n; }
-        else { row = idx / W; w = idx - row * W; }
-        sm[w * LineGeom<S>::kStride + LineGeom<S>::pos(row)] = __ldg(F + m.addr(L0 + w, row));
-    }
-}
-
-// cooperative store (mode 0: out = v, 1: out += v)
-template <int S, int W>
-__device__ __forceinline__ void tile_store(const double *sm, double *__restrict__ O, const LineMap &m,
-                                           size_t L0, int add) {
-    const int n = kSeg * S;
-    for (int idx = threadIdx.x; idx < W * n; idx += blockDim.x) {
-        int w, row;
-        if (m.dir == 1) { w = idx / n; row = idx - w * n; }
-        else { row = idx / W; w = idx - row * W; }
-        size_t g = m.addr(L0 + w, row);
-        double v = sm[w * LineGeom<S>::kStride + LineGeom<S>::pos(row)];
-        O[g] = add ? O[g] + v : v;
-    }
-}
-
-// write a lane's segment back into its staged line
-template <int S>
-__device__ __forceinline__ void seg_to_line(double *line, int lane, const double (&r)[S]) {
+    if (a < 4 || a + S > n - 4) {
 #pragma unroll
-    for (int t = 0; t < S; t++) line[LineGeom<S>::kPadL + lane * (S + 1) + t] = r[t];
+        for (int t = 0; t < S; t++) {
+            const int i = a + t;
+            auto f = [&](int k) { return F(i + k); };
+            if (i == 0) v[t] = g[4] * (2.0 * f(4)) + g[3] * (2.0 * f(3)) + g[2] * (2.0 * f(2)) +
+                               g[1] * (2.0 * f(1)) + g[0] * f(0);
+            else if (i == 1) v[t] = g[4] * (f(2) + f(4)) + g[3] * (f(1) + f(3)) + g[2] * (f(0) + f(2)) +
+                                    g[1] * (f(-1) + f(1)) + g[0] * f(0);
+            else if (i == 2) v[t] = g[4] * (f(0) + f(4)) + g[3] * (f(-1) + f(3)) + g[2] * (f(-2) + f(2)) +
+                                    g[1] * (f(-1) + f(1)) + g[0] * f(0);
+            else if (i == 3) v[t] = g[4] * (f(-2) + f(4)) + g[3] * (f(-3) + f(3)) + g[2] * (f(-2) + f(2)) +
+                                    g[1] * (f(-1) + f(1)) + g[0] * f(0);
+            if (i >= n - 4) v[t] = f(0);
+        }
+    }
 }
 
 }  // namespace st

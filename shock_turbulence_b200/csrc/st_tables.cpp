@@ -8,11 +8,13 @@
 // (direction, scheme, boundary kind) computed with the reference's own
 // operation order gives the same pivots and multipliers.
 //
-// The segmented solve splits each line into kSeg contiguous segments of
-// S = n/kSeg rows.  Each segment runs the Thomas recurrences with a zero
-// carry; the true carries are then obtained by an affine scan over the
-// segments (tables bk/gk, mk/nk) and added back through the per-row carry
-// responses (g, h).  In exact arithmetic this is the Thomas algorithm.
+// The segmented solve splits each line into P contiguous segments of S rows.
+// Each segment runs the Thomas recurrences with a zero carry; the true carry
+// into segment s is a linear combination of the end values of the segments
+// before it (forward) or after it (backward), with the constant weights
+// wf/wb (mf/mb for 2-vector carries), and it is added back through the
+// per-row carry responses (g, h).  In exact arithmetic this is the Thomas
+// algorithm.
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -21,6 +23,13 @@
 namespace st {
 
 static const double kTiny = (double)FLT_MIN;   // tiny(1.0), src/tridiagonal.f90:275
+
+int choose_seg(int n) {
+    static const int sup[] = {2, 3, 4, 6, 8, 12, 16};
+    for (int S : sup)
+        if (n % S == 0 && n / S <= kMaxSeg) return S;
+    return 0;
+}
 
 void fill_consts(Consts &k) {
     // FDL3DI sixth-order compact tridiagonal set, src/header:191-204
@@ -94,14 +103,34 @@ static void filter_lhs(int n, int asym, std::vector<double> M[5]) {
 
 // ---- tables ---------------------------------------------------------------
 struct TriHost {
-    std::vector<double> l, g, up, id, h, bk, gk;
+    std::vector<double> l, g, up, id, h, wf, wb;
+    int kf = 0, kb = 0;
 };
 struct PenHost {
-    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mk, nk;
+    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mf, mb;
+    int kf = 0, kb = 0;
 };
 
+// Carry weights decay geometrically with the distance between segments.
+// Contributions with weight below 1e-20 cannot change an FP64 result of the
+// size of the solution, so the device loops stop at the farthest segment
+// whose weight (max norm of the 2x2 block for pentadiagonal carries) is at
+// least that large.
+static int carry_span(const std::vector<double> &w, int P, int blk, bool fwd) {
+    int span = 0;
+    for (int s = 0; s < P; s++)
+        for (int sp = 0; sp < P; sp++) {
+            int dist = fwd ? s - sp : sp - s;
+            if (dist <= 0) continue;
+            double m = 0.0;
+            for (int q = 0; q < blk; q++) m = std::fmax(m, std::fabs(w[((size_t)sp * P + s) * blk + q]));
+            if (m >= 1e-20 && dist > span) span = dist;
+        }
+    return span;
+}
+
 static TriHost tri_tables(const std::vector<double> &a, const std::vector<double> &b,
-                          const std::vector<double> &c, int n) {
+                          const std::vector<double> &c, int n, int S) {
     TriHost t;
     std::vector<double> bp(n);
     t.l.assign(n, 0.0);
@@ -114,10 +143,10 @@ static TriHost tri_tables(const std::vector<double> &a, const std::vector<double
     t.id.resize(n);
     for (int i = 0; i < n - 1; i++) t.id[i] = 1.0 / (bp[i] + kTiny);
     t.id[n - 1] = 1.0 / bp[n - 1];
-    const int S = n / kSeg;
+    const int P = n / S;
     t.g.assign(n, 0.0); t.h.assign(n, 0.0);
-    std::vector<double> B(kSeg), G(kSeg);
-    for (int s = 0; s < kSeg; s++) {
+    std::vector<double> B(P), G(P);
+    for (int s = 0; s < P; s++) {
         int a0 = s * S;
         double pr = 1.0;
         for (int q = 0; q < S; q++) { pr *= -t.l[a0 + q]; t.g[a0 + q] = pr; }
@@ -126,22 +155,16 @@ static TriHost tri_tables(const std::vector<double> &a, const std::vector<double
         for (int q = S - 1; q >= 0; q--) { pr *= -(t.up[a0 + q] * t.id[a0 + q]); t.h[a0 + q] = pr; }
         G[s] = t.h[a0];
     }
-    // running products seen by each lane at each Hillis-Steele step
-    t.bk.assign(kSeg * kScanSteps, 0.0); t.gk.assign(kSeg * kScanSteps, 0.0);
-    std::vector<double> cur = B, nxt(kSeg);
-    for (int k = 0; k < kScanSteps; k++) {
-        int off = 1 << k;
-        for (int s = 0; s < kSeg; s++) t.bk[s * kScanSteps + k] = cur[s];
-        for (int s = 0; s < kSeg; s++) nxt[s] = s >= off ? cur[s] * cur[s - off] : cur[s];
-        cur = nxt;
+    // carry weights: C_s = sum_{s'<s} (prod_{u=s'+1}^{s-1} B_u) A_{s'}
+    t.wf.assign((size_t)P * P, 0.0); t.wb.assign((size_t)P * P, 0.0);
+    for (int s = 0; s < P; s++) {
+        double w = 1.0;
+        for (int sp = s - 1; sp >= 0; sp--) { t.wf[(size_t)sp * P + s] = w; w *= B[sp]; }
+        w = 1.0;
+        for (int sp = s + 1; sp < P; sp++) { t.wb[(size_t)sp * P + s] = w; w *= G[sp]; }
     }
-    cur = G;
-    for (int k = 0; k < kScanSteps; k++) {
-        int off = 1 << k;
-        for (int s = 0; s < kSeg; s++) t.gk[s * kScanSteps + k] = cur[s];
-        for (int s = 0; s < kSeg; s++) nxt[s] = s + off < kSeg ? cur[s] * cur[s + off] : cur[s];
-        cur = nxt;
-    }
+    t.kf = carry_span(t.wf, P, 1, true);
+    t.kb = carry_span(t.wb, P, 1, false);
     return t;
 }
 
@@ -151,7 +174,7 @@ static void mat2mul(const double *A, const double *B, double *C) {  // C = A*B (
     std::memcpy(C, r, sizeof(r));
 }
 
-static PenHost pen_tables(std::vector<double> M[5], int n) {
+static PenHost pen_tables(std::vector<double> M[5], int n, int S) {
     PenHost t;
     std::vector<double> A = M[0], B = M[1], C = M[2], D = M[3], E = M[4];
     std::vector<double> k1(n, 0.0), k2(n, 0.0);
@@ -173,10 +196,10 @@ static PenHost pen_tables(std::vector<double> M[5], int n) {
     for (int i = 0; i <= n - 2; i++) t.q1[i] = D[i];
     for (int i = 0; i <= n - 3; i++) t.q2[i] = E[i];
     for (int i = 0; i < n; i++) t.id[i] = 1.0 / (C[i] + kTiny);
-    const int S = n / kSeg;
+    const int P = n / S;
     t.g1.assign(n, 0.0); t.g2.assign(n, 0.0); t.h1.assign(n, 0.0); t.h2.assign(n, 0.0);
-    std::vector<double> Mseg(kSeg * 4), Nseg(kSeg * 4);
-    for (int s = 0; s < kSeg; s++) {
+    std::vector<double> Mseg(P * 4), Nseg(P * 4);
+    for (int s = 0; s < P; s++) {
         int a0 = s * S;
         for (int which = 0; which < 2; which++) {
             // forward homogeneous response to (r'_{a-1}, r'_{a-2}) = e_which
@@ -206,27 +229,22 @@ static PenHost pen_tables(std::vector<double> M[5], int n) {
             nn[0] = t.h1[a0]; nn[1] = t.h2[a0]; nn[2] = 1.0; nn[3] = 0.0;
         }
     }
-    t.mk.assign(kSeg * kScanSteps * 4, 0.0); t.nk.assign(kSeg * kScanSteps * 4, 0.0);
-    std::vector<double> cur = Mseg, nxt(kSeg * 4);
-    for (int k = 0; k < kScanSteps; k++) {
-        int off = 1 << k;
-        for (int s = 0; s < kSeg; s++) std::memcpy(&t.mk[(s * kScanSteps + k) * 4], &cur[s * 4], 32);
-        for (int s = 0; s < kSeg; s++) {
-            if (s >= off) mat2mul(&cur[s * 4], &cur[(s - off) * 4], &nxt[s * 4]);
-            else std::memcpy(&nxt[s * 4], &cur[s * 4], 32);
+    // carry weights: C_s = sum_{s'<s} (M_{s-1} ... M_{s'+1}) A_{s'} (2x2 products)
+    t.mf.assign((size_t)P * P * 4, 0.0); t.mb.assign((size_t)P * P * 4, 0.0);
+    for (int s = 0; s < P; s++) {
+        double w[4] = {1.0, 0.0, 0.0, 1.0};
+        for (int sp = s - 1; sp >= 0; sp--) {
+            std::memcpy(&t.mf[((size_t)sp * P + s) * 4], w, 32);
+            mat2mul(w, &Mseg[sp * 4], w);
         }
-        cur = nxt;
-    }
-    cur = Nseg;
-    for (int k = 0; k < kScanSteps; k++) {
-        int off = 1 << k;
-        for (int s = 0; s < kSeg; s++) std::memcpy(&t.nk[(s * kScanSteps + k) * 4], &cur[s * 4], 32);
-        for (int s = 0; s < kSeg; s++) {
-            if (s + off < kSeg) mat2mul(&cur[s * 4], &cur[(s + off) * 4], &nxt[s * 4]);
-            else std::memcpy(&nxt[s * 4], &cur[s * 4], 32);
+        double v[4] = {1.0, 0.0, 0.0, 1.0};
+        for (int sp = s + 1; sp < P; sp++) {
+            std::memcpy(&t.mb[((size_t)sp * P + s) * 4], v, 32);
+            mat2mul(v, &Nseg[sp * 4], v);
         }
-        cur = nxt;
     }
+    t.kf = carry_span(t.mf, P, 4, true);
+    t.kb = carry_span(t.mb, P, 4, false);
     return t;
 }
 
@@ -246,22 +264,24 @@ int build_tables(st_ctx *c) {
         for (int kind = 0; kind < 4; kind++) {
             std::vector<double> a, b, cc;
             deriv_lhs(n, kind < 2 ? 1 : 2, kind & 1, a, b, cc);
-            TriHost h = tri_tables(a, b, cc, n);
+            TriHost h = tri_tables(a, b, cc, n, c->seg[d]);
             TriTab &t = c->tri[d][kind];
             t.l = upload(c, h.l, &err); t.g = upload(c, h.g, &err); t.up = upload(c, h.up, &err);
             t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
-            t.bk = upload(c, h.bk, &err); t.gk = upload(c, h.gk, &err);
+            t.wf = upload(c, h.wf, &err); t.wb = upload(c, h.wb, &err);
+            t.kf = h.kf; t.kb = h.kb;
         }
         for (int kind = 0; kind < 2; kind++) {
             std::vector<double> M[5];
             filter_lhs(n, kind, M);
-            PenHost h = pen_tables(M, n);
+            PenHost h = pen_tables(M, n, c->seg[d]);
             PenTab &t = c->pen[d][kind];
             t.p1 = upload(c, h.p1, &err); t.p2 = upload(c, h.p2, &err);
             t.g1 = upload(c, h.g1, &err); t.g2 = upload(c, h.g2, &err);
             t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
-            t.mk = upload(c, h.mk, &err); t.nk = upload(c, h.nk, &err);
+            t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
+            t.kf = h.kf; t.kb = h.kb;
         }
     }
     if (err) return fail(c, ST_E_NOMEM, "could not allocate or upload the LU tables");
