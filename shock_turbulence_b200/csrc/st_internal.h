@@ -60,6 +60,23 @@ struct Consts {
     double ga[5];                          // Gaussian coefficients (float32 values)
 };
 
+// Pointwise expression that a line kernel evaluates while loading its rows
+// (so that a flux need not be stored before it is differentiated).  The
+// operand order of each form matches the reference statement it replaces.
+enum ProdOp {
+    PR_A = 0,        // a
+    PR_MUL,          // a*b
+    PR_ADDMUL,       // (a+b)*c
+    PR_MULMUL,       // c*(a*b)
+    PR_SPEC,         // a*b*c + a*c*k0*k1             (Species_RHS flux)
+    PR_SPECT,        // (k0*d)*(a*b*c + a*c*k0b*k1)    (its energy counterpart)
+};
+struct Prod {
+    int op;
+    const double *a, *b, *c, *d;
+    double k0, k1, k2;
+};
+
 enum { G_DUX_DX, G_DUY_DX, G_DUZ_DX, G_DUX_DY, G_DUY_DY, G_DUZ_DY,
        G_DUX_DZ, G_DUY_DZ, G_DUZ_DZ, G_DTDX, G_DTDY, G_DTDZ };
 enum { H_BETA, H_VISC, H_K, H_D };
@@ -154,6 +171,7 @@ struct Scratch {                                 // RAII helper
 
 // line operators on device arrays (st_kernels.cu)
 int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd);
+int dev_dfd_prod(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int iadd, double cadd);
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd);
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0);
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg);

@@ -6,7 +6,7 @@
 namespace st {
 
 struct LineArgs {
-    const double *F;
+    Prod F;
     double *O1, *O2;
     LineGeo geo;
     int S, P;
@@ -25,14 +25,14 @@ struct LineArgs {
     extern __shared__ double tile[];                                                   \
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5, n = a.geo.n, row0 = s * S; \
     const ColMap m = a.geo.map(blockIdx.x);                                            \
-    const RowReader rd = YT ? RowReader{tile + lane * (n + 1), 1}                      \
-                            : RowReader{a.F + m.base + (size_t)lane * m.lstride, m.rstride};
+    const RowReader<OP> rd = YT ? RowReader<OP>{tile + lane * (n + 1), nullptr, 0, 0}  \
+                                : RowReader<OP>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
 
-template <int S, int H, bool YT>
-__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const double *F,
+template <int S, int H, bool YT, int OP>
+__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const Prod &F,
                                          const ColMap &m, int lane, int a, int n) {
     if (YT) ytile_rows<S, H>(v, tile, lane, a, n);
-    else load_rows<S, H>(v, F, m, lane, a, n);
+    else load_rows<S, H, OP>(v, F, m, lane, a, n);
 }
 template <int S, bool YT, int N>
 __device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, double *O, const ColMap &m,
@@ -48,12 +48,12 @@ __device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, dou
 }
 
 // DF*_sym/_asym: O1 (=|+=) cadd * dF/ds
-template <int S, bool YT>
+template <int S, bool YT, int OP>
 __global__ void __launch_bounds__(1024) k_dfd(LineArgs a) {
     LINE_PROLOGUE
-    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
     double v[S + 4];
-    get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+    get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n);
     rhs_d1<S, 2>(v, row0, n, a.asym, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
     put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd);
@@ -63,20 +63,21 @@ __global__ void __launch_bounds__(1024) k_dfd(LineArgs a) {
 // derivative re-reads the rows (the CTA's lines are still in L2).
 template <int S, bool YT>
 __global__ void __launch_bounds__(1024) k_d2fd2(LineArgs a) {
+    constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
-        if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
         double v[S + 4];
-        get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+        get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n);
         rhs_d2<S, 2>(v, row0, n, a.asym, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
         put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0);
     }
     if (a.iadd) {
         __syncthreads();   // carry buffers and tile are reused
-        if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
         double v[S + 4];
-        get_rows<S, 2, YT>(v, tile, a.F, m, lane, row0, n);
+        get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n);
         rhs_d1<S, 2>(v, row0, n, a.asym, a.fac1, a.K, rd);
         tri_solve<S>(v, a.t1, s, a.P, lane, cb);
         put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
@@ -88,10 +89,11 @@ __global__ void __launch_bounds__(1024) k_d2fd2(LineArgs a) {
 // barrier and every write after its last one.
 template <int S, bool YT>
 __global__ void __launch_bounds__(1024) k_filter(LineArgs a) {
+    constexpr int OP = PR_A;
     LINE_PROLOGUE
-    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
     double v[S + 8];
-    get_rows<S, 4, YT>(v, tile, a.F, m, lane, row0, n);
+    get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n);
     rhs_filter<S, 4>(v, row0, n, a.asym, a.K, rd);
     pen_solve<S>(v, a.p, s, a.P, lane, cb);
     put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
@@ -100,11 +102,12 @@ __global__ void __launch_bounds__(1024) k_filter(LineArgs a) {
 // Gaussian_Filter_X/Y/Z: O1 = explicit 9-point Gaussian of F (O1 != F)
 template <int S, bool YT>
 __global__ void __launch_bounds__(1024) k_gauss(LineArgs a) {
+    constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;
-    if (YT) { ytile_load(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
     double v[S + 8];
-    get_rows<S, 4, YT>(v, tile, a.F, m, lane, row0, n);
+    get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n);
     rhs_gauss<S, 4>(v, row0, n, a.K, rd);
     put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
 }
@@ -129,13 +132,21 @@ static void launch_SY(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) 
     const size_t smem = YT ? (size_t)kLanes * (a.geo.n + 1) * sizeof(double) : 0;
     // algorithmic bytes: every input and output field touched once
     const double n3 = (double)c->dm.n3;
-    double b = 16.0;
-    if (op == OP_D1 && a.iadd) b = 24.0;
-    if (op == OP_D2 && a.iadd) b = 24.0;
+    // inputs: 1 field, or every field a producer expression reads
+    static const int nin[6] = {1, 2, 3, 3, 3, 4};
+    double b = 8.0 * nin[a.F.op] + 8.0;          // + one output
+    if (op == OP_D1 && a.iadd) b += 8.0;           // read-modify-write
+    if (op == OP_D2 && a.iadd) b += 8.0;           // second output
     static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
     int pi = prof_start(c, names[op], b * n3);
     switch (op) {
-        case OP_D1: set_smem<k_dfd<S, YT>>(smem); k_dfd<S, YT><<<grid, block, smem, st>>>(a); break;
+        case OP_D1:
+            switch (a.F.op) {
+#define PCASE(o_) case o_: set_smem<k_dfd<S, YT, o_>>(smem); k_dfd<S, YT, o_><<<grid, block, smem, st>>>(a); break;
+                PCASE(PR_A) PCASE(PR_MUL) PCASE(PR_ADDMUL) PCASE(PR_MULMUL) PCASE(PR_SPEC) PCASE(PR_SPECT)
+#undef PCASE
+            }
+            break;
         case OP_D2: set_smem<k_d2fd2<S, YT>>(smem); k_d2fd2<S, YT><<<grid, block, smem, st>>>(a); break;
         case OP_FILTER: set_smem<k_filter<S, YT>>(smem); k_filter<S, YT><<<grid, block, smem, st>>>(a); break;
         case OP_GAUSS: set_smem<k_gauss<S, YT>>(smem); k_gauss<S, YT><<<grid, block, smem, st>>>(a); break;
@@ -172,7 +183,18 @@ static LineArgs make_args(st_ctx *c, int dir) {
     return a;
 }
 
+static Prod plain(const double *F) {
+    Prod p{};
+    p.op = PR_A;
+    p.a = F;
+    return p;
+}
+
 int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
+    return dev_dfd_prod(c, dir, asym, plain(F), dF, iadd, cadd);
+}
+
+int dev_dfd_prod(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int iadd, double cadd) {
     LineArgs a = make_args(c, dir);
     a.F = F; a.O1 = dF; a.asym = asym; a.iadd = iadd;
     a.fac1 = cadd * c->s1[dir] * (double)(a.geo.n - 1);           // src/derivCDopt6_sym_tri.f:424
@@ -182,7 +204,7 @@ int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd,
 
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
     LineArgs a = make_args(c, dir);
-    a.F = F; a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;
+    a.F = plain(F); a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;
     a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
     a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];   // src/derivCDopt6_sym_tri.f:554
     a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
@@ -192,14 +214,14 @@ int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double 
 
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
     LineArgs a = make_args(c, dir);
-    a.F = F; a.O1 = F0; a.asym = asym;
+    a.F = plain(F); a.O1 = F0; a.asym = asym;
     a.p = c->pen[dir][asym ? K_FA : K_FS];
     return launch_line(c, OP_FILTER, a);
 }
 
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg) {
     LineArgs a = make_args(c, dir);
-    a.F = F; a.O1 = Fg;
+    a.F = plain(F); a.O1 = Fg;
     return launch_line(c, OP_GAUSS, a);
 }
 

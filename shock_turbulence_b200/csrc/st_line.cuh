@@ -36,17 +36,37 @@ struct LineGeo {
     }
 };
 
+template <int OP>
+__device__ __forceinline__ double prod_eval(const Prod &P, size_t i) {
+    if constexpr (OP == PR_MUL) {
+        return __ldg(P.a + i) * __ldg(P.b + i);
+    } else if constexpr (OP == PR_ADDMUL) {
+        return (__ldg(P.a + i) + __ldg(P.b + i)) * __ldg(P.c + i);
+    } else if constexpr (OP == PR_MULMUL) {
+        return __ldg(P.c + i) * (__ldg(P.a + i) * __ldg(P.b + i));
+    } else if constexpr (OP == PR_SPEC) {
+        double a = __ldg(P.a + i), b = __ldg(P.b + i), c = __ldg(P.c + i);
+        return a * b * c + a * c * P.k0 * P.k1;
+    } else if constexpr (OP == PR_SPECT) {
+        double a = __ldg(P.a + i), b = __ldg(P.b + i), c = __ldg(P.c + i), d = __ldg(P.d + i);
+        double fl = a * b * c + a * c * P.k0 * P.k1;
+        return P.k2 * d * fl;
+    } else {
+        return __ldg(P.a + i);
+    }
+}
+
 // rows a-H .. a+S+H-1 of this lane's line into v (rows clamped into the
 // line; clamped values are never used by the stencils)
-template <int S, int H>
-__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const double *__restrict__ F,
-                                          const ColMap &m, int lane, int a, int n) {
-    const double *p = F + m.base + (size_t)lane * m.lstride;
+template <int S, int H, int OP>
+__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const Prod &F, const ColMap &m, int lane,
+                                          int a, int n) {
+    const size_t p = m.base + (size_t)lane * m.lstride;
 #pragma unroll
     for (int q = 0; q < S + 2 * H; q++) {
         int row = a - H + q;
         row = row < 0 ? 0 : (row > n - 1 ? n - 1 : row);
-        v[q] = __ldg(p + (size_t)row * m.rstride);
+        v[q] = prod_eval<OP>(F, p + (size_t)row * m.rstride);
     }
 }
 
@@ -155,10 +175,14 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
 // the reference formulas term by term (Fortran evaluates left to right).
 // Boundary rows belong to the first/last segment only: those warps re-read
 // the few rows they need from global memory (warp-uniform branch).
+template <int OP>
 struct RowReader {
-    const double *p;          // global or shared memory
-    size_t rstride;
-    __device__ __forceinline__ double operator()(int row) const { return p[(size_t)row * rstride]; }
+    const double *tile;       // shared tile row (y lines) or null
+    const Prod *F;            // global producer (x, z lines)
+    size_t base, rstride;
+    __device__ __forceinline__ double operator()(int row) const {
+        return tile ? tile[row] : prod_eval<OP>(*F, base + (size_t)row * rstride);
+    }
 };
 
 // ---- y lines: staging through shared memory ------------------------------
@@ -166,18 +190,34 @@ struct RowReader {
 // are copied with 16-byte coalesced accesses into a [32][n+1] tile (odd
 // stride: lane l reading row r of line l hits bank (l*(n+1)+r) mod 32, all
 // distinct), so that each thread reads its segment conflict-free.
-__device__ __forceinline__ void ytile_load(double *tile, const double *__restrict__ F, size_t base, int n) {
-    const double2 *src = reinterpret_cast<const double2 *>(F + base);
+template <int OP>
+__device__ __forceinline__ void ytile_load(double *tile, const Prod &F, size_t base, int n) {
     const int half = kLanes * n / 2;
-    for (int q = threadIdx.x; q < half; q += blockDim.x) {
-        double2 d = __ldg(src + q);
-        int e = 2 * q, line = e / n, row = e - line * n;
-        tile[line * (n + 1) + row] = d.x;
-        tile[line * (n + 1) + row + 1] = d.y;
+    if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
+        const double2 *src = reinterpret_cast<const double2 *>(F.a + base);
+        for (int q = threadIdx.x; q < half; q += blockDim.x) {
+            double2 d = __ldg(src + q);
+            int e = 2 * q, line = e / n, row = e - line * n;
+            tile[line * (n + 1) + row] = d.x;
+            tile[line * (n + 1) + row + 1] = d.y;
+        }
+    } else {
+        for (int q = threadIdx.x; q < 2 * half; q += blockDim.x) {
+            int line = q / n, row = q - line * n;
+            tile[line * (n + 1) + row] = prod_eval<OP>(F, base + q);
+        }
     }
 }
 __device__ __forceinline__ void ytile_store(const double *tile, double *__restrict__ O, size_t base, int n,
                                             int add) {
+    if (reinterpret_cast<uintptr_t>(O + base) & 15) {
+        for (int q = threadIdx.x; q < kLanes * n; q += blockDim.x) {
+            int line = q / n, row = q - line * n;
+            double v = tile[line * (n + 1) + row];
+            O[base + q] = add ? O[base + q] + v : v;
+        }
+        return;
+    }
     double2 *dst = reinterpret_cast<double2 *>(O + base);
     const int half = kLanes * n / 2;
     for (int q = threadIdx.x; q < half; q += blockDim.x) {
@@ -210,9 +250,9 @@ __device__ __forceinline__ void ytile_put(double *tile, const double (&r)[N], in
 
 // DFDX_sym/_asym RHS, src/derivCDopt6_sym_tri.f:458-514,
 // src/derivCDopt6_asym_tri.f:461-516  (H = 2)
-template <int S, int H>
+template <int S, int H, class RD>
 __device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
-                                       const Consts &K, const RowReader &F) {
+                                       const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
@@ -235,9 +275,9 @@ __device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int
 
 // D2FDX2_sym/_asym RHS, src/derivCDopt6_sym_tri.f:587-645,
 // src/derivCDopt6_asym_tri.f:588-643  (H = 2)
-template <int S, int H>
+template <int S, int H, class RD>
 __device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
-                                       const Consts &K, const RowReader &F) {
+                                       const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
@@ -261,9 +301,9 @@ __device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int
 
 // Compact_Filter_X_sym/_asym RHS, src/filters_sym.f:483-616,
 // src/filters_asym.f:435-565  (H = 4)
-template <int S, int H>
+template <int S, int H, class RD>
 __device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n, int asym, const Consts &K,
-                                           const RowReader &F) {
+                                           const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
@@ -309,9 +349,9 @@ __device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n,
 
 // Gaussian_Filter_X, src/filters_sym.f:1119-1212: explicit, symmetric low end,
 // last four points copied  (H = 4)
-template <int S, int H>
+template <int S, int H, class RD>
 __device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, const Consts &K,
-                                          const RowReader &F) {
+                                          const RD &F) {
     const double *g = K.ga;
 #pragma unroll
     for (int t = 0; t < S; t++) {

@@ -18,8 +18,7 @@ __global__ void k_pfor(size_t n, Fn fn) {
 }
 template <class Fn>
 static int pfor(st_ctx *c, size_t n, Fn fn) {
-    size_t blocks = (n + 255) / 256;
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    size_t blocks = (n + 255) / 256;    // one element per thread
     if (blocks == 0) return ST_OK;
     int pi = prof_start(c, "k_pointwise", 0.0);
     k_pfor<<<(unsigned)blocks, 256, 0, c->stream>>>(n, fn);
@@ -28,6 +27,15 @@ static int pfor(st_ctx *c, size_t n, Fn fn) {
     return ST_OK;
 }
 #define PFOR(c, n, ...) ST_TRY(pfor((c), (n), [=] __device__(size_t p) __VA_ARGS__))
+
+// producer expressions evaluated by the derivative kernels while loading
+static Prod pr_mul(const double *a, const double *b) { Prod p{}; p.op = PR_MUL; p.a = a; p.b = b; return p; }
+static Prod pr_addmul(const double *a, const double *b, const double *c) {
+    Prod p{}; p.op = PR_ADDMUL; p.a = a; p.b = b; p.c = c; return p;
+}
+static Prod pr_mulmul(const double *a, const double *b, const double *c) {
+    Prod p{}; p.op = PR_MULMUL; p.a = a; p.b = b; p.c = c; return p;
+}
 
 struct Phys {
     double g1, g2, eps, vis_exp, Re1_inv, Re2_inv, Pr_inv, Sc_inv, bulk;
@@ -81,261 +89,230 @@ int dev_compute_gamma(st_ctx *c, const double *Y) {
     return ST_OK;
 }
 
-// ---- RHS_x (src/rhsv_sym_mf.f:37-481); Q is the copy Ux --------------------
-static int rhs_x(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Qcx, double *Qcy, double *Qcz,
-                 double *Qv) {
+// ---- RHS (src/rhsv_sym_mf.f:9-1428) ------------------------------------------
+// The reference runs RHS_x on a copy Ux of Q and hands Ux to RHS_yz holding
+// du/dx, dv/dx, dw/dx, dT/dx and mu.  Here those quantities live in the
+// /GRAD/ arrays and in named scratch fields, with these exact rewrites:
+//  - accumulators (Qrhs, Qconvx/y/z, Qvisc) are assigned by their first
+//    contribution instead of being zeroed first (0 + x == x);
+//  - the /GRAD/ copies are written in place by the derivative kernels;
+//  - quantities RHS_yz recomputes with the same expression from the same
+//    inputs (Vs, P, T, u, v, w, mu, dmu/dT) are computed once;
+//  - d(rho)/dy (src/rhsv_sym_mf.f:953), which the reference overwrites before
+//    any use, is not computed;
+//  - when the molecular viscous term is not added (Re <= 0, the reference
+//    build, src/rhsv_sym_mf.f:1420-1424) the Qvisc work, whose only consumer
+//    is that sum, is skipped; the /GRAD/ first derivatives are still formed.
+int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     const size_t n3 = c->dm.n3;
-    Phys f = phys(c);
+    const Phys f = phys(c);
+    const bool visc = c->p.re > 0.0;
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    Scratch P(c), Vs(c), T(c), FF(c), Flux(c), dF(c);
-    double *pP = P, *pVs = Vs, *pT = T, *pFF = FF, *pFl = Flux, *pdF = dF;
-    ST_CUDA(c, cudaMemsetAsync(Qrhs, 0, 5 * n3 * 8, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(Qcx, 0, 5 * n3 * 8, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(Qcy, 0, 5 * n3 * 8, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(Qcz, 0, 5 * n3 * 8, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(Qv, 0, 5 * n3 * 8, c->stream));
+    double *Gxx = c->grad[G_DUX_DX], *Gyx = c->grad[G_DUY_DX], *Gzx = c->grad[G_DUZ_DX];
+    double *Gxy = c->grad[G_DUX_DY], *Gyy = c->grad[G_DUY_DY], *Gzy = c->grad[G_DUZ_DY];
+    double *Gxz = c->grad[G_DUX_DZ], *Gyz = c->grad[G_DUY_DZ], *Gzz = c->grad[G_DUZ_DZ];
+    double *GTx = c->grad[G_DTDX], *GTy = c->grad[G_DTDY], *GTz = c->grad[G_DTDZ];
+    Scratch sQcx(c, 5), sQcy(c, 5), sQcz(c, 5), sQv(c, 5);
+    double *Qcx = sQcx, *Qcy = sQcy, *Qcz = sQcz, *Qv = sQv;
+    ScratchN s(c, 17);
+    double *Vs = s[0], *P = s[1], *T = s[2], *u = s[3], *v = s[4], *w = s[5], *mu = s[6], *dmu = s[7];
+    double *Flux = s[8], *FF = s[9], *dF = s[10], *dFz = s[11], *U4 = s[12], *U5 = s[13], *Tdy = s[14];
+    double *Tdz = s[15], *T2 = s[16];
     const double *g = c->gamma_eff;
-    PFOR(c, n3, {
-        thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], pVs[p], pP[p], pT[p]);
-        pdF[p] = Q1[p] * pVs[p];
-        pFF[p] = pdF[p];
-        pFl[p] = Q4[p] * pFF[p];
-    });
-    ST_TRY(dev_dfd(c, 0, 1, pFl, Qcx + 3 * n3, 1, -1.0));
-    PFOR(c, n3, { pFl[p] = (Q5[p] + pP[p]) * pFF[p]; });
-    ST_TRY(dev_dfd(c, 0, 1, pFl, Qcx + 4 * n3, 1, -1.0));
-    PFOR(c, n3, { pFF[p] = pdF[p]; pFl[p] = Q1[p] * pFF[p]; });
-    ST_TRY(dev_dfd(c, 0, 0, pFl, Qcx, 1, -5.0e-1));
-    ST_TRY(dev_dfd(c, 0, 0, pP, Qcx, 1, -1.0));
-    PFOR(c, n3, { pFl[p] = Q2[p] * pFF[p]; });
-    ST_TRY(dev_dfd(c, 0, 1, pFl, Qcx + n3, 1, -5.0e-1));
-    PFOR(c, n3, { pFl[p] = Q3[p] * pFF[p]; });
-    ST_TRY(dev_dfd(c, 0, 1, pFl, Qcx + 2 * n3, 1, -5.0e-1));
-    ST_TRY(dev_dfd(c, 0, 1, Q1, pFF, 0, 1.0));
-    PFOR(c, n3, {
-        double mu, dmu;
-        Q1[p] = pdF[p];
-        Q2[p] = Q2[p] * pVs[p];
-        Q3[p] = Q3[p] * pVs[p];
-        viscosity(f, pT[p], Y[p], mu, dmu);
-        Q5[p] = mu;
-        pFl[p] = dmu;
-        double fac2 = -5.0e-1 * pFF[p];
-        Qcx[p] = Qcx[p] + fac2 * Q1[p];
-        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * Q2[p];
-        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * Q3[p];
-    });
-    ST_TRY(dev_d2fd2(c, 0, 0, pT, pFF, pdF, 1));
-    ST_CUDA(c, cudaMemcpyAsync(c->grad[G_DTDX], pFF, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    {
-        double fac1 = f.Pr_inv;
-        PFOR(c, n3, { Qv[4 * n3 + p] = Qv[4 * n3 + p] + fac1 * (Q5[p] * pdF[p] + pFl[p] * pFF[p] * pFF[p]); });
-    }
-    ST_TRY(dev_d2fd2(c, 0, 1, Q1, pFl, pdF, 1));
-    ST_CUDA(c, cudaMemcpyAsync(c->grad[G_DUX_DX], pFl, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    {
-        double fac1 = 4.0 / 3.0 + f.bulk;
-        PFOR(c, n3, {
-            double fac2 = fac1 * Q5[p] * pdF[p];
-            Qv[p] = Qv[p] + fac2;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q1[p] * fac2;
-        });
-    }
-    ST_TRY(dev_d2fd2(c, 0, 0, Q2, pT, pdF, 1));
-    ST_CUDA(c, cudaMemcpyAsync(c->grad[G_DUY_DX], pT, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    PFOR(c, n3, {
-        double fac2 = Q5[p] * pdF[p];
-        Qv[n3 + p] = Qv[n3 + p] + fac2;
-        Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q2[p] * fac2;
-        Q2[p] = pT[p];
-    });
-    ST_TRY(dev_d2fd2(c, 0, 0, Q3, pVs, pdF, 1));
-    ST_CUDA(c, cudaMemcpyAsync(c->grad[G_DUZ_DX], pVs, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    PFOR(c, n3, {
-        double fac2 = Q5[p] * pdF[p];
-        Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac2;
-        Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q3[p] * fac2;
-        Q3[p] = pVs[p];
-    });
-    PFOR(c, n3, {
-        double fac2 = -5.0e-1 * Q4[p] * Q1[p];
-        Q1[p] = pFl[p];
-        Q4[p] = pFF[p];
-        Qcx[p] = Qcx[p] + fac2 * Q1[p];
-        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * Q2[p];
-        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * Q3[p];
-    });
-    return ST_OK;
-}
 
-// ---- RHS_yz (src/rhsv_sym_mf.f:492-1428) ---------------------------------
-static int rhs_yz(st_ctx *c, double *Q, double *Ux, double *Qrhs, const double *Y, double *Qcx, double *Qcy,
-                  double *Qcz, double *Qv) {
-    const size_t n3 = c->dm.n3;
-    Phys f = phys(c);
-    double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    double *U1 = Ux, *U2 = Ux + n3, *U3 = Ux + 2 * n3, *U4 = Ux + 3 * n3, *U5 = Ux + 4 * n3;
-    ScratchN s(c, 12);
-    double *P = s[0], *Vs = s[1], *T = s[2], *vis = s[3], *dF = s[4], *Flux = s[5];
-    double *Tdy = s[6], *Tdz = s[7], *Udz = s[8], *dFz = s[9], *Udx = s[10], *Udy = s[11];
-    const double *g = c->gamma_eff;
-    double **G = c->grad;
+    // ---- RHS_x (src/rhsv_sym_mf.f:37-481)
     PFOR(c, n3, {
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs[p], P[p], T[p]);
-        U5[p] = Q2[p] * Vs[p];
-        Flux[p] = Q1[p] * U5[p];
+        u[p] = Q1[p] * Vs[p];
     });
-    ST_TRY(dev_dfd(c, 1, 1, Q2, dF, 0, 1.0));
-    PFOR(c, n3, { Qcy[3 * n3 + p] = Qcy[3 * n3 + p] - dF[p]; });
-    ST_TRY(dev_dfd(c, 1, 1, Flux, Qcy, 1, -5.0e-1));
-    PFOR(c, n3, { Flux[p] = Q2[p] * U5[p]; });
-    ST_TRY(dev_dfd(c, 1, 0, Flux, Qcy + n3, 1, -5.0e-1));
-    ST_TRY(dev_dfd(c, 1, 0, P, Qcy + n3, 1, -1.0));
-    PFOR(c, n3, { Flux[p] = Q3[p] * U5[p]; });
-    ST_TRY(dev_dfd(c, 1, 1, Flux, Qcy + 2 * n3, 1, -5.0e-1));
-    PFOR(c, n3, { Flux[p] = (Q5[p] + P[p]) * U5[p]; });
-    ST_TRY(dev_dfd(c, 1, 1, Flux, Qcy + 4 * n3, 1, -1.0));
-    ST_TRY(dev_dfd(c, 2, 1, Q3, dFz, 0, 1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q4, u), Qcx + 3 * n3, 0, -1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_addmul(Q5, P, u), Qcx + 4 * n3, 0, -1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 0, pr_mul(Q1, u), Qcx, 0, -5.0e-1));
+    ST_TRY(dev_dfd(c, 0, 0, P, Qcx, 1, -1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q2, u), Qcx + n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q3, u), Qcx + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd(c, 0, 1, Q1, FF, 0, 1.0));
     PFOR(c, n3, {
-        Qcz[3 * n3 + p] = Qcz[3 * n3 + p] - dFz[p];
-        U5[p] = Q3[p] * Vs[p];
-        Flux[p] = Q1[p] * U5[p];
+        double m, dm;
+        v[p] = Q2[p] * Vs[p];
+        w[p] = Q3[p] * Vs[p];
+        viscosity(f, T[p], Y[p], m, dm);
+        mu[p] = m;
+        dmu[p] = dm;
+        double fac2 = -5.0e-1 * FF[p];
+        Qcx[p] = Qcx[p] + fac2 * u[p];
+        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * v[p];
+        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * w[p];
     });
-    ST_TRY(dev_dfd(c, 2, 1, Flux, Qcz, 1, -5.0e-1));
-    PFOR(c, n3, { Flux[p] = Q2[p] * U5[p]; });
-    ST_TRY(dev_dfd(c, 2, 1, Flux, Qcz + n3, 1, -5.0e-1));
-    PFOR(c, n3, { Flux[p] = Q3[p] * U5[p]; });
-    ST_TRY(dev_dfd(c, 2, 0, Flux, Qcz + 2 * n3, 1, -5.0e-1));
-    ST_TRY(dev_dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
-    PFOR(c, n3, { Flux[p] = (Q5[p] + P[p]) * U5[p]; });
-    ST_TRY(dev_dfd(c, 2, 1, Flux, Qcz + 4 * n3, 1, -1.0));
-    PFOR(c, n3, {
-        Q1[p] = Q1[p] * Vs[p];
-        Q2[p] = Q2[p] * Vs[p];
-        Q3[p] = Q3[p] * Vs[p];
-        double fac2 = -5.0e-1 * dF[p];
-        Qcy[p] = Qcy[p] + fac2 * Q1[p];
-        Qcy[n3 + p] = Qcy[n3 + p] + fac2 * Q2[p];
-        Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * Q3[p];
-        fac2 = -5.0e-1 * dFz[p];
-        Qcz[p] = Qcz[p] + fac2 * Q1[p];
-        Qcz[n3 + p] = Qcz[n3 + p] + fac2 * Q2[p];
-        Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * Q3[p];
-    });
-    ST_TRY(dev_d2fd2(c, 1, 0, T, Tdy, U5, 1));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DTDY], Tdy, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_d2fd2(c, 2, 0, T, Tdz, Flux, 1));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DTDZ], Tdz, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    {
-        double fac2 = f.Pr_inv;
+    if (visc) {
+        const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
+        ST_TRY(dev_d2fd2(c, 0, 0, T, GTx, dF, 1));
+        PFOR(c, n3, { Qv[4 * n3 + p] = Pri * (mu[p] * dF[p] + dmu[p] * GTx[p] * GTx[p]); });
+        ST_TRY(dev_d2fd2(c, 0, 1, u, Gxx, dF, 1));
         PFOR(c, n3, {
-            viscosity(f, T[p], Y[p], vis[p], Udz[p]);
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + fac2 * (vis[p] * (U5[p] + Flux[p]) +
-                                                      Udz[p] * (Tdy[p] * Tdy[p] + Tdz[p] * Tdz[p]));
-            U4[p] = Udz[p] * U4[p];
-            Tdy[p] = Udz[p] * Tdy[p];
-            Tdz[p] = Udz[p] * Tdz[p];
+            double fac2 = fac1 * mu[p] * dF[p];
+            Qv[p] = fac2;
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac2;
+        });
+        ST_TRY(dev_d2fd2(c, 0, 0, v, Gyx, dF, 1));
+        PFOR(c, n3, {
+            double fac2 = mu[p] * dF[p];
+            Qv[n3 + p] = fac2;
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + v[p] * fac2;
+        });
+        ST_TRY(dev_d2fd2(c, 0, 0, w, Gzx, dF, 1));
+        PFOR(c, n3, {
+            double fac2 = mu[p] * dF[p];
+            Qv[2 * n3 + p] = fac2;
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + w[p] * fac2;
+        });
+    } else {
+        ST_TRY(dev_dfd(c, 0, 0, T, GTx, 0, 1.0));
+        ST_TRY(dev_dfd(c, 0, 1, u, Gxx, 0, 1.0));
+        ST_TRY(dev_dfd(c, 0, 0, v, Gyx, 0, 1.0));
+        ST_TRY(dev_dfd(c, 0, 0, w, Gzx, 0, 1.0));
+    }
+    PFOR(c, n3, {
+        double fac2 = -5.0e-1 * Q4[p] * u[p];
+        Qcx[p] = Qcx[p] + fac2 * Gxx[p];
+        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * Gyx[p];
+        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * Gzx[p];
+    });
+
+    // ---- RHS_yz (src/rhsv_sym_mf.f:492-1428)
+    // d(rho v)/dy and d(rho w)/dz with iadd=0, cadd=-1: Qconv(4) = 0 - d(.) exactly
+    ST_TRY(dev_dfd(c, 1, 1, Q2, Qcy + 3 * n3, 0, -1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q1, v), Qcy, 0, -5.0e-1));
+    ST_TRY(dev_dfd_prod(c, 1, 0, pr_mul(Q2, v), Qcy + n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd(c, 1, 0, P, Qcy + n3, 1, -1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q3, v), Qcy + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_addmul(Q5, P, v), Qcy + 4 * n3, 0, -1.0));
+    ST_TRY(dev_dfd(c, 2, 1, Q3, Qcz + 3 * n3, 0, -1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q1, w), Qcz, 0, -5.0e-1));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q2, w), Qcz + n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd_prod(c, 2, 0, pr_mul(Q3, w), Qcz + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dev_dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_addmul(Q5, P, w), Qcz + 4 * n3, 0, -1.0));
+    // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
+    const double *dFy = Qcy + 3 * n3, *dFzz = Qcz + 3 * n3;
+    PFOR(c, n3, {
+        double fac2 = -5.0e-1 * (-dFy[p]);
+        Qcy[p] = Qcy[p] + fac2 * u[p];
+        Qcy[n3 + p] = Qcy[n3 + p] + fac2 * v[p];
+        Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * w[p];
+        fac2 = -5.0e-1 * (-dFzz[p]);
+        Qcz[p] = Qcz[p] + fac2 * u[p];
+        Qcz[n3 + p] = Qcz[n3 + p] + fac2 * v[p];
+        Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * w[p];
+    });
+    if (visc) {
+        const double Pri = f.Pr_inv;
+        ST_TRY(dev_d2fd2(c, 1, 0, T, GTy, U5, 1));
+        ST_TRY(dev_d2fd2(c, 2, 0, T, GTz, Flux, 1));
+        PFOR(c, n3, {
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + Pri * (mu[p] * (U5[p] + Flux[p]) +
+                                                    dmu[p] * (GTy[p] * GTy[p] + GTz[p] * GTz[p]));
+            U4[p] = dmu[p] * GTx[p];
+            Tdy[p] = dmu[p] * GTy[p];
+            Tdz[p] = dmu[p] * GTz[p];
+        });
+        ST_TRY(dev_d2fd2(c, 1, 0, u, Gxy, U5, 1));
+        ST_TRY(dev_d2fd2(c, 1, 1, v, Gyy, dF, 1));
+        ST_TRY(dev_d2fd2(c, 1, 0, w, Gzy, T2, 1));
+    } else {
+        ST_TRY(dev_dfd(c, 1, 0, T, GTy, 0, 1.0));
+        ST_TRY(dev_dfd(c, 2, 0, T, GTz, 0, 1.0));
+        ST_TRY(dev_dfd(c, 1, 0, u, Gxy, 0, 1.0));
+        ST_TRY(dev_dfd(c, 1, 1, v, Gyy, 0, 1.0));
+        ST_TRY(dev_dfd(c, 1, 0, w, Gzy, 0, 1.0));
+    }
+    ST_TRY(dev_dfd(c, 2, 0, u, Gxz, 0, 1.0));
+    ST_TRY(dev_dfd(c, 2, 0, v, Gyz, 0, 1.0));
+    ST_TRY(dev_dfd(c, 2, 1, w, Gzz, 0, 1.0));
+    {
+        const double fac1 = f.bulk + 4.0 / 3.0;
+        PFOR(c, n3, {
+            double fac2 = -5.0e-1 * Q4[p] * v[p];
+            Qcy[p] = Qcy[p] + fac2 * Gxy[p];
+            Qcy[n3 + p] = Qcy[n3 + p] + fac2 * Gyy[p];
+            Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * Gzy[p];
+            fac2 = -5.0e-1 * Q4[p] * w[p];
+            Qcz[p] = Qcz[p] + fac2 * Gxz[p];
+            Qcz[n3 + p] = Qcz[n3 + p] + fac2 * Gyz[p];
+            Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * Gzz[p];
+            if (visc) {
+                double fac_X = mu[p] * U5[p];
+                double fac_Y = fac1 * mu[p] * dF[p];
+                double fac_Z = mu[p] * T2[p];
+                Qv[p] = Qv[p] + fac_X;
+                Qv[n3 + p] = Qv[n3 + p] + fac_Y;
+                Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
+                Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z;
+            }
         });
     }
-    // d(rho)/dy into Udz: computed by the reference and overwritten before use
-    ST_TRY(dev_dfd(c, 1, 0, Q4, Udz, 0, 1.0));
-    ST_TRY(dev_d2fd2(c, 1, 0, Q1, P, U5, 1));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUX_DY], P, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_d2fd2(c, 1, 1, Q2, Flux, dF, 1));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUY_DY], Flux, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_d2fd2(c, 1, 0, Q3, Udz, T, 1));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUZ_DY], Udz, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_dfd(c, 2, 0, Q1, Udx, 0, 1.0));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUX_DZ], Udx, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_dfd(c, 2, 0, Q2, Udy, 0, 1.0));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUY_DZ], Udy, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_dfd(c, 2, 1, Q3, dFz, 0, 1.0));
-    ST_CUDA(c, cudaMemcpyAsync(G[G_DUZ_DZ], dFz, n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    {
-        double fac1 = f.bulk + 4.0 / 3.0;
+    if (visc) {
+        const double fac1 = f.bulk - 2.0 / 3.0, fac2 = f.bulk + 4.0 / 3.0, fac3 = f.bulk + 1.0 / 3.0;
+        ST_TRY(dev_d2fd2(c, 2, 1, w, nullptr, T2, 0));
+        ST_TRY(dev_dfd(c, 1, 0, Gzz, U5, 0, 1.0));
         PFOR(c, n3, {
-            double fac2 = -5.0e-1 * Q4[p] * Q2[p];
-            Qcy[p] = Qcy[p] + fac2 * P[p];
-            Qcy[n3 + p] = Qcy[n3 + p] + fac2 * Flux[p];
-            Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * Udz[p];
-            fac2 = -5.0e-1 * Q4[p] * Q3[p];
-            Qcz[p] = Qcz[p] + fac2 * Udx[p];
-            Qcz[n3 + p] = Qcz[n3 + p] + fac2 * Udy[p];
-            Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * dFz[p];
-            double fac_X = vis[p] * U5[p];
-            double fac_Y = fac1 * vis[p] * dF[p];
-            double fac_Z = vis[p] * T[p];
+            double tmp1 = Gxx[p];
+            double dil = tmp1 + Gyy[p] + Gzz[p];
+            double fac_X = U4[p] * (2.0 * tmp1 + fac1 * dil);
+            double fac_Y = Tdy[p] * (2.0 * Gyy[p] + fac1 * dil) + fac3 * mu[p] * U5[p];
+            double fac_Z = Tdz[p] * (2.0 * Gzz[p] + fac1 * dil) + fac2 * mu[p] * T2[p];
             Qv[p] = Qv[p] + fac_X;
             Qv[n3 + p] = Qv[n3 + p] + fac_Y;
             Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q1[p] * fac_X + Q2[p] * fac_Y + Q3[p] * fac_Z;
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
+                             mu[p] * (2.0 * (tmp1 * tmp1 + Gyy[p] * Gyy[p] + Gzz[p] * Gzz[p]) + fac1 * dil * dil);
+        });
+        ST_TRY(dev_d2fd2(c, 2, 0, u, nullptr, dF, 0));
+        ST_TRY(dev_d2fd2(c, 2, 0, v, nullptr, U5, 0));
+        PFOR(c, n3, {
+            double tmp1 = Gyx[p] + Gxy[p];
+            double tmp2 = Gzx[p] + Gxz[p];
+            double tmp3 = Gzy[p] + Gyz[p];
+            double fac_X = Tdy[p] * tmp1 + Tdz[p] * tmp2 + mu[p] * dF[p];
+            double fac_Y = U4[p] * tmp1 + Tdz[p] * tmp3 + mu[p] * U5[p];
+            double fac_Z = U4[p] * tmp2 + Tdy[p] * tmp3;
+            Qv[p] = Qv[p] + fac_X;
+            Qv[n3 + p] = Qv[n3 + p] + fac_Y;
+            Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
+            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
+                             mu[p] * (tmp1 * tmp1 + tmp2 * tmp2 + tmp3 * tmp3);
+        });
+        ST_TRY(dev_dfd(c, 1, 0, Gxx, U4, 0, 1.0));
+        ST_TRY(dev_dfd(c, 2, 0, Gxx, U5, 0, 1.0));
+        ST_TRY(dev_dfd(c, 1, 1, Gyx, Tdy, 0, 1.0));
+        ST_TRY(dev_dfd(c, 2, 1, Gzx, Tdz, 0, 1.0));
+        ST_TRY(dev_dfd(c, 1, 1, Gyz, T2, 0, 1.0));
+    }
+    {
+        const double fac3 = f.bulk + 1.0 / 3.0;
+        PFOR(c, n3, {
+            if (visc) {
+                double fac_X = fac3 * mu[p] * (Tdy[p] + Tdz[p]);
+                double fac_Y = fac3 * mu[p] * U4[p];
+                double fac_Z = fac3 * mu[p] * (U5[p] + T2[p]);
+                Qv[p] = Qv[p] + fac_X;
+                Qv[n3 + p] = Qv[n3 + p] + fac_Y;
+                Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
+                Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z;
+            }
+            // velocities back to momenta, (m/rho)*rho as the reference does
+            Q1[p] = u[p] * Q4[p];
+            Q2[p] = v[p] * Q4[p];
+            Q3[p] = w[p] * Q4[p];
+            for (int l = 0; l < 5; l++) {
+                size_t q = l * n3 + p;
+                double r = Qcx[q] + Qcy[q] + Qcz[q];
+                if (visc && l != 3) r = r + Qv[q];   // Qvisc(:,:,:,4) stays zero
+                Qrhs[q] = r;
+            }
         });
     }
-    ST_TRY(dev_d2fd2(c, 2, 1, Q3, dF, T, 0));
-    ST_CUDA(c, cudaMemcpyAsync(dF, G[G_DUZ_DZ], n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_dfd(c, 1, 0, dF, U5, 0, 1.0));
-    const double fac1 = f.bulk - 2.0 / 3.0, fac2 = f.bulk + 4.0 / 3.0, fac3 = f.bulk + 1.0 / 3.0;
-    PFOR(c, n3, {
-        double tmp1 = U1[p];
-        double dil = tmp1 + Flux[p] + dF[p];
-        double fac_X = U4[p] * (2.0 * tmp1 + fac1 * dil);
-        double fac_Y = Tdy[p] * (2.0 * Flux[p] + fac1 * dil) + fac3 * vis[p] * U5[p];
-        double fac_Z = Tdz[p] * (2.0 * dF[p] + fac1 * dil) + fac2 * vis[p] * T[p];
-        Qv[p] = Qv[p] + fac_X;
-        Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-        Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-        Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q1[p] * fac_X + Q2[p] * fac_Y + Q3[p] * fac_Z +
-                         vis[p] * (2.0 * (tmp1 * tmp1 + Flux[p] * Flux[p] + dF[p] * dF[p]) + fac1 * dil * dil);
-    });
-    ST_TRY(dev_d2fd2(c, 2, 0, Q1, T, dF, 0));
-    ST_CUDA(c, cudaMemcpyAsync(T, G[G_DUX_DZ], n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(dev_d2fd2(c, 2, 0, Q2, Flux, U5, 0));
-    ST_CUDA(c, cudaMemcpyAsync(Flux, G[G_DUY_DZ], n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    PFOR(c, n3, {
-        double tmp1 = U2[p] + P[p];
-        double tmp2 = U3[p] + T[p];
-        double tmp3 = Udz[p] + Flux[p];
-        double fac_X = Tdy[p] * tmp1 + Tdz[p] * tmp2 + vis[p] * dF[p];
-        double fac_Y = U4[p] * tmp1 + Tdz[p] * tmp3 + vis[p] * U5[p];
-        double fac_Z = U4[p] * tmp2 + Tdy[p] * tmp3;
-        Qv[p] = Qv[p] + fac_X;
-        Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-        Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-        Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q1[p] * fac_X + Q2[p] * fac_Y + Q3[p] * fac_Z +
-                         vis[p] * (tmp1 * tmp1 + tmp2 * tmp2 + tmp3 * tmp3);
-    });
-    ST_TRY(dev_dfd(c, 1, 0, U1, U4, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, U1, U5, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 1, U2, Tdy, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 1, U3, Tdz, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 1, Flux, T, 0, 1.0));
-    const bool add_visc = c->p.re > 0.0;
-    PFOR(c, n3, {
-        double fac_X = fac3 * vis[p] * (Tdy[p] + Tdz[p]);
-        double fac_Y = fac3 * vis[p] * U4[p];
-        double fac_Z = fac3 * vis[p] * (U5[p] + T[p]);
-        Qv[p] = Qv[p] + fac_X;
-        Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-        Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-        Qv[4 * n3 + p] = Qv[4 * n3 + p] + Q1[p] * fac_X + Q2[p] * fac_Y + Q3[p] * fac_Z;
-        Q1[p] = Q1[p] * Q4[p];
-        Q2[p] = Q2[p] * Q4[p];
-        Q3[p] = Q3[p] * Q4[p];
-        for (int l = 0; l < 5; l++) {
-            size_t q = l * n3 + p;
-            if (add_visc) Qrhs[q] = Qrhs[q] + Qcx[q] + Qcy[q] + Qcz[q] + Qv[q];
-            else Qrhs[q] = Qrhs[q] + Qcx[q] + Qcy[q] + Qcz[q];
-        }
-    });
     return ST_OK;
-}
-
-int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
-    const size_t n3 = c->dm.n3;
-    Scratch Ux(c, 5), Qcx(c, 5), Qcy(c, 5), Qcz(c, 5), Qv(c, 5);
-    ST_CUDA(c, cudaMemcpyAsync(Ux, Q, 5 * n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
-    ST_TRY(rhs_x(c, Ux, Qrhs, Y, Qcx, Qcy, Qcz, Qv));
-    return rhs_yz(c, Q, Ux, Qrhs, Y, Qcx, Qcy, Qcz, Qv);
 }
 
 // ---- artificial viscosity -----------------------------------------------------
@@ -426,137 +403,102 @@ int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
     return ST_OK;
 }
 
-// Hyper_RHS src/hyper_rhs_sym_mf.f:12-500
+// Hyper_RHS src/hyper_rhs_sym_mf.f:12-500.  Each sum Qh = Qh + dFx + dFy + dFz
+// is accumulated by the derivative kernels themselves in the reference's
+// x, y, z order (iadd), so dF*/dE* are never stored; fluxes that are products
+// of stored fields are formed by the derivative kernels while loading.
 int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
     if (c->p.hyper_param == 0) return ST_OK;
     const size_t n3 = c->dm.n3;
     ST_TRY(dev_compute_hyper(c, Q, Y));
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3;
-    ScratchN s(c, 16);
+    ScratchN s(c, 9);
     double *U1 = s[0], *U2 = s[1], *U3 = s[2], *dila = s[3], *S1 = s[4], *S2 = s[5], *S3 = s[6];
-    double *Flux = s[7], *FF = s[8], *dFx = s[9], *dFy = s[10], *dFz = s[11], *dEx = s[12], *dEy = s[13],
-           *dEz = s[14];
+    double *Flux = s[7], *Flux2 = s[8];
     Scratch Qhs(c, 5);
-    double *Qh = Qhs;
-    ST_CUDA(c, cudaMemsetAsync(Qh, 0, 5 * n3 * 8, c->stream));
+    double *Qh = Qhs;   // Qh(:,:,:,4) stays zero and is never added
+    double *h1 = Qh, *h2 = Qh + n3, *h3 = Qh + 2 * n3, *h5 = Qh + 4 * n3;
     const double *G0 = c->grad[0], *G1 = c->grad[1], *G2 = c->grad[2], *G3 = c->grad[3], *G4 = c->grad[4],
                  *G5 = c->grad[5], *G6 = c->grad[6], *G7 = c->grad[7], *G8 = c->grad[8];
     const double *GTx = c->grad[G_DTDX], *GTy = c->grad[G_DTDY], *GTz = c->grad[G_DTDZ];
     const double *vh = c->hyp[H_VISC], *bh = c->hyp[H_BETA], *kh = c->hyp[H_K];
-    {
-        PFOR(c, n3, {
-            U1[p] = Q1[p] / Q4[p];
-            U2[p] = Q2[p] / Q4[p];
-            U3[p] = Q3[p] / Q4[p];
-            dila[p] = G0[p] + G4[p] + G8[p];
-            S1[p] = G3[p] + G1[p];
-            S2[p] = G6[p] + G2[p];
-            S3[p] = G7[p] + G5[p];
-        });
-        double *h1 = Qh, *h2 = Qh + n3, *h3 = Qh + 2 * n3, *h5 = Qh + 4 * n3;
-        // x momentum
-        PFOR(c, n3, {
-            Flux[p] = 2.0 * vh[p] * G0[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
-            FF[p] = U1[p] * Flux[p];
-        });
-        ST_TRY(dev_dfd(c, 0, 0, Flux, dFx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 1, FF, dEx, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S1[p]; FF[p] = U1[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 1, 1, Flux, dFy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, FF, dEy, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S2[p]; FF[p] = U1[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 2, 1, Flux, dFz, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 1, FF, dEz, 0, 1.0));
-        PFOR(c, n3, {
-            h1[p] = h1[p] + dFx[p] + dFy[p] + dFz[p];
-            h5[p] = h5[p] + dEx[p] + dEy[p] + dEz[p];
-        });
-        // y momentum
-        PFOR(c, n3, {
-            Flux[p] = 2.0 * vh[p] * G4[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
-            FF[p] = U2[p] * Flux[p];
-        });
-        ST_TRY(dev_dfd(c, 1, 0, Flux, dFy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, FF, dEy, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S1[p]; FF[p] = U2[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 0, 1, Flux, dFx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 1, FF, dEx, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S3[p]; FF[p] = U2[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 2, 1, Flux, dFz, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 1, FF, dEz, 0, 1.0));
-        PFOR(c, n3, {
-            h2[p] = h2[p] + dFx[p] + dFy[p] + dFz[p];
-            h5[p] = h5[p] + dEx[p] + dEy[p] + dEz[p];
-        });
-        // z momentum
-        PFOR(c, n3, {
-            Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
-            FF[p] = U3[p] * Flux[p];
-        });
-        ST_TRY(dev_dfd(c, 2, 0, Flux, dFz, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 1, FF, dEz, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S2[p]; FF[p] = U3[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 0, 1, Flux, dFx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 1, FF, dEx, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = vh[p] * S3[p]; FF[p] = U3[p] * Flux[p]; });
-        ST_TRY(dev_dfd(c, 1, 1, Flux, dFy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, FF, dEy, 0, 1.0));
-        PFOR(c, n3, {
-            h3[p] = h3[p] + dFx[p] + dFy[p] + dFz[p];
-            h5[p] = h5[p] + dEx[p] + dEy[p] + dEz[p];
-        });
-        // artificial heat flux
-        PFOR(c, n3, { Flux[p] = kh[p] * GTx[p]; });
-        ST_TRY(dev_dfd(c, 0, 0, Flux, dFx, 0, 1.0));
-        PFOR(c, n3, { FF[p] = kh[p] * GTy[p]; });
-        ST_TRY(dev_dfd(c, 1, 0, FF, dFy, 0, 1.0));
-        PFOR(c, n3, { Flux[p] = kh[p] * GTz[p]; });
-        ST_TRY(dev_dfd(c, 2, 0, Flux, dFz, 0, 1.0));
-        PFOR(c, n3, {
-            h5[p] = h5[p] + dFx[p] + dFy[p] + dFz[p];
-            for (int l = 0; l < 5; l++) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] + Qh[l * n3 + p];
-        });
-    }
+    PFOR(c, n3, {
+        U1[p] = Q1[p] / Q4[p];
+        U2[p] = Q2[p] / Q4[p];
+        U3[p] = Q3[p] / Q4[p];
+        dila[p] = G0[p] + G4[p] + G8[p];
+        S1[p] = G3[p] + G1[p];
+        S2[p] = G6[p] + G2[p];
+        S3[p] = G7[p] + G5[p];
+        Flux[p] = 2.0 * vh[p] * G0[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
+        Flux2[p] = 2.0 * vh[p] * G4[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
+    });
+    // x momentum: Qh1 = dFx + dFy + dFz, Qh5 = dEx + dEy + dEz
+    ST_TRY(dev_dfd(c, 0, 0, Flux, h1, 0, 1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(U1, Flux), h5, 0, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(vh, S1), h1, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mulmul(vh, S1, U1), h5, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(vh, S2), h1, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mulmul(vh, S2, U1), h5, 1, 1.0));
+    // y momentum (x, y, z accumulation order)
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(vh, S1), h2, 0, 1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mulmul(vh, S1, U2), h5, 1, 1.0));
+    ST_TRY(dev_dfd(c, 1, 0, Flux2, h2, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(U2, Flux2), h5, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
+    // z momentum
+    PFOR(c, n3, { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mulmul(vh, S3, U3), h5, 1, 1.0));
+    ST_TRY(dev_dfd(c, 2, 0, Flux, h3, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(U3, Flux), h5, 1, 1.0));
+    // artificial heat flux
+    ST_TRY(dev_dfd_prod(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 0, pr_mul(kh, GTz), h5, 1, 1.0));
+    PFOR(c, n3, {
+        for (int l = 0; l < 5; l++)
+            if (l != 3) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] + Qh[l * n3 + p];
+    });
     return ST_OK;
 }
 
-// Species_RHS src/species_rhs_sym.f:9-207
+// Species_RHS src/species_rhs_sym.f:9-207.  Yrhs accumulates the three
+// convective derivatives in x, y, z order, then adds Ydiff, as
+// Yrhs = Yconvx + Yconvy + Yconvz + Ydiff does.
 int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (c->p.hyper_param == 0) return ST_OK;
     const size_t n3 = c->dm.n3;
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    ScratchN s(c, 7);
-    double *Ycx = s[0], *Ycy = s[1], *Ycz = s[2], *Yd = s[3], *Flux = s[4], *FF = s[5], *T = s[6];
+    ScratchN s(c, 2);
+    double *Yd = s[0], *T = s[1];
     const double *Dh = c->hyp[H_D];
     const double *g = c->gamma_eff;
     PFOR(c, n3, {
         double Vs, P, Tt;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, P, Tt);
         T[p] = Tt;
-        Yrhs[p] = 0.0; Ycx[p] = 0.0; Ycy[p] = 0.0; Ycz[p] = 0.0; Yd[p] = 0.0;
     });
     ST_TRY(dev_dfd(c, 0, 0, Y, c->dYd[0], 0, 1.0));
     ST_TRY(dev_dfd(c, 1, 0, Y, c->dYd[1], 0, 1.0));
     ST_TRY(dev_dfd(c, 2, 0, Y, c->dYd[2], 0, 1.0));
-    PFOR(c, n3, { Flux[p] = Q1[p] * Y[p]; });
-    ST_TRY(dev_dfd(c, 0, 1, Flux, Ycx, 1, -1.0));
-    PFOR(c, n3, { Flux[p] = Q2[p] * Y[p]; });
-    ST_TRY(dev_dfd(c, 1, 1, Flux, Ycy, 1, -1.0));
-    PFOR(c, n3, { Flux[p] = Q3[p] * Y[p]; });
-    ST_TRY(dev_dfd(c, 2, 1, Flux, Ycz, 1, -1.0));
-    const double cst0 = f.eps * f.g2 * (f.g1 - 1.0) / (f.g1 * (f.g2 - 1.0));
-    const double Re1i = f.Re1_inv, Sci = f.Sc_inv;
+    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q1, Y), Yrhs, 0, -1.0));
+    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q2, Y), Yrhs, 1, -1.0));
+    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q3, Y), Yrhs, 1, -1.0));
+    const double cst = 1.0 - f.eps * f.g2 * (f.g1 - 1.0) / (f.g1 * (f.g2 - 1.0));
     for (int d = 0; d < 3; d++) {
-        const double *dY = c->dYd[d];
-        PFOR(c, n3, {
-            Flux[p] = Q4[p] * Dh[p] * dY[p] + Q4[p] * dY[p] * Re1i * Sci;
-            FF[p] = (1.0 - cst0) * T[p] * Flux[p];
-        });
-        ST_TRY(dev_dfd(c, d, 1, Flux, Yd, 1, 1.0));
-        ST_TRY(dev_dfd(c, d, 1, FF, Qrhs + 4 * n3, 1, 1.0));
+        Prod fl{};
+        fl.op = PR_SPEC; fl.a = Q4; fl.b = Dh; fl.c = c->dYd[d]; fl.k0 = f.Re1_inv; fl.k1 = f.Sc_inv;
+        Prod ft = fl;
+        ft.op = PR_SPECT; ft.d = T; ft.k2 = cst;
+        ST_TRY(dev_dfd_prod(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
+        ST_TRY(dev_dfd_prod(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
     }
-    PFOR(c, n3, { Yrhs[p] = Ycx[p] + Ycy[p] + Ycz[p] + Yd[p]; });
+    PFOR(c, n3, { Yrhs[p] = Yrhs[p] + Yd[p]; });
     return ST_OK;
 }
 
@@ -817,6 +759,10 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
 // ---- LDDRK4 (src/lddrk4_nonperiodic_mf.f:428-541) -------------------------------
 // dt is read from dscal[6] on the device (set by dev_compute_tstep or
 // st_set_tstep), so the whole step can run without a host round trip.
+// The QW = 0 / rYW = 0 resets at the start of each loop are folded into the
+// first stage, whose coefficient alpha(1) is 0 (0*0 + dt*dQ == dt*dQ); the
+// last filter pass of each conserved variable writes Q itself (Q = Qf), and
+// Compute_Y is fused with Fix_Pressure.
 int dev_lddrk4(st_ctx *c, bool) {
     static const double alpha1[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
                                      -2.016477077503357e+00, -1.056444269767207e+00};
@@ -828,11 +774,10 @@ int dev_lddrk4(st_ctx *c, bool) {
     const double *dtp = c->dscal + 6;
     double *timep = c->dscal + 7;
     for (int loop = 0; loop < 2; loop++) {
-        ST_CUDA(c, cudaMemsetAsync(c->QW, 0, 5 * n3 * 8, c->stream));
-        ST_CUDA(c, cudaMemsetAsync(c->rYW, 0, n3 * 8, c->stream));
         for (int K = 0; K < 5; K++) {
             const bool real = loop == 0 || c->p.rk_mode == 1;
             const double al = real ? alpha1[K] : 0.0, be = real ? beta1[K] : 0.0;
+            const bool first = K == 0;
             double *Q = c->Q, *dQ = c->dQ, *QW = c->QW, *Y = c->Y, *drYi = c->drYi, *rYW = c->rYW;
             ST_TRY(dev_compute_gamma(c, Y));
             ST_TRY(dev_rhs(c, Q, dQ, Y));
@@ -845,21 +790,34 @@ int dev_lddrk4(st_ctx *c, bool) {
                 double ry = Q[3 * n3 + p] * Y[p];
                 for (int l = 0; l < 5; l++) {
                     size_t q = l * n3 + p;
-                    QW[q] = al * QW[q] + dt * dQ[q];
-                    Q[q] = Q[q] + be * QW[q];
+                    double qw = first ? dt * dQ[q] : al * QW[q] + dt * dQ[q];
+                    QW[q] = qw;
+                    Q[q] = Q[q] + be * qw;
                 }
-                rYW[p] = al * rYW[p] + dt * drYi[p];
-                rY[p] = ry + be * rYW[p];
+                double rw = first ? dt * drYi[p] : al * rYW[p] + dt * drYi[p];
+                rYW[p] = rw;
+                rY[p] = ry + be * rw;
             });
-            ST_TRY(dev_compact_filter(c, Q, Qf, 5));
+            // Compact_Filter(Q, Qf, 5) then Q = Qf (src/lddrk4_nonperiodic_mf.f:476-481)
+            for (int l = 0; l < 5; l++) {
+                ST_TRY(dev_filter(c, 0, l == 0, Q + l * n3, Qf + l * n3));
+                ST_TRY(dev_filter(c, 1, l == 1, Qf + l * n3, Qf + l * n3));
+                ST_TRY(dev_filter(c, 2, l == 2, Qf + l * n3, Q + l * n3));
+            }
             ST_TRY(dev_filter(c, 0, 0, rY, rY));
             ST_TRY(dev_filter(c, 1, 0, rY, rY));
             ST_TRY(dev_filter(c, 2, 0, rY, rY));
+            // Compute_Y + Fix_Pressure (pproc/pproc_mf.f:190-233)
+            const double *g = c->gamma_eff;
             PFOR(c, n3, {
-                for (int l = 0; l < 5; l++) Q[l * n3 + p] = Qf[l * n3 + p];
-                Y[p] = rY[p] / Q[3 * n3 + p];
+                double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p];
+                Y[p] = rY[p] / q4;
+                double fac1 = g[p] - 1.0;
+                double Vs = 1.0 / q4;
+                double P = fac1 * (Q[4 * n3 + p] - 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3));
+                if (P < 0.0) P = 0.71429;
+                Q[4 * n3 + p] = (1.0 / fac1) * P + 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3);
             });
-            ST_TRY(dev_fix_pressure(c, Q));
         }
         PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
     }
