@@ -15,10 +15,11 @@
 namespace st {
 
 constexpr int kMaxSeg = 32;       // max segments per line (warps per CTA)
-constexpr int kLanes = 32;        // lines per CTA (lanes of a warp)
+constexpr int kLanes = 16;        // lines per CTA (half a warp; a warp holds two segments)
 
-// A line of n rows is split into P = n/S segments of S rows; warp s of a CTA
-// owns segment s of 32 neighbouring lines (lane = line).  Supported S.
+// A line of n rows is split into P = n/S segments of S rows; thread t of a CTA
+// works on line t%16 and segment t/16 of 16 neighbouring lines, so a warp
+// holds two adjacent segments of the same 16 lines.  Supported S.
 int choose_seg(int n);
 
 // Row tables of a constant-coefficient tridiagonal system, factorised as the

@@ -23,7 +23,7 @@ struct LineArgs {
 #define LINE_PROLOGUE                                                                  \
     __shared__ CarryBuf cb;                                                            \
     extern __shared__ double tile[];                                                   \
-    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5, n = a.geo.n, row0 = s * S; \
+    const int lane = threadIdx.x & (kLanes - 1), s = threadIdx.x / kLanes, n = a.geo.n, row0 = s * S; \
     const ColMap m = a.geo.map(blockIdx.x);                                            \
     const RowReader<OP> rd = YT ? RowReader<OP>{tile + lane * (n + 1), nullptr, 0, 0}  \
                                 : RowReader<OP>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
@@ -49,7 +49,7 @@ __device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, dou
 
 // DF*_sym/_asym: O1 (=|+=) cadd * dF/ds
 template <int S, bool YT, int OP>
-__global__ void __launch_bounds__(1024) k_dfd(LineArgs a) {
+__global__ void __launch_bounds__(512, 2) k_dfd(LineArgs a) {
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
     double v[S + 4];
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(1024) k_dfd(LineArgs a) {
 // D2F*2_sym/_asym: O2 = d2F/ds2; if iadd, O1 = dF/ds (cadd = 1).  The first
 // derivative re-reads the rows (the CTA's lines are still in L2).
 template <int S, bool YT>
-__global__ void __launch_bounds__(1024) k_d2fd2(LineArgs a) {
+__global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgs a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(1024) k_d2fd2(LineArgs a) {
 // F (including the boundary re-reads) happens before the solve's first
 // barrier and every write after its last one.
 template <int S, bool YT>
-__global__ void __launch_bounds__(1024) k_filter(LineArgs a) {
+__global__ void __launch_bounds__(512, 2) k_filter(LineArgs a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(1024) k_filter(LineArgs a) {
 
 // Gaussian_Filter_X/Y/Z: O1 = explicit 9-point Gaussian of F (O1 != F)
 template <int S, bool YT>
-__global__ void __launch_bounds__(1024) k_gauss(LineArgs a) {
+__global__ void __launch_bounds__(512, 2) k_gauss(LineArgs a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;

@@ -1,13 +1,16 @@
 // st_line.cuh - device building blocks of the line operators.
 //
-// Work decomposition ("columns"): a CTA owns 32 neighbouring lines of one
-// direction; lane l of every warp works on line l and warp s on the rows
-// [s*S, s*S+S) of those lines, held in registers.  Consequences:
-//  - for x and z lines the 32 lanes touch 32 adjacent doubles of every row,
-//    so every global access is one coalesced 256-byte transaction;
-//  - all lanes of a warp are on the same row, so the LU-table reads are
-//    warp-uniform (one broadcast);
-//  - boundary rows belong to the first and last warp only (no divergence);
+// Work decomposition ("columns"): a CTA owns 16 neighbouring lines of one
+// direction; thread t works on line t%16 and on the rows [s*S, s*S+S) of
+// segment s = t/16, held in registers (a warp holds two adjacent segments).
+// Consequences:
+//  - for x and z lines 16 threads touch 16 adjacent doubles of every row, so
+//    every global access is a full 128-byte transaction;
+//  - the 16 threads of a segment are on the same row, so the LU-table reads
+//    are uniform per half-warp (two broadcasts per warp);
+//  - boundary rows belong to the first and last segments only;
+//  - 512-thread CTAs at 64 registers let two CTAs share an SM, so one CTA's
+//    loads overlap the other's solve;
 //  - segments exchange their end values through shared memory once per
 //    recurrence direction; the carry into each segment is a fixed linear
 //    combination of those values (tables wf/wb, mf/mb).
