@@ -105,6 +105,17 @@ int  st_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C
 int  st_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C,
                       const double *D, const double *E, double *R,
                       int n, int lot, int nper);
+/* No counterpart in the reference.  st_tridiagonal for callers that must not
+ * allocate device memory (code running during stream capture, or code that owns
+ * the device's memory through its own pool): the working copies of A and B live
+ * in a fixed static device array instead of cudaMalloc'd buffers.
+ * n*lot <= 262144 (ST_E_ARG beyond); A, B, C, R must be device arrays of the
+ * context's device (ST_E_ARG for host arrays).  The first call on a device
+ * looks the array up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  The array is shared per device: calls whose GPU work overlaps race
+ * on it.  Returns once R is written. */
+int  st_tridiagonal_noalloc(st_ctx *c, const double *A, const double *B, const double *C,
+                            double *R, int n, int lot, int nper);
 
 /* ---- compact derivatives ------------------------------------------------ */
 /* DFDX_sym(F,dF,iadd,cadd) src/derivCDopt6_sym_tri.f:409-535, DFDY_sym :672,

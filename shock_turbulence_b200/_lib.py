@@ -28,6 +28,7 @@ SIGNATURES = {
     "st_set_common": [_ctx, ctypes.c_char_p, _dp],
     "st_tridiagonal": [_ctx, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "st_pentadiagonal": [_ctx, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "st_tridiagonal_noalloc": [_ctx, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "st_compact_filter": [_ctx, _dp, _dp, ctypes.c_int],
     "st_gaussian_filter": [_ctx, _dp, _dp, ctypes.c_int],
     "st_compute_gamma": [_ctx, _dp],

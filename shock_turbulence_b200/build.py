@@ -10,7 +10,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libst_b200.so")
-SOURCES = ["st_kernels.cu", "st_physics.cu", "st_tables.cpp", "st_api.cpp"]
+SOURCES = ["st_kernels.cu", "st_physics.cu", "st_noalloc.cu", "st_tables.cpp", "st_api.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "--fmad=false", "--extended-lambda", "-std=c++17",
