@@ -172,7 +172,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=384, help="grid points per direction")
-    ap.add_argument("--cpu-n", type=int, default=64, help="grid of the CPU-oracle sample")
+    ap.add_argument("--cpu-n", type=int, default=96, help="grid of the CPU-oracle sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -197,9 +197,10 @@ def main():
         return
 
     from shock_turbulence_b200 import Solver
+    from shock_turbulence_b200.replicas import aggregate_rate, max_over_ranks, replica_seed
     torch.cuda.set_device(local)
     p = make_params(args.n, device=local)
-    Q, Y = make_state(p, seed=1 + rank)
+    Q, Y = make_state(p, seed=replica_seed(1, rank))
     s = Solver(p)
     stream = torch.cuda.current_stream()
     s._check(s.lib.st_set_stream(s._h, stream.cuda_stream), "st_set_stream")
@@ -238,13 +239,9 @@ def main():
     buf = ctypes.create_string_buffer(1 << 16)
     s._check(s.lib.st_profile_report(s._h, buf, len(buf)), "st_profile_report")
     prof = json.loads(buf.value.decode())
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     cells = args.n ** 3
-    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    value = aggregate_rate(cells, args.steps, ms, world)
     mon = s.monitors()
     finite = bool(math.isfinite(mon[0]) and math.isfinite(mon[5]))
 
@@ -266,12 +263,8 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms_e2e = f0.elapsed_time(f1)
-        if dist is not None:
-            tt = torch.tensor([ms_e2e], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms_e2e = float(tt.item())
-        e2e = world * cells * args.e2e_steps / (ms_e2e / 1e3) / 1e6
+        ms_e2e = max_over_ranks(f0.elapsed_time(f1), dist, "cuda")
+        e2e = aggregate_rate(cells, args.e2e_steps, ms_e2e, world)
 
     # ---- roofline of the dominant kernel ----
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -296,9 +289,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, el = oracle_rate(args.cpu_n, 2, 1, threads)
+        rate, el = oracle_rate(args.cpu_n, 3, 1, threads)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 2 timed steps "
+               "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 3 timed steps "
                          f"({el:.1f} s), {threads} OpenMP threads"}
 
     if rank == 0:
