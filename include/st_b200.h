@@ -62,7 +62,22 @@ typedef struct st_params {
                                    coefficient; 1 reproduces the reference
                                    (src/hyper_dynamic_sym_mf.f:145-147)       */
     int    device;              /* CUDA device ordinal                        */
+    int    family;              /* ST_FAMILY_MF: two-species symmetric octant
+                                   (src/main_mf.f and the *_sym_mf, *_tri,
+                                   filters_sym/asym routines);
+                                   ST_FAMILY_PERIODIC: single-fluid triply
+                                   periodic box (src/main.f with
+                                   derivCDopt6_periodic.f, filters_periodic.f,
+                                   rhsv_periodic_sf.f, hyper_dynamic.f,
+                                   hyper_rhs.f, lddrk4_periodic_sf.f).  In the
+                                   periodic family gamma1 is the fluid's gamma,
+                                   re its Reynolds number (re1 is ignored), and
+                                   x_leng = period_x*(nx-1)/nx as Define_Param
+                                   sets it (src/define_periodic_sf.f:42).      */
 } st_params;
+
+#define ST_FAMILY_MF        0
+#define ST_FAMILY_PERIODIC  1
 
 typedef struct st_ctx st_ctx;
 
@@ -136,6 +151,16 @@ int  st_d2fdz2_sym (st_ctx *c, const double *F, double *dF, double *d2F, int iad
 int  st_d2fdx2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
 int  st_d2fdy2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
 int  st_d2fdz2_asym(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+/* Periodic family (ST_FAMILY_PERIODIC contexts only): DFDX(F,dF,iadd,cadd)
+ * src/derivCDopt6_periodic.f:164-278, DFDY :400, DFDZ :631 and
+ * D2FDX2(F,dF,d2F,iadd) :281-397, D2FDY2 :515, D2FDZ2 :747.  Cyclic
+ * sixth-order compact schemes with the FDL3DI constants. */
+int  st_dfdx(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdy(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_dfdz(st_ctx *c, const double *F, double *dF, int iadd, double cadd);
+int  st_d2fdx2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdy2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
+int  st_d2fdz2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd);
 
 /* ---- filters -------------------------------------------------------------- */
 /* Compact_Filter(F,F0,N) src/filters_sym.f:398-432 (variable 1 filtered with
@@ -150,6 +175,12 @@ int  st_compact_filter_z_sym (st_ctx *c, const double *F, double *F0);
 int  st_compact_filter_x_asym(st_ctx *c, const double *F, double *F0);
 int  st_compact_filter_y_asym(st_ctx *c, const double *F, double *F0);
 int  st_compact_filter_z_asym(st_ctx *c, const double *F, double *F0);
+/* Periodic family: Compact_Filter_{X,Y,Z} src/filters_periodic.f:115-250,
+ * 254-389, 393-528 (cyclic eighth-order filter).  st_compact_filter and
+ * st_gaussian_filter* serve both families. */
+int  st_compact_filter_x(st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_y(st_ctx *c, const double *F, double *F0);
+int  st_compact_filter_z(st_ctx *c, const double *F, double *F0);
 /* Gaussian_Filter(F,Fg,N) src/filters_sym.f:1046-1071 and its X/Y/Z passes
  * :1076-1554 (coefficients rounded to float32, src/LES_header:153-157). */
 int  st_gaussian_filter  (st_ctx *c, const double *F, double *Fg, int nvar);

@@ -69,6 +69,8 @@ def lib():
 
 
 def _p(a):
+    if a is None:
+        return None
     assert a.dtype == np.float64 and a.flags.c_contiguous, "oracle needs C-contiguous float64"
     return a.ctypes.data_as(_dp)
 
@@ -109,7 +111,7 @@ class Oracle:
     # --- state ---------------------------------------------------------
     def set_state(self, Q, Y):
         lib().orc_set_state(ctypes.c_void_p(self._c), _p(np.ascontiguousarray(Q)),
-                            _p(np.ascontiguousarray(Y)))
+                            None if Y is None else _p(np.ascontiguousarray(Y)))
 
     def get_state(self):
         Q, Y = self.field(5), self.field()
@@ -155,13 +157,13 @@ class Oracle:
     def compute_gamma(self, Y):
         lib().orc_compute_gamma(ctypes.c_void_p(self._c), _p(Y))
 
-    def rhs(self, Q, Qrhs, Y):
+    def rhs(self, Q, Qrhs, Y=None):
         lib().orc_rhs(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y))
 
-    def compute_hyper(self, Q, Y):
+    def compute_hyper(self, Q, Y=None):
         lib().orc_compute_hyper(ctypes.c_void_p(self._c), _p(Q), _p(Y))
 
-    def hyper_rhs(self, Q, Qrhs, Y):
+    def hyper_rhs(self, Q, Qrhs, Y=None):
         lib().orc_hyper_rhs(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y))
 
     def species_rhs(self, Q, Qrhs, Y, Yrhs):
@@ -173,7 +175,7 @@ class Oracle:
     def sponge_forcing(self, Q, Qrhs, Y, Yrhs):
         lib().orc_sponge_forcing(ctypes.c_void_p(self._c), _p(Q), _p(Qrhs), _p(Y), _p(Yrhs))
 
-    def fix_pressure(self, Q, Y):
+    def fix_pressure(self, Q, Y=None):
         lib().orc_fix_pressure(ctypes.c_void_p(self._c), _p(Q), _p(Y))
 
     def compute_cfl(self, Q):

@@ -311,6 +311,14 @@ orc *orc_create(const st_params *p) {
     for (int g = 0; g < 12; g++) c->grad[g] = NEWF(c);
     for (int h = 0; h < 4; h++) c->hyp[h] = NEWF(c);
     for (int h = 0; h < 3; h++) c->dYd[h] = NEWF(c);
+    if (c->p.family == ST_FAMILY_PERIODIC) {
+        /* single fluid (src/define_periodic_sf.f:178-189): Re_inv = 1/Re, gamma
+         * everywhere, mass fraction one, so the mixture formulas of the shared
+         * RHS code reduce exactly to the single-fluid ones */
+        c->Re1_inv = p->re > 0.0 ? 1.0 / p->re : 0.0;
+        c->Re2_inv = 0.0;
+        for (size_t q = 0; q < c->n3; q++) { c->gamma_eff[q] = p->gamma1; c->Y[q] = 1.0; }
+    }
     return c;
 }
 
@@ -331,11 +339,157 @@ void orc_destroy(orc *c) {
     free(c);
 }
 
+/* ---- periodic single-fluid family (ST_FAMILY_PERIODIC) --------------------
+ * Operators of src/derivCDopt6_periodic.f and src/filters_periodic.f on one
+ * rank: the MPI halo planes FP/FN are the line's own far rows, so every row
+ * uses the interior formula with indices taken modulo n, and the system is
+ * solved by pentadiagonal_periodic_serial (src/pentadiagonal.f90:381-504).
+ *
+ * Constant set (the periodic routines were written for a pentadiagonal
+ * scheme with an f(i+-3) term, while src/header:191-204 activates the
+ * FDL3DI tridiagonal set): the FDL3DI values are mapped onto the periodic
+ * formulas as the tridiagonal scheme they denote -- first derivative
+ * c1 = 0, beta1 = 0; second derivative with zero weight on f(i+-3) and
+ * centre weight 2(a2+b2), beta2 = 0.  The shipped header's literal
+ * substitution (c2_pade6 = 2(a2+b2) on f(i+-3), d2_pade6 = 0 at the centre,
+ * src/derivCDopt6_periodic.f:326-329) is not a consistent second derivative
+ * and is not reproduced. */
+static const double per_c1 = 0.0;             /* f(i+-3) weight, first derivative  */
+static const double per_c2 = 0.0;             /* f(i+-3) weight, second derivative */
+#define PER_D2 C2_P6                          /* centre weight, second derivative   */
+
+static int is_per(const orc *c) { return c->p.family == ST_FAMILY_PERIODIC; }
+
+/* pentadiagonal_periodic_serial for one contiguous line with constant rows
+ * (bt, al, 1, al, bt); wk holds 7n doubles.  src/pentadiagonal.f90:381-504 */
+static void per_pen_line(double bt, double al, double *R, int n, double *wk) {
+    if (n < 5) {
+        double *A = wk, *B = wk + n, *C = wk + 2 * n, *D = wk + 3 * n, *E = wk + 4 * n;
+        for (int i = 0; i < n; i++) { A[i] = bt; B[i] = al; C[i] = 1.0; D[i] = al; E[i] = bt; }
+        orc_pentadiagonal(A, B, C, D, E, R, n, 1, 1);
+        return;
+    }
+    double *A = wk, *B = wk + n, *C = wk + 2 * n, *D = wk + 3 * n, *E = wk + 4 * n;
+    double *s1 = wk + 5 * n, *s2 = wk + 6 * n;
+    for (int i = 0; i < n; i++) {
+        A[i] = bt; B[i] = al; C[i] = 1.0; D[i] = al; E[i] = bt; s1[i] = 0.0; s2[i] = 0.0;
+    }
+    s1[0] = A[0];
+    s1[n - 4] = s1[n - 4] + E[n - 4];
+    s1[n - 3] = D[n - 3];
+    s1[n - 2] = C[n - 2];
+    s1[n - 1] = B[n - 1];
+    s2[0] = B[0];
+    s2[1] = A[1];
+    s2[n - 3] = s2[n - 3] + E[n - 3];
+    s2[n - 2] = D[n - 2];
+    s2[n - 1] = C[n - 1];
+    for (int i = 0; i <= n - 3; i++) {
+        double cs = B[i + 1] / C[i];
+        C[i + 1] = C[i + 1] - D[i] * cs;
+        D[i + 1] = D[i + 1] - E[i] * cs;
+        R[i + 1] = R[i + 1] - R[i] * cs;
+        s1[i + 1] = s1[i + 1] - s1[i] * cs;
+        s2[i + 1] = s2[i + 1] - s2[i] * cs;
+        cs = A[i + 2] / C[i];
+        B[i + 2] = B[i + 2] - D[i] * cs;
+        C[i + 2] = C[i + 2] - E[i] * cs;
+        R[i + 2] = R[i + 2] - R[i] * cs;
+        s1[i + 2] = s1[i + 2] - s1[i] * cs;
+        s2[i + 2] = s2[i + 2] - s2[i] * cs;
+    }
+    for (int i = n - 3; i >= 2; i--) {
+        double cs = D[i - 1] / C[i];
+        R[i - 1] = R[i - 1] - R[i] * cs;
+        s1[i - 1] = s1[i - 1] - s1[i] * cs;
+        s2[i - 1] = s2[i - 1] - s2[i] * cs;
+        cs = E[i - 2] / C[i];
+        R[i - 2] = R[i - 2] - R[i] * cs;
+        s1[i - 2] = s1[i - 2] - s1[i] * cs;
+        s2[i - 2] = s2[i - 2] - s2[i] * cs;
+    }
+    {
+        double cs = D[0] / C[1];
+        R[0] = R[0] - R[1] * cs;
+        s1[0] = s1[0] - s1[1] * cs;
+        s2[0] = s2[0] - s2[1] * cs;
+    }
+    double cs = E[n - 2] / C[0];
+    R[n - 2] = R[n - 2] - R[0] * cs;
+    s1[n - 2] = s1[n - 2] - s1[0] * cs;
+    s2[n - 2] = s2[n - 2] - s2[0] * cs;
+    cs = D[n - 1] / C[0];
+    R[n - 1] = R[n - 1] - R[0] * cs;
+    s1[n - 1] = s1[n - 1] - s1[0] * cs;
+    s2[n - 1] = s2[n - 1] - s2[0] * cs;
+    cs = E[n - 1] / C[1];
+    R[n - 1] = R[n - 1] - R[1] * cs;
+    s1[n - 1] = s1[n - 1] - s1[1] * cs;
+    s2[n - 1] = s2[n - 1] - s2[1] * cs;
+    cs = s1[n - 1] / s1[n - 2];
+    R[n - 1] = R[n - 1] - R[n - 2] * cs;
+    s2[n - 1] = s2[n - 1] - s2[n - 2] * cs;
+    R[n - 1] = R[n - 1] / s2[n - 1];
+    R[n - 2] = (R[n - 2] - s2[n - 2] * R[n - 1]) / s1[n - 2];
+    for (int i = n - 3; i >= 0; i--) R[i] = (R[i] - s1[i] * R[n - 2] - s2[i] * R[n - 1]) / C[i];
+}
+
+enum { PER_D1, PER_D2OP, PER_FILT, PER_GAUSS };
+
+/* One periodic line operator over all lines of direction d.
+ * DFDX src/derivCDopt6_periodic.f:164-278 (RHS :205-248, solve :251),
+ * D2FDX2 :281-397, Compact_Filter_X src/filters_periodic.f:115-250,
+ * Gaussian_Filter_X :565-676, and the y/z twins of each. */
+static void per_line_op(orc *c, int d, int kind, const double *F, double *O, int iadd, double cadd) {
+    int n; size_t st, lot;
+    line_geom(c, d, &n, &st, &lot);
+    double fac = 0.0;
+    if (kind == PER_D1) fac = cadd * c->s1[d] * (double)(n - 1);
+    if (kind == PER_D2OP) fac = ((double)((n - 1) * (n - 1))) * c->s2[d];
+    const double g0 = c->ag[0], g1 = c->ag[1], g2 = c->ag[2], g3 = c->ag[3], g4 = c->ag[4];
+#pragma omp parallel
+    {
+        double *wk = dalloc(8 * (size_t)n);
+        double *R = wk + 7 * (size_t)n;
+#pragma omp for schedule(static)
+        for (size_t L = 0; L < lot; L++) {
+            const double *f = F + line_base(c, d, L);
+#define FW_(i) f[(size_t)((((i) % n) + n) % n) * st]
+            for (int i = 0; i < n; i++) {
+                if (kind == PER_D1)
+                    R[i] = fac * (per_c1 * (FW_(i + 3) - FW_(i - 3)) + b1_p6 * (FW_(i + 2) - FW_(i - 2))
+                                  + a1_p6 * (FW_(i + 1) - FW_(i - 1)));
+                else if (kind == PER_D2OP)
+                    R[i] = fac * (per_c2 * (FW_(i + 3) + FW_(i - 3)) + b2_p6 * (FW_(i + 2) + FW_(i - 2))
+                                  + a2_p6 * (FW_(i + 1) + FW_(i - 1)) - PER_D2 * FW_(i));
+                else if (kind == PER_FILT)
+                    R[i] = a4_f4 * (FW_(i + 4) + FW_(i - 4)) + a3_f4 * (FW_(i + 3) + FW_(i - 3))
+                           + a2_f4 * (FW_(i + 2) + FW_(i - 2)) + a1_f4 * (FW_(i + 1) + FW_(i - 1))
+                           + a0_f4 * FW_(i);
+                else
+                    R[i] = g4 * (FW_(i + 4) + FW_(i - 4)) + g3 * (FW_(i + 3) + FW_(i - 3))
+                           + g2 * (FW_(i + 2) + FW_(i - 2)) + g1 * (FW_(i + 1) + FW_(i - 1)) + g0 * FW_(i);
+            }
+#undef FW_
+            if (kind == PER_D1) per_pen_line(0.0, alpha1_p6, R, n, wk);
+            else if (kind == PER_D2OP) per_pen_line(0.0, alpha2_p6, R, n, wk);
+            else if (kind == PER_FILT) per_pen_line(beta_f4, alpha_f4, R, n, wk);
+            double *o = O + line_base(c, d, L);
+            for (int i = 0; i < n; i++) {
+                if (iadd == 1) o[(size_t)i * st] = o[(size_t)i * st] + R[i];
+                else o[(size_t)i * st] = R[i];
+            }
+        }
+        free(wk);
+    }
+}
+
 /* ---- derivatives ---------------------------------------------------------- */
 /* DFDX_sym src/derivCDopt6_sym_tri.f:409-535 / DFDX_asym
  * src/derivCDopt6_asym_tri.f:412-537 and their y/z twins (the one-rank
  * branches xrank==0 and xrank==Px-1 both apply). */
 void orc_dfd(orc *c, int d, int asym, const double *F, double *dF, int iadd, double cadd) {
+    if (is_per(c)) { per_line_op(c, d, PER_D1, F, dF, iadd, cadd); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
     double fac = cadd * c->s1[d] * (double)(n - 1);
@@ -374,6 +528,12 @@ void orc_dfd(orc *c, int d, int asym, const double *F, double *dF, int iadd, dou
 /* D2FDX2_sym src/derivCDopt6_sym_tri.f:538-669 / D2FDX2_asym
  * src/derivCDopt6_asym_tri.f:540-667 and y/z twins */
 void orc_d2fd2(orc *c, int d, int asym, const double *F, double *dF, double *d2F, int iadd) {
+    if (is_per(c)) {
+        /* D2FDX2 src/derivCDopt6_periodic.f:270-392: dF by DFDX when iadd = 1 */
+        if (iadd == 1) per_line_op(c, d, PER_D1, F, dF, 0, 1.0);
+        per_line_op(c, d, PER_D2OP, F, d2F, 0, 1.0);
+        return;
+    }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
     double fac = ((double)((n - 1) * (n - 1))) * c->s2[d];
@@ -413,6 +573,7 @@ void orc_d2fd2(orc *c, int d, int asym, const double *F, double *dF, double *d2F
 /* Compact_Filter_X_sym src/filters_sym.f:436-634 / Compact_Filter_X_asym
  * src/filters_asym.f:388-583 and y/z twins */
 void orc_filter(orc *c, int d, int asym, const double *F, double *F0) {
+    if (is_per(c)) { per_line_op(c, d, PER_FILT, F, F0, 0, 1.0); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
     const struct bndyc *b = &c->bc;
@@ -476,6 +637,7 @@ void orc_compact_filter(orc *c, const double *F, double *F0, int nvar) {
 
 /* Gaussian_Filter_X src/filters_sym.f:1076-1219 and Y/Z :1222-1554 */
 void orc_gauss(orc *c, int d, const double *F, double *Fg) {
+    if (is_per(c)) { per_line_op(c, d, PER_GAUSS, F, Fg, 0, 1.0); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
     double a0 = c->ag[0], a1 = c->ag[1], a2 = c->ag[2], a3 = c->ag[3], a4 = c->ag[4];
@@ -1010,7 +1172,9 @@ static void rhs_yz(orc *c, double *Q, double *Ux, double *Qrhs, const double *Y,
         Q2[p] = Q2[p] * Q4[p];
         Q3[p] = Q3[p] * Q4[p];
     }
-    if (c->p.re > 0.0) {
+    /* src/rhsv_sym_mf.f:1420-1424 adds Qvisc only when Re > 0;
+     * src/rhsv_periodic_sf.f:1381 always adds it */
+    if (c->p.re > 0.0 || c->p.family == ST_FAMILY_PERIODIC) {
         PAR FOR_P for (int l = 0; l < 5; l++) {
             size_t q = l * n3 + p;
             Qrhs[q] = Qrhs[q] + Qcx[q] + Qcy[q] + Qcz[q] + Qv[q];
@@ -1027,6 +1191,7 @@ static void rhs_yz(orc *c, double *Q, double *Ux, double *Qrhs, const double *Y,
 
 /* RHS src/rhsv_sym_mf.f:9-26 */
 void orc_rhs(orc *c, double *Q, double *Qrhs, const double *Y) {
+    if (!Y) Y = c->Y;   /* the periodic single-fluid routines take no Y */
     size_t n3 = c->n3;
     double *Ux = dalloc(5 * n3), *Qcx = dalloc(5 * n3), *Qcy = dalloc(5 * n3), *Qcz = dalloc(5 * n3),
            *Qv = dalloc(5 * n3);
@@ -1041,6 +1206,15 @@ void orc_rhs(orc *c, double *Q, double *Qrhs, const double *Y) {
 static void laplacian(orc *c, const double *S, double *d2S) {
     size_t n3 = c->n3;
     double *dS = NEWF(c), *t1 = NEWF(c), *t2 = NEWF(c);
+    if (is_per(c)) {
+        /* Compute_Laplacian src/hyper_dynamic.f:41-58 */
+        orc_d2fd2(c, 0, 0, S, dS, t1, 0);
+        orc_d2fd2(c, 1, 0, S, dS, t2, 0);
+        orc_d2fd2(c, 2, 0, S, dS, d2S, 0);
+        PAR FOR_P d2S[p] = d2S[p] + t1[p] + t2[p];
+        free(dS); free(t1); free(t2);
+        return;
+    }
     orc_dfd(c, 0, 0, S, dS, 0, 1.0);
     orc_dfd(c, 0, 1, dS, t1, 0, 1.0);
     orc_dfd(c, 1, 0, S, dS, 0, 1.0);
@@ -1051,9 +1225,85 @@ static void laplacian(orc *c, const double *S, double *d2S) {
     free(dS); free(t1); free(t2);
 }
 
+/* Compute_hyper of the periodic single-fluid family, src/hyper_dynamic.f:
+ * Compute_coeff1 :72-165 (vorticity and dilatation from periodic first
+ * derivatives of u), Compute_hyper :173-321 (Laplacians by D2FD*2 :41-58,
+ * three Gaussian-filtered fields, coefficients applied after the filter). */
+static void compute_hyper_sf(orc *c, const double *Q) {
+    size_t n3 = c->n3;
+    const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
+    double **G = c->grad;
+    const double gam = c->p.gamma1;
+    double *U = dalloc(3 * n3), *Gr = dalloc(4 * n3), *tmp = NEWF(c), *Cbeta = NEWF(c);
+    /* Compute_coeff1 */
+    PAR FOR_P {
+        double t = 1.0 / Q4[p];
+        U[p] = Q1[p] * t; U[n3 + p] = Q2[p] * t; U[2 * n3 + p] = Q3[p] * t;
+    }
+    orc_dfd(c, 1, 0, U + 2 * n3, Gr, 0, 1.0);
+    orc_dfd(c, 2, 0, U + n3, Gr, 1, -1.0);
+    orc_dfd(c, 0, 0, U + 2 * n3, Gr + n3, 0, -1.0);
+    orc_dfd(c, 2, 0, U, Gr + n3, 1, 1.0);
+    orc_dfd(c, 0, 0, U + n3, Gr + 2 * n3, 0, 1.0);
+    orc_dfd(c, 1, 0, U, Gr + 2 * n3, 1, -1.0);
+    orc_dfd(c, 0, 0, U, Gr + 3 * n3, 0, 1.0);
+    orc_dfd(c, 1, 0, U + n3, tmp, 0, 1.0);
+    PAR FOR_P Gr[3 * n3 + p] = Gr[3 * n3 + p] + tmp[p];
+    orc_dfd(c, 2, 0, U + 2 * n3, tmp, 0, 1.0);
+    PAR FOR_P Gr[3 * n3 + p] = Gr[3 * n3 + p] + tmp[p];
+    double scale = c->p.c_beta_scale;
+    PAR FOR_P {
+        double eps = 1.0e-7, fac2 = 10.0;
+        double G1 = Gr[p], G2 = Gr[n3 + p], G3 = Gr[2 * n3 + p], G4 = Gr[3 * n3 + p];
+        double fac = 5.0e-1 * (1.0 - tanh(2.5 + fac2 * G4));
+        double om2 = G1 * G1 + G2 * G2 + G3 * G3;
+        Cbeta[p] = (fac * G4 * G4 / (G4 * G4 + om2 + eps) + 1.0e-20) * scale;
+    }
+    const double C_mu = 2.0e-3, C_k = 1.0e-2;
+    /* strain magnitude, P, T, e */
+    double *S = NEWF(c), *e = NEWF(c), *P = NEWF(c), *T = NEWF(c), *Vs = NEWF(c);
+    double *d2 = NEWF(c), *d4S = NEWF(c), *d4e = NEWF(c);
+    double fac1 = gam - 1.0, fac2 = gam / fac1;
+    PAR FOR_P {
+        double s1 = G[G_DUX_DX][p], s5 = G[G_DUY_DY][p], s9 = G[G_DUZ_DZ][p];
+        double s2 = 5.0e-1 * (G[G_DUX_DY][p] + G[G_DUY_DX][p]);
+        double s3 = 5.0e-1 * (G[G_DUX_DZ][p] + G[G_DUZ_DX][p]);
+        double s6 = 5.0e-1 * (G[G_DUY_DZ][p] + G[G_DUZ_DY][p]);
+        double s4 = s2, s7 = s3, s8 = s6;
+        Vs[p] = 1.0 / Q4[p];
+        P[p] = fac1 * (Q5[p] - 5.0e-1 * Vs[p] * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+        T[p] = fac2 * Vs[p] * P[p];
+        e[p] = Vs[p] * (Q5[p] - 5.0e-1 * Vs[p] * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+        S[p] = sqrt(5.0e-1 * (s1 * s1 + s5 * s5 + s9 * s9 + 2.0 * (s2 * s4 + s3 * s7 + s6 * s8)));
+    }
+    laplacian(c, S, d2);
+    laplacian(c, d2, d4S);
+    laplacian(c, e, d2);
+    laplacian(c, d2, d4e);
+    PAR FOR_P { d4S[p] = fabs(d4S[p]); d4e[p] = fabs(d4e[p]); }
+    double *eta = dalloc(3 * n3), *etag = dalloc(3 * n3);
+    PAR FOR_P {
+        double fac3 = (Q4[p] / T[p]) * sqrt(gam * P[p] * Vs[p]);
+        eta[p] = Q4[p] * d4S[p];
+        eta[2 * n3 + p] = Q4[p] * d4S[p];
+        eta[n3 + p] = fac3 * d4e[p];
+    }
+    orc_gaussian_filter(c, eta, etag, 3);
+    double DX6 = pow(c->DX, 6.0), DX5 = pow(c->DX, 5.0);
+    PAR FOR_P {
+        c->hyp[H_BETA][p] = Cbeta[p] * etag[2 * n3 + p] * DX6;
+        c->hyp[H_VISC][p] = C_mu * etag[p] * DX6;
+        c->hyp[H_K][p] = C_k * etag[n3 + p] * DX5;
+    }
+    free(U); free(Gr); free(tmp); free(Cbeta); free(S); free(e); free(P); free(T); free(Vs);
+    free(d2); free(d4S); free(d4e); free(eta); free(etag);
+}
+
 /* Compute_hyper src/hyper_dynamic_sym_mf.f:166-334 with Compute_coeff1
  * :79-158 and Compute_Contraction :12-33 */
 void orc_compute_hyper(orc *c, const double *Q, const double *Y) {
+    if (!Y) Y = c->Y;   /* the periodic single-fluid routines take no Y */
+    if (is_per(c)) { compute_hyper_sf(c, Q); return; }
     size_t n3 = c->n3;
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     double **G = c->grad;
@@ -1123,6 +1373,7 @@ void orc_compute_hyper(orc *c, const double *Q, const double *Y) {
 
 /* Hyper_RHS src/hyper_rhs_sym_mf.f:12-500 */
 void orc_hyper_rhs(orc *c, const double *Q, double *Qrhs, const double *Y) {
+    if (!Y) Y = c->Y;   /* the periodic single-fluid routines take no Y */
     if (c->p.hyper_param == 0) return;
     size_t n3 = c->n3;
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
@@ -1359,11 +1610,13 @@ void orc_sponge_forcing(orc *c, const double *Q, double *Qrhs, const double *Y, 
 
 /* Fix_Pressure pproc/pproc_mf.f:190-233 */
 void orc_fix_pressure(orc *c, double *Q, const double *Y) {
+    if (!Y) Y = c->Y;   /* the periodic single-fluid routines take no Y */
     (void)Y;
     size_t n3 = c->n3;
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
-    double base_pressure = 0.71429;
+    /* Fix_Pressure of the periodic family, src/lddrk4_periodic_sf.f:436-473 */
+    double base_pressure = is_per(c) ? 0.71463 : 0.71429;
     PAR FOR_P {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
@@ -1395,7 +1648,43 @@ void orc_compute_cfl(orc *c, const double *Q, double *cfl_stab, double *cfl_resv
 }
 
 /* Compute_Tstep src/lddrk4_nonperiodic_mf.f:75-160 */
+/* Compute_Tstep of the periodic family, src/lddrk4_periodic_sf.f:74-145:
+ * hyperviscous limits from step 2 on, single-fluid temperature, and the
+ * factor 0.2 written as a default-REAL literal (float32). */
+static double compute_tstep_sf(orc *c, const double *Q, double cfl_resv, int step) {
+    size_t n3 = c->n3;
+    const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
+    double Tstep = c->p.cfl_cal / cfl_resv;
+    double del = c->DX, gam = c->p.gamma1;
+    double fac = gam * (gam - 1.0);
+    if (c->p.hyper_param == 1 && step > 1) {
+        double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY;
+        const double *vh = c->hyp[H_VISC], *bh = c->hyp[H_BETA], *kh = c->hyp[H_K];
+#pragma omp parallel for schedule(static) reduction(min : m3, m4, m5)
+        for (size_t p = 0; p < n3; p++) {
+            double tmp1 = 1.0 / Q4[p];
+            double tmp2 = sqrt(fac * tmp1 * (Q5[p] - 5.0e-1 * tmp1 * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p])));
+            double T = gam * tmp1 * (Q5[p] - 5.0e-1 * tmp1 * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+            double w3 = Q4[p] * pow(del, 2.0) / vh[p];
+            double w4 = Q4[p] * pow(del, 2.0) / bh[p];
+            double w5 = Q4[p] * pow(del * tmp2, 2.0) / ((kh[p]) * T);
+            if (w3 < m3) m3 = w3;
+            if (w4 < m4) m4 = w4;
+            if (w5 < m5) m5 = w5;
+        }
+        const double f02 = (double)0.2f;
+        double t = c->p.cfl_cal / cfl_resv;
+        double cand[3] = {f02 * m3, f02 * m4, f02 * m5};
+        for (int q = 0; q < 3; q++) if (cand[q] < t) t = cand[q];
+        Tstep = t;
+    }
+    c->Tstep = Tstep;
+    return Tstep;
+}
+
 double orc_compute_tstep(orc *c, const double *Q, const double *Y, double cfl_resv, int step) {
+    if (!Y) Y = c->Y;   /* the periodic single-fluid routines take no Y */
+    if (is_per(c)) return compute_tstep_sf(c, Q, cfl_resv, step);
     size_t n3 = c->n3;
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
@@ -1463,6 +1752,22 @@ static void monitors(orc *c) {
     c->mon[4] = csum(c, Q + 3 * n3) / N;
     /* Compute_Energy :265-278 */
     c->mon[5] = csum(c, Q + 4 * n3) / N;
+    if (is_per(c)) {
+        /* Compute_Entropy src/lddrk4_periodic_sf.f:268-300: fac1 is an
+         * undeclared (default REAL, float32) local; Entropy2 is not computed */
+        float fac1 = (float)(c->p.gamma1 - 1.0);
+        double gam = c->p.gamma1;
+        PAR FOR_P {
+            double Vs = 1.0 / Q[3 * n3 + p];
+            double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p];
+            double P = (double)fac1 * (Q[4 * n3 + p] - 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3));
+            tmp[p] = Q[3 * n3 + p] * log(P * pow(Vs, gam));
+        }
+        c->mon[6] = csum(c, tmp) / N;
+        c->mon[7] = 0.0;
+        free(tmp); free(tmp2);
+        return;
+    }
     /* Compute_Entropy :287-327 */
     PAR FOR_P {
         double fac1 = c->gamma_eff[p] - 1.0;
@@ -1478,8 +1783,49 @@ static void monitors(orc *c) {
     free(tmp); free(tmp2);
 }
 
+/* Second-loop coefficients of the commented-out HHM 4-6 scheme,
+ * src/header:267-276 (used by rk_mode 1 of the periodic family). */
+static const double alpha2_hhm[6] = {0.0, -4.4127377153877382565e-1, -1.073982008079781868e0,
+                                     -1.7063570791256758809e0, -2.7979293162682443056e0,
+                                     -4.0913537120919160454e0};
+static const double beta2_hhm[6] = {1.1584888181285561688e-1, 3.7287699051652864918e-1,
+                                    7.3795368921435295698e-1, 5.7981109366311039538e-1,
+                                    1.031284991300145194e0, 1.5e-1};
+
+/* LDDRK4 of the periodic family, src/lddrk4_periodic_sf.f:311-430:
+ * 5 stages with alpha1/beta1, then 6 stages with alpha2/beta2 (never
+ * assigned in the reference build: zero, rk_mode 0). */
+static void lddrk4_sf(orc *c, double *time, int *step) {
+    size_t n3 = c->n3;
+    double *Q = c->Q, *dQ = c->dQ, *QW = c->QW;
+    double *Qf = dalloc(5 * n3);
+    double dt = c->Tstep;
+    for (int loop = 0; loop < 2; loop++) {
+        memset(QW, 0, 5 * n3 * 8);
+        int ns = loop == 0 ? 5 : 6;
+        for (int K = 0; K < ns; K++) {
+            double al, be;
+            if (loop == 0) { al = alpha1_rk[K]; be = beta1_rk[K]; }
+            else if (c->p.rk_mode == 1) { al = alpha2_hhm[K]; be = beta2_hhm[K]; }
+            else { al = 0.0; be = 0.0; }
+            orc_rhs(c, Q, dQ, c->Y);
+            orc_hyper_rhs(c, Q, dQ, c->Y);
+            PAR for (size_t q = 0; q < 5 * n3; q++) QW[q] = al * QW[q] + dt * dQ[q];
+            PAR for (size_t q = 0; q < 5 * n3; q++) Q[q] = Q[q] + be * QW[q];
+            orc_compact_filter(c, Q, Qf, 5);
+            memcpy(Q, Qf, 5 * n3 * 8);
+            orc_fix_pressure(c, Q, c->Y);
+        }
+        *time = *time + dt;
+    }
+    *step = *step + 1;
+    monitors(c);
+    free(Qf);
+}
+
 /* LDDRK4 src/lddrk4_nonperiodic_mf.f:428-541 */
 void orc_lddrk4(orc *c, double *time, int *step) {
+    if (is_per(c)) { lddrk4_sf(c, time, step); return; }
     size_t n3 = c->n3;
     double *Q = c->Q, *dQ = c->dQ, *QW = c->QW, *Y = c->Y, *drYi = c->drYi, *rYW = c->rYW;
     double *rY = NEWF(c), *Qf = dalloc(5 * n3);
@@ -1536,7 +1882,7 @@ void orc_get_monitors(orc *c, double out[10]) {
 /* ---- state / COMMON access -------------------------------------------------- */
 void orc_set_state(orc *c, const double *Q, const double *Y) {
     memcpy(c->Q, Q, 5 * c->n3 * 8);
-    memcpy(c->Y, Y, c->n3 * 8);
+    if (Y && !is_per(c)) memcpy(c->Y, Y, c->n3 * 8);
     memset(c->QW, 0, 5 * c->n3 * 8); memset(c->dQ, 0, 5 * c->n3 * 8);
     memset(c->rYW, 0, c->n3 * 8); memset(c->drYi, 0, c->n3 * 8);
 }

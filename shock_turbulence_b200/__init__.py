@@ -3,5 +3,5 @@ stage update of the compact-difference shock-turbulence solver (two-species
 "_mf" family).  The compute path is ``libst_b200.so`` (CUDA, C ABI in
 include/st_b200.h); this package is its host-side mirror of the reference's
 subroutine interface."""
-from .params import StParams, default_params  # noqa: F401
+from .params import FAMILY_MF, FAMILY_PERIODIC, StParams, default_params, periodic_params  # noqa: F401
 from .api import Solver, StError  # noqa: F401

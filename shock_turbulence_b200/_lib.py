@@ -57,6 +57,9 @@ for _d in ("x", "y", "z"):
         SIGNATURES[f"st_d2fd{_d}2_{_s}"] = [_ctx, _dp, _dp, _dp, ctypes.c_int]
         SIGNATURES[f"st_compact_filter_{_d}_{_s}"] = [_ctx, _dp, _dp]
     SIGNATURES[f"st_gaussian_filter_{_d}"] = [_ctx, _dp, _dp]
+    SIGNATURES[f"st_df{_d.join(['d', ''])}"] = [_ctx, _dp, _dp, ctypes.c_int, ctypes.c_double]
+    SIGNATURES[f"st_d2fd{_d}2"] = [_ctx, _dp, _dp, _dp, ctypes.c_int]
+    SIGNATURES[f"st_compact_filter_{_d}"] = [_ctx, _dp, _dp]
 
 _RESTYPES = {"st_last_error": ctypes.c_char_p, "st_status_string": ctypes.c_char_p,
              "st_default_params": None}

@@ -63,6 +63,10 @@ class Solver:
     def _a(self, a, nf=1):
         return _addr(a, nf * self.n3)
 
+    def _y(self, Y):
+        """Mass-fraction argument: None (NULL) is allowed in the periodic family."""
+        return None if Y is None else self._a(Y)
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.st_destroy(self._h)
@@ -78,8 +82,8 @@ class Solver:
         return np.zeros(self.shape if n is None else (n,) + self.shape)
 
     # -- state and COMMON blocks -----------------------------------------
-    def set_state(self, Q, Y):
-        self._check(self.lib.st_set_state(self._h, self._a(Q, 5), self._a(Y)), "st_set_state")
+    def set_state(self, Q, Y=None):
+        self._check(self.lib.st_set_state(self._h, self._a(Q, 5), self._y(Y)), "st_set_state")
 
     def get_state(self, Q=None, Y=None):
         Q = self.field(5) if Q is None else Q
@@ -120,14 +124,14 @@ class Solver:
     def Compute_gamma(self, Y):
         self._check(self.lib.st_compute_gamma(self._h, self._a(Y)), "Compute_gamma")
 
-    def RHS(self, Q, Qrhs, Y):
-        self._check(self.lib.st_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y)), "RHS")
+    def RHS(self, Q, Qrhs, Y=None):
+        self._check(self.lib.st_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._y(Y)), "RHS")
 
-    def Compute_hyper(self, Q, Y):
-        self._check(self.lib.st_compute_hyper(self._h, self._a(Q, 5), self._a(Y)), "Compute_hyper")
+    def Compute_hyper(self, Q, Y=None):
+        self._check(self.lib.st_compute_hyper(self._h, self._a(Q, 5), self._y(Y)), "Compute_hyper")
 
-    def Hyper_RHS(self, Q, Qrhs, Y):
-        self._check(self.lib.st_hyper_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y)), "Hyper_RHS")
+    def Hyper_RHS(self, Q, Qrhs, Y=None):
+        self._check(self.lib.st_hyper_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._y(Y)), "Hyper_RHS")
 
     def Species_RHS(self, Q, Qrhs, Y, Yrhs):
         self._check(self.lib.st_species_rhs(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y),
@@ -141,8 +145,8 @@ class Solver:
         self._check(self.lib.st_sponge_forcing(self._h, self._a(Q, 5), self._a(Qrhs, 5), self._a(Y),
                                                self._a(Yrhs)), "Sponge_Forcing")
 
-    def Fix_Pressure(self, Q, Y):
-        self._check(self.lib.st_fix_pressure(self._h, self._a(Q, 5), self._a(Y)), "Fix_Pressure")
+    def Fix_Pressure(self, Q, Y=None):
+        self._check(self.lib.st_fix_pressure(self._h, self._a(Q, 5), self._y(Y)), "Fix_Pressure")
 
     def Compact_Filter(self, F, F0, N):
         self._check(self.lib.st_compact_filter(self._h, self._a(F, N), self._a(F0, N), N), "Compact_Filter")
@@ -158,7 +162,7 @@ class Solver:
 
     def Compute_Tstep(self, Q, Y, cfl_resv, step):
         t = ctypes.c_double()
-        self._check(self.lib.st_compute_tstep(self._h, self._a(Q, 5), self._a(Y), float(cfl_resv), int(step),
+        self._check(self.lib.st_compute_tstep(self._h, self._a(Q, 5), self._y(Y), float(cfl_resv), int(step),
                                               ctypes.byref(t)), "Compute_Tstep")
         return t.value
 
@@ -204,5 +208,9 @@ for _d in ("X", "Y", "Z"):
         setattr(Solver, f"D2FD{_d}2_{_s}", _make_line_op(f"st_d2fd{_d.lower()}2_{_s}", "d2"))
         setattr(Solver, f"Compact_Filter_{_d}_{_s}", _make_line_op(f"st_compact_filter_{_d.lower()}_{_s}", "f"))
     setattr(Solver, f"Gaussian_Filter_{_d}", _make_line_op(f"st_gaussian_filter_{_d.lower()}", "f"))
+    # periodic family (src/derivCDopt6_periodic.f, src/filters_periodic.f)
+    setattr(Solver, f"DFD{_d}", _make_line_op(f"st_dfd{_d.lower()}", "d1"))
+    setattr(Solver, f"D2FD{_d}2", _make_line_op(f"st_d2fd{_d.lower()}2", "d2"))
+    setattr(Solver, f"Compact_Filter_{_d}", _make_line_op(f"st_compact_filter_{_d.lower()}", "f"))
 
 __all__ = ["Solver", "StError", "StParams", "default_params"]

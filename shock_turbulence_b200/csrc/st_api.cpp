@@ -146,6 +146,7 @@ void st_default_params(st_params *p, int nx, int ny, int nz) {
     p->gamma1 = 1.4; p->gamma2 = 1.09; p->epsilon = 0.198265856; p->vis_exp = 0.76;
     p->bulk_ratio = 0.0; p->t_ratio = 1.0;
     p->hyper_param = 1; p->rk_mode = 0; p->cfl_cal = 0.5; p->c_beta_scale = 1.0; p->device = 0;
+    p->family = ST_FAMILY_MF;
 }
 
 int st_create(const st_params *p, st_ctx **out) {
@@ -154,6 +155,8 @@ int st_create(const st_params *p, st_ctx **out) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return ST_E_NODEVICE; }
     if (p->device < 0 || p->device >= ndev) return ST_E_ARG;
+    if (p->family != ST_FAMILY_MF && p->family != ST_FAMILY_PERIODIC) return ST_E_ARG;
+    if (p->rk_mode != 0 && p->rk_mode != 1) return ST_E_ARG;
     const int n[3] = {p->nx, p->ny, p->nz};
     for (int d = 0; d < 3; d++)
         if (n[d] % kLanes != 0 || n[d] < kLanes || choose_seg(n[d]) == 0) return ST_E_UNSUPPORTED;
@@ -185,6 +188,13 @@ int st_create(const st_params *p, st_ctx **out) {
     c->Re2_inv = p->re2 > 0.0 ? 1.0 / p->re2 : 0.0;
     c->Pr_inv = p->pr > 0.0 ? 1.0 / p->pr : 0.0;
     c->Sc_inv = p->sc > 0.0 ? 1.0 / p->sc : 0.0;
+    if (p->family == ST_FAMILY_PERIODIC) {
+        // Define_Param src/define_periodic_sf.f:178-189: one fluid, Re_inv = 1/Re.
+        // The shared RHS code sees Y = 1 and gamma_eff = gamma, for which the
+        // mixture expressions reduce exactly to the single-fluid ones.
+        c->Re1_inv = p->re > 0.0 ? 1.0 / p->re : 0.0;
+        c->Re2_inv = 0.0;
+    }
     fill_consts(c->k);
     if (build_tables(c) != ST_OK) return bail(ST_E_NOMEM, "tables");
     const size_t b = c->dm.n3 * sizeof(double);
@@ -199,6 +209,11 @@ int st_create(const st_params *p, st_ctx **out) {
          cudaMemset(c->dscal, 0, 16 * sizeof(double)) == cudaSuccess &&
          cudaMallocHost((void **)&c->hpinned, 16 * sizeof(double)) == cudaSuccess;
     if (!ok) { cudaGetLastError(); return bail(ST_E_NOMEM, "device allocation of the COMMON blocks failed"); }
+    if (p->family == ST_FAMILY_PERIODIC) {
+        if (dev_fill(c, c->gamma_eff, c->dm.n3, p->gamma1) != ST_OK || dev_fill(c, c->Y, c->dm.n3, 1.0) != ST_OK ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return bail(ST_E_CUDA, "initialising the single-fluid fields");
+    }
     *out = c;
     return ST_OK;
 }
@@ -231,11 +246,13 @@ int st_sync(st_ctx *c) {
 
 // ---- state -------------------------------------------------------------------
 int st_set_state(st_ctx *c, const double *Q, const double *Y) {
-    if (!Q || !Y) return ST_E_ARG;
+    if (!Q) return ST_E_ARG;
+    if (!Y && (!c || c->p.family != ST_FAMILY_PERIODIC)) return ST_E_ARG;
     API_BEGIN(c)
     const size_t b = c->dm.n3 * 8;
     ST_CUDA(c, cudaMemcpyAsync(c->Q, Q, 5 * b, cudaMemcpyDefault, c->stream));
-    ST_CUDA(c, cudaMemcpyAsync(c->Y, Y, b, cudaMemcpyDefault, c->stream));
+    // the periodic family has no species: its Y stays 1
+    if (c->p.family != ST_FAMILY_PERIODIC) ST_CUDA(c, cudaMemcpyAsync(c->Y, Y, b, cudaMemcpyDefault, c->stream));
     ST_CUDA(c, cudaMemsetAsync(c->QW, 0, 5 * b, c->stream));
     ST_CUDA(c, cudaMemsetAsync(c->dQ, 0, 5 * b, c->stream));
     ST_CUDA(c, cudaMemsetAsync(c->rYW, 0, b, c->stream));
@@ -359,8 +376,24 @@ int st_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *
 }
 
 // ---- derivatives and filters ------------------------------------------------
+// asym: 0 / 1 for the _sym / _asym routines of the _mf family, PER for the
+// periodic family's routines (no suffix).  Each family only has its own.
+static const int PER = 2;
+static int family_ok(st_ctx *c, int asym) {
+    const bool per = c->p.family == ST_FAMILY_PERIODIC;
+    if (per != (asym == PER))
+        return fail(c, ST_E_UNSUPPORTED, per ? "the periodic family has no _sym/_asym routines"
+                                             : "periodic routines need a ST_FAMILY_PERIODIC context");
+    return ST_OK;
+}
+#define FAMILY_CHECK(c, asym) \
+    do { int rc_ = family_ok(c, asym); if (rc_ != ST_OK) return rc_; } while (0)
+
 static int do_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
     if (!F || !dF || (iadd != 0 && iadd != 1)) return ST_E_ARG;
+    if (!c) return ST_E_ARG;
+    FAMILY_CHECK(c, asym);
+    if (asym == PER) asym = 0;
     API_BEGIN(c)
     Args a(c);
     double *dFd = a.map(dF, 1, iadd == 1, true);
@@ -371,6 +404,9 @@ static int do_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int
 }
 static int do_d2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
     if (!F || !d2F || (iadd && !dF)) return ST_E_ARG;
+    if (!c) return ST_E_ARG;
+    FAMILY_CHECK(c, asym);
+    if (asym == PER) asym = 0;
     API_BEGIN(c)
     Args a(c);
     const double *Fd = a.map(F, 1, true, false);
@@ -382,6 +418,9 @@ static int do_d2(st_ctx *c, int dir, int asym, const double *F, double *dF, doub
 }
 static int do_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
     if (!F || !F0) return ST_E_ARG;
+    if (!c) return ST_E_ARG;
+    FAMILY_CHECK(c, asym);
+    if (asym == PER) asym = 0;
     API_BEGIN(c)
     Args a(c);
     const double *Fd = a.map(F, 1, true, false);
@@ -425,6 +464,15 @@ int st_compact_filter_z_sym(st_ctx *c, const double *F, double *F0) { return do_
 int st_compact_filter_x_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 0, 1, F, F0); }
 int st_compact_filter_y_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 1, 1, F, F0); }
 int st_compact_filter_z_asym(st_ctx *c, const double *F, double *F0) { return do_filter(c, 2, 1, F, F0); }
+int st_dfdx(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 0, PER, F, dF, iadd, cadd); }
+int st_dfdy(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 1, PER, F, dF, iadd, cadd); }
+int st_dfdz(st_ctx *c, const double *F, double *dF, int iadd, double cadd) { return do_dfd(c, 2, PER, F, dF, iadd, cadd); }
+int st_d2fdx2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 0, PER, F, dF, d2F, iadd); }
+int st_d2fdy2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 1, PER, F, dF, d2F, iadd); }
+int st_d2fdz2(st_ctx *c, const double *F, double *dF, double *d2F, int iadd) { return do_d2(c, 2, PER, F, dF, d2F, iadd); }
+int st_compact_filter_x(st_ctx *c, const double *F, double *F0) { return do_filter(c, 0, PER, F, F0); }
+int st_compact_filter_y(st_ctx *c, const double *F, double *F0) { return do_filter(c, 1, PER, F, F0); }
+int st_compact_filter_z(st_ctx *c, const double *F, double *F0) { return do_filter(c, 2, PER, F, F0); }
 int st_gaussian_filter_x(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 0, F, Fg); }
 int st_gaussian_filter_y(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 1, F, Fg); }
 int st_gaussian_filter_z(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 2, F, Fg); }
@@ -453,8 +501,22 @@ int st_gaussian_filter(st_ctx *c, const double *F, double *Fg, int nvar) {
 }
 
 // ---- physics operators ---------------------------------------------------------
+// Y argument of the physics routines: required in the _mf family; the
+// periodic family's routines take none (pass NULL), and its Y field is 1.
+static bool y_missing(st_ctx *c, const void *Y) {
+    return !Y && (!c || c->p.family != ST_FAMILY_PERIODIC);
+}
+static int mf_only(st_ctx *c, const char *what) {
+    if (c && c->p.family == ST_FAMILY_PERIODIC)
+        return fail(c, ST_E_UNSUPPORTED, std::string(what) + " has no counterpart in the periodic family");
+    return ST_OK;
+}
+#define MF_ONLY(c, what) \
+    do { int rc_ = mf_only(c, what); if (rc_ != ST_OK) return rc_; } while (0)
+
 int st_compute_gamma(st_ctx *c, const double *Y) {
     if (!Y) return ST_E_ARG;
+    MF_ONLY(c, "Compute_gamma");
     API_BEGIN(c)
     Args a(c);
     ST_TRY(dev_compute_gamma(c, a.map(Y, 1, true, false)));
@@ -463,35 +525,35 @@ int st_compute_gamma(st_ctx *c, const double *Y) {
 }
 
 int st_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
-    if (!Q || !Qrhs || !Y) return ST_E_ARG;
+    if (!Q || !Qrhs || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
     double *Qd = a.map(Q, 5, true, true);
     double *Rd = a.map(Qrhs, 5, false, true);
-    const double *Yd = a.map(Y, 1, true, false);
+    const double *Yd = Y ? a.map(Y, 1, true, false) : c->Y;
     ST_TRY(dev_rhs(c, Qd, Rd, Yd));
     return a.finish();
     API_END(c)
 }
 
 int st_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
-    if (!Q || !Y) return ST_E_ARG;
+    if (!Q || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
     const double *Qd = a.map(Q, 5, true, false);
-    const double *Yd = a.map(Y, 1, true, false);
+    const double *Yd = Y ? a.map(Y, 1, true, false) : c->Y;
     ST_TRY(dev_compute_hyper(c, Qd, Yd));
     return a.finish();
     API_END(c)
 }
 
 int st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
-    if (!Q || !Qrhs || !Y) return ST_E_ARG;
+    if (!Q || !Qrhs || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
     const double *Qd = a.map(Q, 5, true, false);
     double *Rd = a.map(Qrhs, 5, true, true);
-    const double *Yd = a.map(Y, 1, true, false);
+    const double *Yd = Y ? a.map(Y, 1, true, false) : c->Y;
     ST_TRY(dev_hyper_rhs(c, Qd, Rd, Yd));
     return a.finish();
     API_END(c)
@@ -499,6 +561,7 @@ int st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
 
 int st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    MF_ONLY(c, "Species_RHS");
     API_BEGIN(c)
     Args a(c);
     const double *Qd = a.map(Q, 5, true, false);
@@ -513,6 +576,7 @@ int st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, do
 int st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs, double time) {
     (void)time;
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    MF_ONLY(c, "bc_RHS");
     API_BEGIN(c)
     Args a(c);
     double *Qd = a.map(Q, 5, true, true);
@@ -526,6 +590,7 @@ int st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs,
 
 int st_sponge_forcing(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
+    MF_ONLY(c, "Sponge_Forcing");
     API_BEGIN(c)
     Args a(c);
     const double *Qd = a.map(Q, 5, true, false);
@@ -558,11 +623,11 @@ int st_compute_cfl(st_ctx *c, const double *Q, double *cfl_stab, double *cfl_res
 }
 
 int st_compute_tstep(st_ctx *c, const double *Q, const double *Y, double cfl_resv, int step, double *tstep) {
-    if (!Q || !Y) return ST_E_ARG;
+    if (!Q || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
     const double *Qd = a.map(Q, 5, true, false);
-    const double *Yd = a.map(Y, 1, true, false);
+    const double *Yd = Y ? a.map(Y, 1, true, false) : c->Y;
     ST_TRY(dev_compute_tstep(c, Qd, Yd, step, false, cfl_resv));
     ST_CUDA(c, cudaMemcpyAsync(c->hpinned + 6, c->dscal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     ST_TRY(a.finish());

@@ -34,6 +34,7 @@ struct TriTab {
     const double *wf;   // [P][P]: carry into segment s = sum_{s'<s} wf[s'][s] * A_{s'}
     const double *wb;   // [P][P]: carry into segment s = sum_{s'>s} wb[s'][s] * B_{s'}
     int kf, kb;         // segments back/ahead whose carry weight is >= 1e-20
+    const double *cyc;  // periodic family: [n][2] corner correction (see st_tables.cpp), else null
 };
 
 // Same for the pentadiagonal systems of the compact filter
@@ -48,6 +49,7 @@ struct PenTab {
     const double *mf;        // [P][P][4]
     const double *mb;        // [P][P][4]
     int kf, kb;              // segments back/ahead whose carry weight is >= 1e-20
+    const double *cyc;       // periodic family: [n][4] corner correction, else null
 };
 
 enum TriKind { K_D1S = 0, K_D1A = 1, K_D2S = 2, K_D2A = 3 };
@@ -176,6 +178,7 @@ int dev_dfd_prod(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int ia
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd);
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0);
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg);
+int dev_fill(st_ctx *c, double *x, size_t n, double v);
 int dev_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C, double *R,
                     int n, int lot, int nper);
 int dev_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C,

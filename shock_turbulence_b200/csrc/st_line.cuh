@@ -59,16 +59,21 @@ __device__ __forceinline__ double prod_eval(const Prod &P, size_t i) {
     }
 }
 
-// rows a-H .. a+S+H-1 of this lane's line into v (rows clamped into the
-// line; clamped values are never used by the stencils)
+// row index of a halo row: wrapped around the line for periodic lines,
+// otherwise clamped into the line (clamped values are never used by the
+// stencils, whose boundary rows re-read what they need)
+__device__ __forceinline__ int halo_row(int row, int n, int cyc) {
+    return row < 0 ? (cyc ? row + n : 0) : (row > n - 1 ? (cyc ? row - n : n - 1) : row);
+}
+
+// rows a-H .. a+S+H-1 of this lane's line into v
 template <int S, int H, int OP>
 __device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const Prod &F, const ColMap &m, int lane,
-                                          int a, int n) {
+                                          int a, int n, int cyc) {
     const size_t p = m.base + (size_t)lane * m.lstride;
 #pragma unroll
     for (int q = 0; q < S + 2 * H; q++) {
-        int row = a - H + q;
-        row = row < 0 ? 0 : (row > n - 1 ? n - 1 : row);
+        int row = halo_row(a - H + q, n, cyc);
         v[q] = prod_eval<OP>(F, p + (size_t)row * m.rstride);
     }
 }
@@ -89,11 +94,42 @@ __device__ __forceinline__ void store_rows(const double (&r)[N], double *__restr
     }
 }
 
-// shared buffers for the segment end values of one solve
+// shared buffers for the segment end values of one solve, and the corner
+// values of a periodic line (rows 0, 1, n-2, n-1 of the banded solution)
 struct CarryBuf {
     double a[kMaxSeg][kLanes][2];
     double b[kMaxSeg][kLanes][2];
+    double cy[kLanes][4];
 };
+
+// ---- periodic lines: corner correction after the banded solve ------------
+// x_i = y_i - sum_k K_ik y_{j_k} with the corner rows j = {0, n-1} (K = 2,
+// tridiagonal) or {0, 1, n-2, n-1} (K = 4, pentadiagonal); the table holds
+// -K row-major.  The first and last segments publish the corner values; the
+// barrier also orders them after every read of the previous solve's cy.
+template <int S, int N, int KC>
+__device__ __forceinline__ void cyc_fix(double (&r)[N], const double *__restrict__ Kt, int s, int P, int lane,
+                                        CarryBuf &cb) {
+    if (KC == 2) {
+        if (s == 0) cb.cy[lane][0] = r[0];
+        if (s == P - 1) cb.cy[lane][1] = r[S - 1];
+    } else {
+        if (s == 0) { cb.cy[lane][0] = r[0]; cb.cy[lane][1] = r[1]; }
+        if (s == P - 1) { cb.cy[lane][2] = r[S - 2]; cb.cy[lane][3] = r[S - 1]; }
+    }
+    __syncthreads();
+    double y[KC];
+#pragma unroll
+    for (int k = 0; k < KC; k++) y[k] = cb.cy[lane][k];
+    const double *kr = Kt + (size_t)s * S * KC;
+#pragma unroll
+    for (int t = 0; t < S; t++) {
+        double v = r[t];
+#pragma unroll
+        for (int k = 0; k < KC; k++) v = fma(__ldg(kr + t * KC + k), y[k], v);
+        r[t] = v;
+    }
+}
 
 // ---- segmented constant-coefficient tridiagonal solve --------------------
 // Forward elimination r'_i = r_i - l_i r'_{i-1} and back substitution
@@ -235,14 +271,11 @@ __device__ __forceinline__ void ytile_store(const double *tile, double *__restri
     }
 }
 template <int S, int H>
-__device__ __forceinline__ void ytile_rows(double (&v)[S + 2 * H], const double *tile, int lane, int a, int n) {
+__device__ __forceinline__ void ytile_rows(double (&v)[S + 2 * H], const double *tile, int lane, int a, int n,
+                                           int cyc) {
     const double *p = tile + lane * (n + 1);
 #pragma unroll
-    for (int q = 0; q < S + 2 * H; q++) {
-        int row = a - H + q;
-        row = row < 0 ? 0 : (row > n - 1 ? n - 1 : row);
-        v[q] = p[row];
-    }
+    for (int q = 0; q < S + 2 * H; q++) v[q] = p[halo_row(a - H + q, n, cyc)];
 }
 template <int S, int N>
 __device__ __forceinline__ void ytile_put(double *tile, const double (&r)[N], int lane, int a, int n) {
@@ -252,16 +285,18 @@ __device__ __forceinline__ void ytile_put(double *tile, const double (&r)[N], in
 }
 
 // DFDX_sym/_asym RHS, src/derivCDopt6_sym_tri.f:458-514,
-// src/derivCDopt6_asym_tri.f:461-516  (H = 2)
+// src/derivCDopt6_asym_tri.f:461-516  (H = 2).  Periodic DFDX,
+// src/derivCDopt6_periodic.f:205-248: the interior formula on every row with
+// wrapped halos (its f(i+-3) weight c1 is zero for the FDL3DI set).
 template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
+__device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
                                        const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
         v[t] = fac * (K.b1 * (f(2) - f(-2)) + K.a1 * (f(1) - f(-1)));
     }
-    if (a < 2 || a + S > n - 2) {
+    if (!cyc && (a < 2 || a + S > n - 2)) {
 #pragma unroll
         for (int t = 0; t < S; t++) {
             const int i = a + t;
@@ -277,16 +312,18 @@ __device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int
 }
 
 // D2FDX2_sym/_asym RHS, src/derivCDopt6_sym_tri.f:587-645,
-// src/derivCDopt6_asym_tri.f:588-643  (H = 2)
+// src/derivCDopt6_asym_tri.f:588-643  (H = 2).  Periodic D2FDX2,
+// src/derivCDopt6_periodic.f:316-370, with zero f(i+-3) weight and centre
+// weight 2(a2+b2).
 template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int asym, double fac,
+__device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
                                        const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
         v[t] = fac * (K.b2 * (f(2) + f(-2)) + K.a2 * (f(1) + f(-1)) - K.c2 * f(0));
     }
-    if (a < 2 || a + S > n - 2) {
+    if (!cyc && (a < 2 || a + S > n - 2)) {
 #pragma unroll
         for (int t = 0; t < S; t++) {
             const int i = a + t;
@@ -303,17 +340,18 @@ __device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int
 }
 
 // Compact_Filter_X_sym/_asym RHS, src/filters_sym.f:483-616,
-// src/filters_asym.f:435-565  (H = 4)
+// src/filters_asym.f:435-565  (H = 4).  Periodic Compact_Filter_X,
+// src/filters_periodic.f:155-229: interior formula, wrapped halos.
 template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n, int asym, const Consts &K,
-                                           const RD &F) {
+__device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n, int asym, int cyc,
+                                           const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
         auto f = [&](int k) { return v[t + k + H]; };
         v[t] = K.fa4 * (f(4) + f(-4)) + K.fa3 * (f(3) + f(-3)) + K.fa2 * (f(2) + f(-2)) +
                K.fa1 * (f(1) + f(-1)) + K.fa0 * f(0);
     }
-    if (a < 4 || a + S > n - 4) {
+    if (!cyc && (a < 4 || a + S > n - 4)) {
 #pragma unroll
         for (int t = 0; t < S; t++) {
             const int i = a + t;
@@ -351,9 +389,10 @@ __device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n,
 }
 
 // Gaussian_Filter_X, src/filters_sym.f:1119-1212: explicit, symmetric low end,
-// last four points copied  (H = 4)
+// last four points copied  (H = 4).  Periodic family,
+// src/filters_periodic.f:601-675: interior formula, wrapped halos.
 template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, const Consts &K,
+__device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, int cyc, const Consts &K,
                                           const RD &F) {
     const double *g = K.ga;
 #pragma unroll
@@ -362,7 +401,7 @@ __device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, 
         v[t] = g[4] * (f(4) + f(-4)) + g[3] * (f(3) + f(-3)) + g[2] * (f(2) + f(-2)) + g[1] * (f(1) + f(-1)) +
                g[0] * f(0);
     }
-    if (a < 4 || a + S > n - 4) {
+    if (!cyc && (a < 4 || a + S > n - 4)) {
 #pragma unroll
         for (int t = 0; t < S; t++) {
             const int i = a + t;

@@ -1,0 +1,194 @@
+// st_linekern.cuh - the line-operator kernels (compact derivatives, compact
+// filter, Gaussian filter) and their launch dispatch, templated on the family:
+// CYC = false for the _mf family's bounded lines, CYC = true for periodic
+// lines (wrapped halos and the corner correction after the banded solve).
+// The two families are instantiated in separate translation units
+// (st_kernels.cu, st_kernels_cyc.cu) so that the bounded-line kernels keep
+// their register allocation.
+#pragma once
+#include <cfloat>
+#include "st_line.cuh"
+
+namespace st {
+
+struct LineArgs {
+    Prod F;
+    double *O1, *O2;
+    LineGeo geo;
+    int S, P;
+    double fac1, fac2;
+    int asym, iadd;
+    int cyc;            // periodic family: wrapped halos, corner correction (selects the CYC kernels)
+    TriTab t1, t2;
+    PenTab p;
+    Consts K;
+};
+
+// Every line kernel is instantiated for x/z lines (YT = false: direct
+// coalesced row accesses) and for y lines (YT = true: staged through a
+// shared [32][n+1] tile).
+#define LINE_PROLOGUE                                                                  \
+    __shared__ CarryBuf cb;                                                            \
+    extern __shared__ double tile[];                                                   \
+    const int lane = threadIdx.x & (kLanes - 1), s = threadIdx.x / kLanes, n = a.geo.n, row0 = s * S; \
+    const ColMap m = a.geo.map(blockIdx.x);                                            \
+    const RowReader<OP> rd = YT ? RowReader<OP>{tile + lane * (n + 1), nullptr, 0, 0}  \
+                                : RowReader<OP>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
+
+template <int S, int H, bool YT, int OP>
+__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const Prod &F,
+                                         const ColMap &m, int lane, int a, int n, int cyc) {
+    if (YT) ytile_rows<S, H>(v, tile, lane, a, n, cyc);
+    else load_rows<S, H, OP>(v, F, m, lane, a, n, cyc);
+}
+template <int S, bool YT, int N>
+__device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, double *O, const ColMap &m,
+                                         int lane, int a, int n, int add) {
+    if (YT) {
+        __syncthreads();                 // every thread has finished reading the tile
+        ytile_put<S>(tile, v, lane, a, n);
+        __syncthreads();
+        ytile_store(tile, O, m.base, n, add);
+    } else {
+        store_rows<S>(v, O, m, lane, a, add);
+    }
+}
+
+// DF*_sym/_asym and the periodic DF*: O1 (=|+=) cadd * dF/ds
+template <int S, bool YT, int OP, bool CYC>
+__global__ void __launch_bounds__(512, 2) k_dfd(LineArgs a) {
+    LINE_PROLOGUE
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 4];
+    get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
+    tri_solve<S>(v, a.t1, s, a.P, lane, cb);
+    if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd);
+}
+
+// D2F*2_sym/_asym and the periodic D2F*2: O2 = d2F/ds2; if iadd, O1 = dF/ds
+// (cadd = 1).  The first
+// derivative re-reads the rows (the CTA's lines are still in L2).
+template <int S, bool YT, bool CYC>
+__global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgs a) {
+    constexpr int OP = PR_A;
+    LINE_PROLOGUE
+    {
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+        double v[S + 4];
+        get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+        rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
+        tri_solve<S>(v, a.t2, s, a.P, lane, cb);
+        if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t2.cyc, s, a.P, lane, cb);
+        put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0);
+    }
+    if (a.iadd) {
+        __syncthreads();   // carry buffers and tile are reused
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+        double v[S + 4];
+        get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+        rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
+        tri_solve<S>(v, a.t1, s, a.P, lane, cb);
+        if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
+        put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+    }
+}
+
+// Compact_Filter_*_sym/_asym and the periodic Compact_Filter_*: O1 = filtered
+// F.  O1 may alias F: every read of
+// F (including the boundary re-reads) happens before the solve's first
+// barrier and every write after its last one.
+template <int S, bool YT, bool CYC>
+__global__ void __launch_bounds__(512, 2) k_filter(LineArgs a) {
+    constexpr int OP = PR_A;
+    LINE_PROLOGUE
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 8];
+    get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    rhs_filter<S, 4>(v, row0, n, a.asym, CYC, a.K, rd);
+    pen_solve<S>(v, a.p, s, a.P, lane, cb);
+    if constexpr (CYC) cyc_fix<S, S + 8, 4>(v, a.p.cyc, s, a.P, lane, cb);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+}
+
+// Gaussian_Filter_X/Y/Z (both families): O1 = explicit 9-point Gaussian of F
+// (O1 != F)
+template <int S, bool YT, bool CYC>
+__global__ void __launch_bounds__(512, 2) k_gauss(LineArgs a) {
+    constexpr int OP = PR_A;
+    LINE_PROLOGUE
+    (void)cb;
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    double v[S + 8];
+    get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    rhs_gauss<S, 4>(v, row0, n, CYC, a.K, rd);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+}
+
+enum OpKind { OP_D1, OP_D2, OP_FILTER, OP_GAUSS };
+
+// opt in to the dynamic shared memory a kernel needs on top of its static
+// carry buffers (the default cap is 48 KB in total); once per kernel and size
+template <auto Kern>
+static void set_smem(size_t bytes) {
+    static size_t done = 0;   // one counter per kernel instantiation
+    if (bytes > done) {
+        cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        done = bytes;
+    }
+}
+
+template <int S, bool YT, bool CYC>
+static void launch_SY(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
+    const size_t nlines = c->dm.n3 / (size_t)a.geo.n;
+    dim3 grid((unsigned)(nlines / kLanes)), block(kLanes * a.P);
+    const size_t smem = YT ? (size_t)kLanes * (a.geo.n + 1) * sizeof(double) : 0;
+    // algorithmic bytes: every input and output field touched once
+    const double n3 = (double)c->dm.n3;
+    // inputs: 1 field, or every field a producer expression reads
+    static const int nin[6] = {1, 2, 3, 3, 3, 4};
+    double b = 8.0 * nin[a.F.op] + 8.0;          // + one output
+    if (op == OP_D1 && a.iadd) b += 8.0;           // read-modify-write
+    if (op == OP_D2 && a.iadd) b += 8.0;           // second output
+    static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
+    int pi = prof_start(c, names[op], b * n3);
+    switch (op) {
+        case OP_D1:
+            switch (a.F.op) {
+#define PCASE(o_) case o_: set_smem<k_dfd<S, YT, o_, CYC>>(smem); k_dfd<S, YT, o_, CYC><<<grid, block, smem, st>>>(a); break;
+                PCASE(PR_A) PCASE(PR_MUL) PCASE(PR_ADDMUL) PCASE(PR_MULMUL) PCASE(PR_SPEC) PCASE(PR_SPECT)
+#undef PCASE
+            }
+            break;
+        case OP_D2: set_smem<k_d2fd2<S, YT, CYC>>(smem); k_d2fd2<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
+        case OP_FILTER: set_smem<k_filter<S, YT, CYC>>(smem); k_filter<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
+        case OP_GAUSS: set_smem<k_gauss<S, YT, CYC>>(smem); k_gauss<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
+    }
+    prof_stop(c, pi);
+}
+
+template <int S, bool CYC>
+static void launch_S(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
+    if (a.geo.dir == 1) launch_SY<S, true, CYC>(c, op, a, st);
+    else launch_SY<S, false, CYC>(c, op, a, st);
+}
+
+// all line-operator launches of one family (CYC: periodic lines)
+template <bool CYC>
+static int launch_line_t(st_ctx *c, OpKind op, const LineArgs &a) {
+    switch (a.S) {
+#define CASE(s_) case s_: launch_S<s_, CYC>(c, op, a, c->stream); break;
+        CASE(2) CASE(3) CASE(4) CASE(6) CASE(8) CASE(12) CASE(16)
+#undef CASE
+        default: return fail(c, ST_E_UNSUPPORTED, "unsupported line segmentation");
+    }
+    ST_CUDA(c, cudaGetLastError());
+    return ST_OK;
+}
+
+
+// periodic-line launches, instantiated in st_kernels_cyc.cu
+int launch_line_cyc(st_ctx *c, OpKind op, const LineArgs &a);
+
+}  // namespace st

@@ -77,6 +77,11 @@ struct ScratchN {
     double *operator[](int i) const { return f[i]; }
 };
 
+int dev_fill(st_ctx *c, double *x, size_t n, double v) {
+    PFOR(c, n, { x[p] = v; });
+    return ST_OK;
+}
+
 int dev_compute_gamma(st_ctx *c, const double *Y) {
     Phys f = phys(c);
     double *ge = c->gamma_eff;
@@ -106,7 +111,8 @@ int dev_compute_gamma(st_ctx *c, const double *Y) {
 int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     const size_t n3 = c->dm.n3;
     const Phys f = phys(c);
-    const bool visc = c->p.re > 0.0;
+    // src/rhsv_periodic_sf.f:1381 adds Qvisc unconditionally
+    const bool visc = c->p.re > 0.0 || c->p.family == ST_FAMILY_PERIODIC;
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     double *Gxx = c->grad[G_DUX_DX], *Gyx = c->grad[G_DUY_DX], *Gzx = c->grad[G_DUZ_DX];
     double *Gxy = c->grad[G_DUX_DY], *Gyy = c->grad[G_DUY_DY], *Gzy = c->grad[G_DUZ_DY];
@@ -320,6 +326,14 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
 static int laplacian(st_ctx *c, const double *S, double *d2S) {
     Scratch dS(c), t1(c), t2(c);
     double *pt1 = t1, *pt2 = t2;
+    if (c->p.family == ST_FAMILY_PERIODIC) {
+        // Compute_Laplacian src/hyper_dynamic.f:41-58 (second derivatives)
+        ST_TRY(dev_d2fd2(c, 0, 0, S, nullptr, t1, 0));
+        ST_TRY(dev_d2fd2(c, 1, 0, S, nullptr, t2, 0));
+        ST_TRY(dev_d2fd2(c, 2, 0, S, nullptr, d2S, 0));
+        PFOR(c, c->dm.n3, { d2S[p] = d2S[p] + pt1[p] + pt2[p]; });
+        return ST_OK;
+    }
     ST_TRY(dev_dfd(c, 0, 0, S, dS, 0, 1.0));
     ST_TRY(dev_dfd(c, 0, 1, dS, t1, 0, 1.0));
     ST_TRY(dev_dfd(c, 1, 0, S, dS, 0, 1.0));
@@ -332,7 +346,82 @@ static int laplacian(st_ctx *c, const double *S, double *d2S) {
 
 // Compute_hyper src/hyper_dynamic_sym_mf.f:166-334 (+ Compute_coeff1 :79-158,
 // Compute_Contraction :12-33)
+// Compute_hyper of the periodic single-fluid family, src/hyper_dynamic.f:
+// Compute_coeff1 :72-165 forms vorticity and dilatation from periodic first
+// derivatives of u (the dilatation sums Grad4 + temp are the iadd
+// accumulations of the derivative kernels), Compute_hyper :173-321 filters
+// eta = (rho|d4S|, fac3|d4e|, rho|d4S|) and applies the coefficients after the
+// filter.  The third field equals the first, so its filtered value is the
+// first one's (same input, same arithmetic) and is filtered once.
+static int compute_hyper_sf(st_ctx *c, const double *Q) {
+    const size_t n3 = c->dm.n3;
+    const double gam = c->p.gamma1;
+    const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
+    ScratchN s(c, 14);
+    double *U1 = s[0], *U2 = s[1], *U3 = s[2], *W1 = s[3], *W2 = s[4], *W3 = s[5], *Dl = s[6];
+    double *Cbeta = s[7], *S = s[8], *e = s[9], *T = s[10], *d2 = s[11], *d4S = s[12], *d4e = s[13];
+    PFOR(c, n3, {
+        double t = 1.0 / Q4[p];
+        U1[p] = Q1[p] * t; U2[p] = Q2[p] * t; U3[p] = Q3[p] * t;
+    });
+    ST_TRY(dev_dfd(c, 1, 0, U3, W1, 0, 1.0));
+    ST_TRY(dev_dfd(c, 2, 0, U2, W1, 1, -1.0));
+    ST_TRY(dev_dfd(c, 0, 0, U3, W2, 0, -1.0));
+    ST_TRY(dev_dfd(c, 2, 0, U1, W2, 1, 1.0));
+    ST_TRY(dev_dfd(c, 0, 0, U2, W3, 0, 1.0));
+    ST_TRY(dev_dfd(c, 1, 0, U1, W3, 1, -1.0));
+    ST_TRY(dev_dfd(c, 0, 0, U1, Dl, 0, 1.0));
+    ST_TRY(dev_dfd(c, 1, 0, U2, Dl, 1, 1.0));
+    ST_TRY(dev_dfd(c, 2, 0, U3, Dl, 1, 1.0));
+    const double *G0 = c->grad[0], *G1 = c->grad[1], *G2 = c->grad[2], *G3 = c->grad[3], *G4 = c->grad[4],
+                 *G5 = c->grad[5], *G6 = c->grad[6], *G7 = c->grad[7], *G8 = c->grad[8];
+    const double scale = c->p.c_beta_scale;
+    double *P = U1, *Vs = U2;   // the velocities are dead from here on
+    PFOR(c, n3, {
+        double eps = 1.0e-7, fac2 = 10.0;
+        double dil = Dl[p];
+        double fac = 5.0e-1 * (1.0 - tanh(2.5 + fac2 * dil));
+        double om2 = W1[p] * W1[p] + W2[p] * W2[p] + W3[p] * W3[p];
+        Cbeta[p] = (fac * dil * dil / (dil * dil + om2 + eps) + 1.0e-20) * scale;
+        double s1 = G0[p], s5 = G4[p], s9 = G8[p];
+        double s2 = 5.0e-1 * (G3[p] + G1[p]);
+        double s3 = 5.0e-1 * (G6[p] + G2[p]);
+        double s6 = 5.0e-1 * (G7[p] + G5[p]);
+        double s4 = s2, s7 = s3, s8 = s6;
+        double fac1 = gam - 1.0, fac2t = gam / fac1;
+        double vs = 1.0 / Q4[p];
+        double pp = fac1 * (Q5[p] - 5.0e-1 * vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+        Vs[p] = vs;
+        P[p] = pp;
+        T[p] = fac2t * vs * pp;
+        e[p] = vs * (Q5[p] - 5.0e-1 * vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+        S[p] = sqrt(5.0e-1 * (s1 * s1 + s5 * s5 + s9 * s9 + 2.0 * (s2 * s4 + s3 * s7 + s6 * s8)));
+    });
+    ST_TRY(laplacian(c, S, d2));
+    ST_TRY(laplacian(c, d2, d4S));
+    ST_TRY(laplacian(c, e, d2));
+    ST_TRY(laplacian(c, d2, d4e));
+    Scratch etas(c, 4);
+    double *eta = etas, *etag = eta + 2 * n3;   // [rho|d4S|, fac3|d4e|] and their filtered values
+    PFOR(c, n3, {
+        double fac3 = (Q4[p] / T[p]) * sqrt(gam * P[p] * Vs[p]);
+        eta[p] = Q4[p] * fabs(d4S[p]);
+        eta[n3 + p] = fac3 * fabs(d4e[p]);
+    });
+    ST_TRY(dev_gaussian_filter(c, eta, etag, 2));
+    const double DX6 = pow(c->DX, 6.0), DX5 = pow(c->DX, 5.0);
+    const double C_mu = 2.0e-3, C_k = 1.0e-2;
+    double *hb = c->hyp[H_BETA], *hv = c->hyp[H_VISC], *hk = c->hyp[H_K];
+    PFOR(c, n3, {
+        hb[p] = Cbeta[p] * etag[p] * DX6;
+        hv[p] = C_mu * etag[p] * DX6;
+        hk[p] = C_k * etag[n3 + p] * DX5;
+    });
+    return ST_OK;
+}
+
 int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
+    if (c->p.family == ST_FAMILY_PERIODIC) return compute_hyper_sf(c, Q);
     const size_t n3 = c->dm.n3;
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
@@ -597,16 +686,18 @@ int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double
     return ST_OK;
 }
 
-// Fix_Pressure pproc/pproc_mf.f:190-233
+// Fix_Pressure pproc/pproc_mf.f:190-233; periodic family
+// src/lddrk4_periodic_sf.f:436-473 (base pressure 0.71463, gamma_eff = gamma)
 int dev_fix_pressure(st_ctx *c, double *Q) {
     const size_t n3 = c->dm.n3;
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
+    const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
     PFOR(c, n3, {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
-        if (P < 0.0) P = 0.71429;
+        if (P < 0.0) P = base;
         Q5[p] = (1.0 / fac1) * P + 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]);
     });
     return ST_OK;
@@ -699,12 +790,40 @@ __global__ void k_tstep(const double *Q, const double *Y, const double *g, const
     }
 }
 
-// dt = min(cfl_cal/cfl_resv, 0.2*minima) -> out[6]; resv taken from out[1]
-__global__ void k_tstep_final(double *out, double cfl_cal, int use_hyper, int resv_dev, double resv_host) {
+// Compute_Tstep of the periodic family, src/lddrk4_periodic_sf.f:105-135:
+// single-fluid temperature, no diffusivity limit (out[5] stays +inf)
+__global__ void k_tstep_sf(const double *Q, const double *vh, const double *bh, const double *kh, size_t n3,
+                           double del, double gam, double *out) {
+    double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY;
+    const double fac = gam * (gam - 1.0);
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
+        double tmp1 = 1.0 / Q[3 * n3 + p];
+        double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p], q5 = Q[4 * n3 + p];
+        double tmp2 = sqrt(fac * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3)));
+        double T = gam * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3));
+        double w3 = q4 * pow(del, 2.0) / vh[p];
+        double w4 = q4 * pow(del, 2.0) / bh[p];
+        double w5 = q4 * pow(del * tmp2, 2.0) / ((kh[p]) * T);
+        m3 = fmin(m3, w3); m4 = fmin(m4, w4); m5 = fmin(m5, w5);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m3 = fmin(m3, __shfl_down_sync(0xffffffffu, m3, o));
+        m4 = fmin(m4, __shfl_down_sync(0xffffffffu, m4, o));
+        m5 = fmin(m5, __shfl_down_sync(0xffffffffu, m5, o));
+    }
+    if ((threadIdx.x & 31) == 0) { atomic_min_pos(out + 2, m3); atomic_min_pos(out + 3, m4); atomic_min_pos(out + 4, m5); }
+}
+
+// dt = min(cfl_cal/cfl_resv, f*minima) -> out[6]; resv taken from out[1].
+// f is 0.2D0 in src/lddrk4_nonperiodic_mf.f:156-157 and the default-REAL
+// literal 0.2 (float32) in src/lddrk4_periodic_sf.f:141-142; out[5] = +inf
+// when a limit is absent.
+__global__ void k_tstep_final(double *out, double cfl_cal, int use_hyper, int resv_dev, double resv_host,
+                              double f) {
     double resv = resv_dev ? out[1] : resv_host;
     double t = cfl_cal / resv;
     if (use_hyper) {
-        double cand[4] = {0.2 * out[2], 0.2 * out[3], 0.2 * out[4], 0.2 * out[5]};
+        double cand[4] = {f * out[2], f * out[3], f * out[4], f * out[5]};
         for (int q = 0; q < 4; q++) if (cand[q] < t) t = cand[q];
     }
     out[6] = t;
@@ -737,21 +856,32 @@ int dev_compute_cfl(st_ctx *c, const double *Q, bool to_host, double *stab, doub
 // when the caller asks for it.
 int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, bool resv_on_device,
                       double cfl_resv_host) {
-    const bool use_hyper = c->p.hyper_param == 1 && step > 0;
+    const bool sf = c->p.family == ST_FAMILY_PERIODIC;
+    // hyperviscous limits from the first step on (_mf) or the second (periodic)
+    const bool use_hyper = c->p.hyper_param == 1 && step > (sf ? 1 : 0);
     if (use_hyper) {
         const double inf = INFINITY;
         double init[4] = {inf, inf, inf, inf};
         ST_CUDA(c, cudaMemcpyAsync(c->dscal + 2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
-        int pi = prof_start(c, "k_tstep", 88.0 * c->dm.n3);
-        k_tstep<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(
-            Q, Y, c->gamma_eff, c->hyp[H_VISC], c->hyp[H_BETA], c->hyp[H_K], c->hyp[H_D], c->dm.n3, c->DX,
-            c->p.gamma1, c->p.gamma2, c->p.epsilon, c->dscal);
-        prof_stop(c, pi);
+        if (sf) {
+            int pi = prof_start(c, "k_tstep", 64.0 * c->dm.n3);
+            k_tstep_sf<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, c->hyp[H_VISC], c->hyp[H_BETA],
+                                                                    c->hyp[H_K], c->dm.n3, c->DX,
+                                                                    c->p.gamma1, c->dscal);
+            prof_stop(c, pi);
+        } else {
+            int pi = prof_start(c, "k_tstep", 88.0 * c->dm.n3);
+            k_tstep<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(
+                Q, Y, c->gamma_eff, c->hyp[H_VISC], c->hyp[H_BETA], c->hyp[H_K], c->hyp[H_D], c->dm.n3, c->DX,
+                c->p.gamma1, c->p.gamma2, c->p.epsilon, c->dscal);
+            prof_stop(c, pi);
+        }
         ST_CUDA(c, cudaGetLastError());
     }
     c->launches++;
+    const double f = sf ? (double)0.2f : 0.2;
     k_tstep_final<<<1, 1, 0, c->stream>>>(c->dscal, c->p.cfl_cal, use_hyper ? 1 : 0, resv_on_device ? 1 : 0,
-                                          cfl_resv_host);
+                                          cfl_resv_host, f);
     ST_CUDA(c, cudaGetLastError());
     return ST_OK;
 }
@@ -763,7 +893,61 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
 // first stage, whose coefficient alpha(1) is 0 (0*0 + dt*dQ == dt*dQ); the
 // last filter pass of each conserved variable writes Q itself (Q = Qf), and
 // Compute_Y is fused with Fix_Pressure.
+// LDDRK4 of the periodic family, src/lddrk4_periodic_sf.f:311-430: 5 stages
+// with alpha1/beta1, then 6 with alpha2/beta2 (unassigned in the reference
+// build, i.e. zero: rk_mode 0; rk_mode 1 takes the commented-out HHM 4-6
+// values of src/header:267-276).  Each stage: RHS, Hyper_RHS, update,
+// Compact_Filter (Q = Qf), Fix_Pressure.
+static int lddrk4_sf(st_ctx *c) {
+    static const double alpha1[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
+                                     -2.016477077503357e+00, -1.056444269767207e+00};
+    static const double beta1[5] = {1.028639988104959e-01, 7.408540575766301e-01, 7.426530946683799e-01,
+                                    4.694937902357905e-01, 1.881733382887932e-01};
+    static const double alpha2[6] = {0.0, -4.4127377153877382565e-1, -1.073982008079781868e0,
+                                     -1.7063570791256758809e0, -2.7979293162682443056e0,
+                                     -4.0913537120919160454e0};
+    static const double beta2[6] = {1.1584888181285561688e-1, 3.7287699051652864918e-1,
+                                    7.3795368921435295698e-1, 5.7981109366311039538e-1,
+                                    1.031284991300145194e0, 1.5e-1};
+    const size_t n3 = c->dm.n3;
+    Scratch Qfs(c, 5);
+    double *Qf = Qfs;
+    const double *dtp = c->dscal + 6;
+    double *timep = c->dscal + 7;
+    for (int loop = 0; loop < 2; loop++) {
+        const int ns = loop == 0 ? 5 : 6;
+        for (int K = 0; K < ns; K++) {
+            double al, be;
+            if (loop == 0) { al = alpha1[K]; be = beta1[K]; }
+            else if (c->p.rk_mode == 1) { al = alpha2[K]; be = beta2[K]; }
+            else { al = 0.0; be = 0.0; }
+            const bool first = K == 0;
+            double *Q = c->Q, *dQ = c->dQ, *QW = c->QW;
+            ST_TRY(dev_rhs(c, Q, dQ, c->Y));
+            ST_TRY(dev_hyper_rhs(c, Q, dQ, c->Y));
+            PFOR(c, n3, {
+                double dt = *dtp;
+                for (int l = 0; l < 5; l++) {
+                    size_t q = l * n3 + p;
+                    double qw = first ? dt * dQ[q] : al * QW[q] + dt * dQ[q];
+                    QW[q] = qw;
+                    Q[q] = Q[q] + be * qw;
+                }
+            });
+            for (int l = 0; l < 5; l++) {
+                ST_TRY(dev_filter(c, 0, 0, Q + l * n3, Qf + l * n3));
+                ST_TRY(dev_filter(c, 1, 0, Qf + l * n3, Qf + l * n3));
+                ST_TRY(dev_filter(c, 2, 0, Qf + l * n3, Q + l * n3));
+            }
+            ST_TRY(dev_fix_pressure(c, Q));
+        }
+        PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
+    }
+    return ST_OK;
+}
+
 int dev_lddrk4(st_ctx *c, bool) {
+    if (c->p.family == ST_FAMILY_PERIODIC) return lddrk4_sf(c);
     static const double alpha1[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
                                      -2.016477077503357e+00, -1.056444269767207e+00};
     static const double beta1[5] = {1.028639988104959e-01, 7.408540575766301e-01, 7.426530946683799e-01,
@@ -825,7 +1009,9 @@ int dev_lddrk4(st_ctx *c, bool) {
 }
 
 // monitoring sums (Compute_Mom/KE/Mass/Energy/Entropy), two-pass block sums
-__global__ void k_monitor_partial(const double *Q, const double *g, size_t n3, double *part) {
+// sf: periodic family, whose Compute_Entropy (src/lddrk4_periodic_sf.f:268-300)
+// holds gamma - 1 in an undeclared (float32) local and skips Entropy2
+__global__ void k_monitor_partial(const double *Q, const double *g, size_t n3, double *part, int sf) {
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
         double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p], q5 = Q[4 * n3 + p];
@@ -835,11 +1021,11 @@ __global__ void k_monitor_partial(const double *Q, const double *g, size_t n3, d
         ke = ke + q4 * u1 * u1;
         ke = ke + q4 * u2 * u2;
         ke = ke + q4 * u3 * u3;
-        double fac1 = g[p] - 1.0;
+        double fac1 = sf ? (double)(float)(g[p] - 1.0) : g[p] - 1.0;
         double Vs = 1.0 / q4;
         double P = fac1 * (q5 - 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3));
         double s1 = q4 * log(P * pow(Vs, g[p]));
-        double s2 = q4 * s1 * s1;
+        double s2 = sf ? 0.0 : q4 * s1 * s1;
         acc[0] += ke; acc[1] += q1; acc[2] += q2; acc[3] += q3; acc[4] += q4; acc[5] += q5;
         acc[6] += s1; acc[7] += s2;
     }
@@ -860,7 +1046,8 @@ int dev_monitors(st_ctx *c) {
     Scratch parts(c);   // >= 8*nb doubles for every supported grid (n3 >= 32^3)
     double *part = parts;
     c->launches++;
-    k_monitor_partial<<<nb, 256, 0, c->stream>>>(c->Q, c->gamma_eff, c->dm.n3, part);
+    k_monitor_partial<<<nb, 256, 0, c->stream>>>(c->Q, c->gamma_eff, c->dm.n3, part,
+                                                 c->p.family == ST_FAMILY_PERIODIC ? 1 : 0);
     ST_CUDA(c, cudaGetLastError());
     std::vector<double> h(8 * nb);
     ST_CUDA(c, cudaMemcpyAsync(h.data(), part, 8 * nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -17,6 +17,7 @@
 // algorithm.
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include "st_internal.h"
 
@@ -99,6 +100,104 @@ static void filter_lhs(int n, int asym, std::vector<double> M[5]) {
     row(n - 3, 0, ab, 1, ab, 0);
     row(3, bf, af, 1, af, bf);
     row(n - 4, bf, af, 1, af, bf);
+}
+
+// Periodic family: the cyclic systems of src/derivCDopt6_periodic.f (first and
+// second derivative, solved with pentadiagonal(...,nper=1), i.e.
+// pentadiagonal_periodic_serial, src/pentadiagonal.f90:381-504) and of
+// src/filters_periodic.f:9-75 have constant rows (beta, alpha, 1, alpha, beta)
+// that wrap around the line.  They are solved as the banded (non-wrapping)
+// part, which the segmented solve handles like any other left-hand side, plus
+// a rank-k correction for the corner entries (Sherman-Morrison-Woodbury):
+//   A_cyc = A_band + U M V^T,  U = [e_j], V^T x = (x_j) for the k corner rows
+//   j = {0, n-1} (k = 2) or {0, 1, n-2, n-1} (k = 4),
+//   x = y - K (V^T y),  y = A_band^{-1} r,  K = Z (I + M V^T Z)^{-1} M,
+//   Z = A_band^{-1} U.
+// K is computed here in long double; the device adds -K (V^T y) after the
+// banded solve.  Both systems are symmetric positive definite Toeplitz
+// matrices (the filter's smallest eigenvalue is about 1.3e-3), so the banded
+// elimination needs no pivoting.
+static void band_rows(int n, double bt, double al, std::vector<double> M[5]) {
+    M[0].assign(n, bt); M[1].assign(n, al); M[2].assign(n, 1.0); M[3].assign(n, al); M[4].assign(n, bt);
+    M[0][0] = 0.0; M[0][1 % n] = 0.0; M[1][0] = 0.0;
+    M[3][n - 1] = 0.0; M[4][n - 1] = 0.0; M[4][n - 2] = 0.0;
+}
+
+static std::vector<double> cyclic_correction(int n, double bt, double al, int k) {
+    typedef long double R;
+    const int w = 2;
+    // banded LU (no pivoting) of the non-wrapping part, rows stored [i][j-i+w]
+    std::vector<R> B((size_t)n * (2 * w + 1), 0.0L);
+    auto at = [&](int i, int j) -> R & { return B[(size_t)i * (2 * w + 1) + (j - i + w)]; };
+    const R co[5] = {bt, al, 1.0L, al, bt};
+    for (int i = 0; i < n; i++)
+        for (int j = i - w; j <= i + w; j++)
+            if (j >= 0 && j < n) at(i, j) = co[j - i + w];
+    for (int j = 0; j < n; j++)
+        for (int i = j + 1; i <= j + w && i < n; i++) {
+            R l = at(i, j) / at(j, j);
+            at(i, j) = l;
+            for (int q = j + 1; q <= j + w && q < n; q++) at(i, q) -= l * at(j, q);
+        }
+    auto solve = [&](std::vector<R> &x) {
+        for (int i = 0; i < n; i++)
+            for (int j = std::max(0, i - w); j < i; j++) x[i] -= at(i, j) * x[j];
+        for (int i = n - 1; i >= 0; i--) {
+            for (int j = i + 1; j <= i + w && j < n; j++) x[i] -= at(i, j) * x[j];
+            x[i] /= at(i, i);
+        }
+    };
+    int idx[4];
+    R Mm[4][4] = {{0}};
+    if (k == 2) {
+        idx[0] = 0; idx[1] = n - 1;
+        Mm[0][1] = al; Mm[1][0] = al;                    // row 0: al*x_{n-1}; row n-1: al*x_0
+    } else {
+        idx[0] = 0; idx[1] = 1; idx[2] = n - 2; idx[3] = n - 1;
+        Mm[0][2] = bt; Mm[0][3] = al;                    // row 0:   bt*x_{n-2} + al*x_{n-1}
+        Mm[1][3] = bt;                                   // row 1:   bt*x_{n-1}
+        Mm[2][0] = bt;                                   // row n-2: bt*x_0
+        Mm[3][0] = al; Mm[3][1] = bt;                    // row n-1: al*x_0 + bt*x_1
+    }
+    std::vector<std::vector<R>> Z(k, std::vector<R>(n, 0.0L));
+    for (int q = 0; q < k; q++) { Z[q][idx[q]] = 1.0L; solve(Z[q]); }
+    // S = I + M V^T Z  (k x k), then its inverse by Gauss-Jordan with pivoting
+    R S[4][8] = {{0}};
+    for (int a = 0; a < k; a++)
+        for (int b = 0; b < k; b++) {
+            R v = a == b ? 1.0L : 0.0L;
+            for (int q = 0; q < k; q++) v += Mm[a][q] * Z[b][idx[q]];
+            S[a][b] = v;
+            S[a][k + b] = a == b ? 1.0L : 0.0L;
+        }
+    for (int col = 0; col < k; col++) {
+        int piv = col;
+        for (int r = col + 1; r < k; r++) if (fabsl(S[r][col]) > fabsl(S[piv][col])) piv = r;
+        for (int q = 0; q < 2 * k; q++) std::swap(S[col][q], S[piv][q]);
+        R d = S[col][col];
+        for (int q = 0; q < 2 * k; q++) S[col][q] /= d;
+        for (int r = 0; r < k; r++)
+            if (r != col) {
+                R f = S[r][col];
+                for (int q = 0; q < 2 * k; q++) S[r][q] -= f * S[col][q];
+            }
+    }
+    // K = Z Sinv M ;  stored negated, row-major [n][k]
+    R SM[4][4];
+    for (int a = 0; a < k; a++)
+        for (int b = 0; b < k; b++) {
+            R v = 0.0L;
+            for (int q = 0; q < k; q++) v += S[a][k + q] * Mm[q][b];
+            SM[a][b] = v;
+        }
+    std::vector<double> K((size_t)n * k);
+    for (int i = 0; i < n; i++)
+        for (int b = 0; b < k; b++) {
+            R v = 0.0L;
+            for (int a = 0; a < k; a++) v += Z[a][i] * SM[a][b];
+            K[(size_t)i * k + b] = (double)(-v);
+        }
+    return K;
 }
 
 // ---- tables ---------------------------------------------------------------
@@ -257,7 +356,51 @@ static const double *upload(st_ctx *c, const std::vector<double> &v, int *err) {
     return (const double *)p;
 }
 
+// Periodic family: every derivative and filter kind of a direction gets the
+// cyclic tables (the periodic routines have no sym/asym variants).  The FDL3DI
+// constants are used as the tridiagonal scheme they define (beta = 0), see
+// the oracle's note on the periodic constant set.
+static int build_tables_periodic(st_ctx *c) {
+    int err = 0;
+    const double al1 = 1.0 / 3.0, al2 = 2.0 / 11.0, af = 6.6624e-01, bf = 1.6688e-01;
+    for (int d = 0; d < 3; d++) {
+        int n = c->dm.n[d];
+        for (int order = 1; order <= 2; order++) {
+            std::vector<double> M[5];
+            double al = order == 1 ? al1 : al2;
+            band_rows(n, 0.0, al, M);
+            TriHost h = tri_tables(M[1], M[2], M[3], n, c->seg[d]);
+            std::vector<double> K = cyclic_correction(n, 0.0, al, 2);
+            for (int asym = 0; asym < 2; asym++) {
+                TriTab &t = c->tri[d][(order - 1) * 2 + asym];
+                t.l = upload(c, h.l, &err); t.g = upload(c, h.g, &err); t.up = upload(c, h.up, &err);
+                t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
+                t.wf = upload(c, h.wf, &err); t.wb = upload(c, h.wb, &err);
+                t.kf = h.kf; t.kb = h.kb;
+                t.cyc = upload(c, K, &err);
+            }
+        }
+        std::vector<double> M[5];
+        band_rows(n, bf, af, M);
+        PenHost h = pen_tables(M, n, c->seg[d]);
+        std::vector<double> K = cyclic_correction(n, bf, af, 4);
+        for (int kind = 0; kind < 2; kind++) {
+            PenTab &t = c->pen[d][kind];
+            t.p1 = upload(c, h.p1, &err); t.p2 = upload(c, h.p2, &err);
+            t.g1 = upload(c, h.g1, &err); t.g2 = upload(c, h.g2, &err);
+            t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
+            t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
+            t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
+            t.kf = h.kf; t.kb = h.kb;
+            t.cyc = upload(c, K, &err);
+        }
+    }
+    if (err) return fail(c, ST_E_NOMEM, "could not allocate or upload the LU tables");
+    return ST_OK;
+}
+
 int build_tables(st_ctx *c) {
+    if (c->p.family == ST_FAMILY_PERIODIC) return build_tables_periodic(c);
     int err = 0;
     for (int d = 0; d < 3; d++) {
         int n = c->dm.n[d];
@@ -270,6 +413,7 @@ int build_tables(st_ctx *c) {
             t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
             t.wf = upload(c, h.wf, &err); t.wb = upload(c, h.wb, &err);
             t.kf = h.kf; t.kb = h.kb;
+            t.cyc = nullptr;
         }
         for (int kind = 0; kind < 2; kind++) {
             std::vector<double> M[5];
@@ -282,6 +426,7 @@ int build_tables(st_ctx *c) {
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
             t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
             t.kf = h.kf; t.kb = h.kb;
+            t.cyc = nullptr;
         }
     }
     if (err) return fail(c, ST_E_NOMEM, "could not allocate or upload the LU tables");

@@ -77,6 +77,24 @@ def blast_in_turbulence(params, k0=8.0, mach_t=0.1, p_ratio=100.0, radius_cells=
     return np.ascontiguousarray(Q), np.ascontiguousarray(Y)
 
 
+def periodic_turbulence(params, k0=4.0, urms=0.1, mach_t=None, seed=0):
+    """Conserved state Q (5, Mx, Mz, My) of decaying isotropic turbulence in
+    the single-fluid periodic box: rho = 1, p = 1/gamma (sound speed 1), zero
+    entropy fluctuation, solenoidal velocity with rms ``urms`` per component.
+    When ``mach_t`` is given it sets urms = mach_t/sqrt(3) instead."""
+    shape = (params.nx, params.nz, params.ny)
+    if mach_t is not None:
+        urms = mach_t / np.sqrt(3.0)
+    u, v, w = solenoidal_velocity(shape, k0, urms, seed)
+    g = params.gamma1
+    rho = np.ones(shape)
+    p = np.full(shape, 1.0 / g)
+    Q = np.empty((5,) + shape)
+    Q[0], Q[1], Q[2], Q[3] = rho * u, rho * v, rho * w, rho
+    Q[4] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return np.ascontiguousarray(Q)
+
+
 def write_restart(path, Q, Y, time, step):
     """Write_Restart layout (src/out_mf.f:469-551)."""
     nx, nz, ny = Y.shape

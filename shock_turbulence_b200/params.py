@@ -23,7 +23,12 @@ class StParams(ctypes.Structure):
         ("cfl_cal", ctypes.c_double),
         ("c_beta_scale", ctypes.c_double),
         ("device", ctypes.c_int),
+        ("family", ctypes.c_int),
     ]
+
+
+FAMILY_MF = 0          # two-species symmetric octant (src/main_mf.f)
+FAMILY_PERIODIC = 1    # single-fluid triply periodic box (src/main.f)
 
 
 def default_params(nx, ny=None, nz=None, length=2.0 * math.pi, **kw):
@@ -48,6 +53,23 @@ def default_params(nx, ny=None, nz=None, length=2.0 * math.pi, **kw):
     p.cfl_cal = 0.5
     p.c_beta_scale = 1.0
     p.device = 0
+    p.family = FAMILY_MF
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"st_params has no field {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def periodic_params(nx, ny=None, nz=None, period=2.0 * math.pi, re=100.0, gamma=1.4, **kw):
+    """Single-fluid periodic box (src/define_periodic_sf.f): gamma and Re of the
+    fluid, and x_leng = period*(N-1)/N as Define_Param sets it (:42)."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = default_params(nx, ny, nz, family=FAMILY_PERIODIC, re=re, re1=re, gamma1=gamma)
+    p.x_leng = period * (nx - 1) / nx
+    p.y_leng = period * (ny - 1) / ny
+    p.z_leng = period * (nz - 1) / nz
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(f"st_params has no field {k!r}")
