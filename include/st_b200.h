@@ -81,6 +81,19 @@ typedef struct st_params {
 
 typedef struct st_ctx st_ctx;
 
+/* Parameters of the 1-D spherical-radial single-fluid family (the program
+ * built by src/makefile_radial: rhsv_radial.f, derivCDopt6_radial.f,
+ * filters_nonperiodic.f, hyper_radial.f, lddrk4_nonperiodic_sf.f).  Each
+ * problem is one run of that program on a line of n points spanning -R..R. */
+typedef struct st_radial_params {
+    double gamma;               /* ratio of specific heats                    */
+    double cfl_cal;             /* target CFL (Compute_Tstep)                 */
+    int    hyper_param;         /* 1: artificial viscosity on                 */
+    int    rk_mode;             /* 0: zero alpha2/beta2 (reference build);
+                                   1: HHM 4-6 second-loop values               */
+    int    device;              /* CUDA device ordinal                        */
+} st_radial_params;
+
 /* ---- context --------------------------------------------------------- */
 /* Replaces Setup_Grid (src/grid.f:15-112), Setup_Derivatives_Sym/_Asym
  * (src/derivCDopt6_sym_tri.f:9-373, src/derivCDopt6_asym_tri.f:9-375) and

@@ -19,15 +19,22 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liborc_st.so")
 
 sys.path.insert(0, os.path.dirname(_HERE))
-from shock_turbulence_b200.params import StParams, default_params  # noqa: E402
+from shock_turbulence_b200.params import StParams, StRadialParams, default_params  # noqa: E402
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
 def build(force=False):
-    """Compile the oracle with its Makefile if the library is missing."""
-    if force or not os.path.exists(_LIB):
-        subprocess.check_call(["make", "-s", "-C", _HERE, "liborc_st.so"])
+    """Compile the oracle with its Makefile (make rebuilds it when a source
+    is newer than the library)."""
+    args = ["make", "-s", "-C", _HERE, "liborc_st.so"]
+    if force:
+        args.insert(1, "-B")
+    try:
+        subprocess.check_call(args)
+    except (OSError, subprocess.CalledProcessError):
+        if not os.path.exists(_LIB):
+            raise
     return _LIB
 
 
@@ -55,6 +62,22 @@ def _load():
     lib.orc_pentadiagonal.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
     lib.orc_set_threads.argtypes = [ctypes.c_int]
+    rp = ctypes.POINTER(StRadialParams)
+    ci, cd = ctypes.c_int, ctypes.c_double
+    lib.orc_rad_radius.argtypes = [ci, cd, _dp]
+    lib.orc_rad_dfdx.argtypes = [ci, cd, _dp, _dp, ci, cd]
+    lib.orc_rad_d2fdx2.argtypes = [ci, cd, _dp, _dp, _dp, ci]
+    lib.orc_rad_filter.argtypes = [ci, _dp, _dp]
+    lib.orc_rad_gauss.argtypes = [ci, _dp, _dp]
+    lib.orc_rad_rhs.argtypes = [rp, ci, cd, _dp, _dp]
+    lib.orc_rad_compute_hyper.argtypes = [rp, ci, cd, _dp, _dp]
+    lib.orc_rad_hyper_rhs.argtypes = [rp, ci, cd, _dp, _dp, _dp]
+    lib.orc_rad_tstep.argtypes = [rp, ci, cd, _dp, _dp, _dp, _dp]
+    lib.orc_rad_tstep.restype = cd
+    lib.orc_rad_step.argtypes = [rp, ci, cd, _dp, _dp, _dp, ctypes.POINTER(ci)]
+    lib.orc_rad_step.restype = cd
+    lib.orc_rad_batch.argtypes = [rp, ci, ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_longlong),
+                                  _dp, _dp, _dp, _dp, ctypes.POINTER(ci), ci]
     return lib
 
 
@@ -200,3 +223,60 @@ class Oracle:
         out = np.zeros(10)
         lib().orc_get_monitors(ctypes.c_void_p(self._c), _p(out))
         return out
+
+
+# ---- 1-D spherical-radial family (st_oracle_radial.c) ---------------------
+class Radial:
+    """Line operators and steps of the radial family on numpy arrays; Q of one
+    problem is an array (3, n) = (u_r, rho, s), hyp (2, n) = (beta, visc)."""
+
+    def __init__(self, params):
+        self.p = params
+
+    def radius(self, n, x_leng):
+        r = np.zeros(n)
+        lib().orc_rad_radius(n, float(x_leng), _p(r))
+        return r
+
+    def dfdx(self, x_leng, F, dF, iadd, cadd):
+        lib().orc_rad_dfdx(F.size, float(x_leng), _p(F), _p(dF), int(iadd), float(cadd))
+
+    def d2fdx2(self, x_leng, F, dF, d2F, iadd):
+        lib().orc_rad_d2fdx2(F.size, float(x_leng), _p(F), _p(dF), _p(d2F), int(iadd))
+
+    def filter(self, F, F0):
+        lib().orc_rad_filter(F.size, _p(F), _p(F0))
+
+    def gauss(self, F, Fg):
+        lib().orc_rad_gauss(F.size, _p(F), _p(Fg))
+
+    def rhs(self, x_leng, Q, Qrhs):
+        lib().orc_rad_rhs(ctypes.byref(self.p), Q.shape[1], float(x_leng), _p(Q), _p(Qrhs))
+
+    def compute_hyper(self, x_leng, Q, hyp):
+        lib().orc_rad_compute_hyper(ctypes.byref(self.p), Q.shape[1], float(x_leng), _p(Q), _p(hyp))
+
+    def hyper_rhs(self, x_leng, Q, Qrhs, hyp):
+        lib().orc_rad_hyper_rhs(ctypes.byref(self.p), Q.shape[1], float(x_leng), _p(Q), _p(Qrhs), _p(hyp))
+
+    def tstep(self, x_leng, Q, hyp):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        dt = lib().orc_rad_tstep(ctypes.byref(self.p), Q.shape[1], float(x_leng), _p(Q), _p(hyp),
+                                 ctypes.byref(a), ctypes.byref(b))
+        return dt, a.value, b.value
+
+    def step(self, x_leng, Q, hyp, time, step):
+        t, s = ctypes.c_double(time), ctypes.c_int(step)
+        lib().orc_rad_step(ctypes.byref(self.p), Q.shape[1], float(x_leng), _p(Q), _p(hyp), ctypes.byref(t),
+                           ctypes.byref(s))
+        return t.value, s.value
+
+    def batch(self, lengths, x_leng, Q, hyp, time, step, nsteps):
+        """nsteps steps of every packed problem (Q: 3*sum(n), hyp: 2*sum(n))."""
+        n = np.ascontiguousarray(lengths, dtype=np.int32)
+        off = np.zeros(len(n), dtype=np.int64)
+        off[1:] = np.cumsum(n)[:-1]
+        xl = np.ascontiguousarray(x_leng, dtype=np.float64)
+        lib().orc_rad_batch(ctypes.byref(self.p), len(n), n.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                            off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _p(xl), _p(Q), _p(hyp),
+                            _p(time), step.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(nsteps))

@@ -68,6 +68,26 @@ void orc_lddrk4(orc *c, double *time, int *step);
 void orc_step(orc *c, double *time, int *step);
 void orc_get_monitors(orc *c, double out[10]);
 
+/* 1-D spherical-radial family (st_oracle_radial.c).  Q = (u_r, rho, s)
+ * with s = P/rho^gamma, n points each; hyp = (beta_hyper, visc_hyper). */
+void orc_rad_radius(int n, double x_leng, double *rad);
+void orc_rad_dfdx(int n, double x_leng, const double *F, double *dF, int iadd, double cadd);
+void orc_rad_d2fdx2(int n, double x_leng, const double *F, double *dF, double *d2F, int iadd);
+void orc_rad_filter(int n, const double *F, double *F0);
+void orc_rad_gauss(int n, const double *F, double *Fg);
+void orc_rad_rhs(const st_radial_params *p, int n, double x_leng, const double *Q, double *Qrhs);
+void orc_rad_compute_hyper(const st_radial_params *p, int n, double x_leng, const double *Q, double *hyp);
+void orc_rad_hyper_rhs(const st_radial_params *p, int n, double x_leng, const double *Q, double *Qrhs,
+                       double *hyp);
+double orc_rad_tstep(const st_radial_params *p, int n, double x_leng, const double *Q, const double *hyp,
+                     double *cfl_stab, double *cfl_resv);
+void orc_rad_lddrk4(const st_radial_params *p, int n, double x_leng, double *Q, double *hyp, double dt,
+                    double *time, int *step);
+double orc_rad_step(const st_radial_params *p, int n, double x_leng, double *Q, double *hyp, double *time,
+                    int *step);
+void orc_rad_batch(const st_radial_params *p, int nprob, const int *n, const long long *off,
+                   const double *x_leng, double *Q, double *hyp, double *time, int *step, int nsteps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,43 @@ def periodic_turbulence(params, k0=4.0, urms=0.1, mach_t=None, seed=0):
     return np.ascontiguousarray(Q)
 
 
+def radial_blast(n, x_leng=2.0, p_ratio=100.0, radius_cells=4.0, rho_amp=0.01, gamma=1.4, rng=None):
+    """One 1-D spherical-radial blast problem on n points spanning
+    -x_leng/2..x_leng/2 (r = |(i - n/2 - 1/2) DX|, src/rhsv_radial.f:55-59):
+    u_r = 0, rho = 1 + rho_amp * (random-phase radial perturbation with a
+    k^2 exp(-k^2/8) spectrum, max |.| = 1), P = (1/gamma) (1 + (p_ratio - 1)
+    exp(-r^2 / (radius_cells DX)^2)), s = P / rho^gamma.  Returns Q (3, n)."""
+    rng = np.random.default_rng(0) if rng is None else rng
+    dx = x_leng / (n - 1)
+    i = np.arange(1, n + 1)
+    r = np.abs(((i - n // 2).astype(np.float32).astype(np.float64) - 0.5) * dx)
+    R = x_leng / 2.0
+    k = np.arange(1, 17)
+    amp = k ** 2 * np.exp(-(k ** 2) / 8.0)
+    ph = rng.uniform(0.0, 2.0 * np.pi, size=k.size)
+    pert = (amp[:, None] * np.cos(np.pi * k[:, None] * r[None, :] / R + ph[:, None])).sum(axis=0)
+    pert /= np.abs(pert).max()
+    rho = 1.0 + rho_amp * pert
+    P = (1.0 / gamma) * (1.0 + (p_ratio - 1.0) * np.exp(-r ** 2 / (radius_cells * dx) ** 2))
+    Q = np.zeros((3, n))
+    Q[1] = rho
+    Q[2] = P / rho ** gamma
+    return Q
+
+
+def radial_batch(nprob, nmin=128, nmax=4096, pmin=10.0, pmax=1000.0, seed=2, gamma=1.4, x_leng=2.0):
+    """Independent radial blast problems with lengths drawn uniformly from
+    [nmin, nmax] and peak pressure ratios from [pmin, pmax] (seeded).
+    Returns (lengths int32, x_leng float64, packed Q): problem k's block of
+    3*n_k values (u, rho, s) starts at 3*sum(n_j, j<k)."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(nmin, nmax + 1, size=nprob).astype(np.int32)
+    ratios = rng.uniform(pmin, pmax, size=nprob)
+    blocks = [radial_blast(int(n), x_leng, float(pr), gamma=gamma, rng=rng).ravel()
+              for n, pr in zip(lengths, ratios)]
+    return lengths, np.full(nprob, float(x_leng)), np.ascontiguousarray(np.concatenate(blocks))
+
+
 def write_restart(path, Q, Y, time, step):
     """Write_Restart layout (src/out_mf.f:469-551)."""
     nx, nz, ny = Y.shape

@@ -75,3 +75,17 @@ def periodic_params(nx, ny=None, nz=None, period=2.0 * math.pi, re=100.0, gamma=
             raise AttributeError(f"st_params has no field {k!r}")
         setattr(p, k, v)
     return p
+
+
+class StRadialParams(ctypes.Structure):
+    """st_radial_params of include/st_b200.h (1-D spherical-radial family)."""
+    _fields_ = [
+        ("gamma", ctypes.c_double), ("cfl_cal", ctypes.c_double),
+        ("hyper_param", ctypes.c_int), ("rk_mode", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+def radial_params(gamma=1.4, cfl_cal=0.5, hyper_param=1, rk_mode=0, device=0):
+    p = StRadialParams()
+    p.gamma, p.cfl_cal, p.hyper_param, p.rk_mode, p.device = gamma, cfl_cal, hyper_param, rk_mode, device
+    return p
