@@ -249,6 +249,53 @@ int  st_get_monitors(st_ctx *c, double out[10]);
 /* Synchronises the context stream. */
 int  st_sync(st_ctx *c);
 
+/* ---- 1-D spherical-radial family, batched ---------------------------------
+ * Many independent problems, each one run of the reference's radial program
+ * (src/makefile_radial) on a line of n[k] points, 16 <= n[k] <= 4096, of
+ * length x_leng[k] spanning -x_leng/2..x_leng/2.  Packed arrays: problem k's
+ * state block Q of 3*n[k] values (u_r, rho, s = P/rho^gamma; the reference's
+ * Q(:,1), Q(:,4), Q(:,5)) starts at 3*sum(n[j], j<k); single fields of the
+ * line operators start at sum(n[j], j<k).  Host or device arrays. */
+typedef struct st_radial st_radial;
+int  st_radial_create(const st_radial_params *p, int nprob, const int *n, const double *x_leng,
+                      st_radial **out);
+int  st_radial_destroy(st_radial *h);
+const char *st_radial_last_error(const st_radial *h);
+int  st_radial_num_points(const st_radial *h, long long *npts);
+/* Sets every problem's state (time and step counters restart at zero). */
+int  st_radial_set_state(st_radial *h, const double *Q);
+int  st_radial_get_state(st_radial *h, double *Q);
+/* /HYPER/ of every problem: 2*n[k] values (beta_hyper, visc_hyper). */
+int  st_radial_get_hyper(st_radial *h, double *hyp);
+int  st_radial_get_time(st_radial *h, double *time, int *step);
+/* nsteps iterations of the main loop (src/main.f:129-136: Compute_CFL,
+ * Compute_Tstep, LDDRK4 src/lddrk4_nonperiodic_sf.f:376-468) of every
+ * problem, each with its own time step, in one persistent launch per problem
+ * class; a problem at step 0 first gets Compute_hyper (src/main.f:100).
+ * st_radial_step waits for completion, st_radial_step_async does not. */
+int  st_radial_step(st_radial *h, int nsteps);
+int  st_radial_step_async(st_radial *h, int nsteps);
+int  st_radial_set_stream(st_radial *h, void *stream);
+/* Kernel configuration per problem class (n <= 1024, n > 1024): index 0..2
+ * into (64,16)/(128,8)/(256,4) and (256,16)/(512,8)/(1024,4) threads x rows
+ * per thread.  st_radial_tune times every candidate for one step of the
+ * current state (which it leaves unchanged) and keeps the fastest; ms[0]
+ * and ms[1] get the best times (ms) of the long and the short class.  No
+ * reference counterpart. */
+int  st_radial_config(st_radial *h, int *cfg_short, int *cfg_long, int set);
+int  st_radial_tune(st_radial *h, double ms[2]);
+/* Line operators of every problem: DFDX src/derivCDopt6_radial.f:637-791,
+ * D2FDX2 :794-953, Compact_Filter_X src/filters_nonperiodic.f:418-619,
+ * Gaussian_Filter_X :1055-1224, RHS (RHS_r src/rhsv_radial.f:30-157) and
+ * RHS + Hyper_RHS (src/hyper_radial.f:75-187; refreshes /HYPER/). */
+int  st_radial_dfdx(st_radial *h, const double *F, double *dF, int iadd, double cadd);
+int  st_radial_d2fdx2(st_radial *h, const double *F, double *dF, double *d2F, int iadd);
+int  st_radial_compact_filter_x(st_radial *h, const double *F, double *F0);
+int  st_radial_gaussian_filter_x(st_radial *h, const double *F, double *Fg);
+int  st_radial_rhs(st_radial *h, const double *Q, double *Qrhs);
+int  st_radial_rhs_hyper(st_radial *h, const double *Q, double *Qrhs);
+int  st_radial_launch_count(const st_radial *h, long long *count);
+
 /* ---- streams, instrumentation (no reference counterpart) ------------------ */
 /* Runs the context's work on a caller-owned cudaStream_t (NULL restores the
  * context's own stream), so callers can order and time it with their own

@@ -50,6 +50,28 @@ SIGNATURES = {
     "st_profile": [_ctx, ctypes.c_int],
     "st_profile_report": [_ctx, ctypes.c_char_p, ctypes.c_int],
     "st_launch_count": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
+    # 1-D spherical-radial batch (handle in place of the context)
+    "st_radial_create": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_void_p)],
+    "st_radial_destroy": [_ctx],
+    "st_radial_last_error": [_ctx],
+    "st_radial_num_points": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
+    "st_radial_set_state": [_ctx, _dp],
+    "st_radial_get_state": [_ctx, _dp],
+    "st_radial_get_hyper": [_ctx, _dp],
+    "st_radial_get_time": [_ctx, _dp, _dp],
+    "st_radial_step": [_ctx, ctypes.c_int],
+    "st_radial_step_async": [_ctx, ctypes.c_int],
+    "st_radial_set_stream": [_ctx, ctypes.c_void_p],
+    "st_radial_config": [_ctx, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int],
+    "st_radial_tune": [_ctx, ctypes.POINTER(ctypes.c_double)],
+    "st_radial_dfdx": [_ctx, _dp, _dp, ctypes.c_int, ctypes.c_double],
+    "st_radial_d2fdx2": [_ctx, _dp, _dp, _dp, ctypes.c_int],
+    "st_radial_compact_filter_x": [_ctx, _dp, _dp],
+    "st_radial_gaussian_filter_x": [_ctx, _dp, _dp],
+    "st_radial_rhs": [_ctx, _dp, _dp],
+    "st_radial_rhs_hyper": [_ctx, _dp, _dp],
+    "st_radial_launch_count": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
 }
 for _d in ("x", "y", "z"):
     for _s in ("sym", "asym"):
@@ -62,6 +84,7 @@ for _d in ("x", "y", "z"):
     SIGNATURES[f"st_compact_filter_{_d}"] = [_ctx, _dp, _dp]
 
 _RESTYPES = {"st_last_error": ctypes.c_char_p, "st_status_string": ctypes.c_char_p,
+             "st_radial_last_error": ctypes.c_char_p,
              "st_default_params": None}
 
 _lib = None
