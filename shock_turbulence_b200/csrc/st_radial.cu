@@ -46,6 +46,8 @@ struct K {
     double g[5];
 };
 
+__constant__ K c_k;        // scheme constants, identical for every batch
+
 struct Tabs {
     const double *L1, *I1, *U1;       // first-derivative system: multiplier, 1/pivot, upper
     const double *L2, *I2, *U2;       // second-derivative system
@@ -116,7 +118,7 @@ __device__ __forceinline__ Map2 comp(const Map2 &f, const Map2 &t) { return comp
 // Exclusive scan over the threads of the CTA.  FWD: thread t receives the
 // composition of the maps of threads 0..t-1 (applied in that order);
 // otherwise of threads T-1..t+1 (applied from the last down).  sh holds
-// >= T/32 maps.  Ends with the CTA synchronised.
+// >= 2*T/32 maps.  Ends with the CTA synchronised.
 template <class M, bool FWD, int T>
 __device__ __forceinline__ M block_scan_excl(M m, M *sh) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -132,7 +134,24 @@ __device__ __forceinline__ M block_scan_excl(M m, M *sh) {
     if (FWD ? lane == 0 : lane == 31) ex = ident(m);
     if (FWD ? lane == 31 : lane == 0) sh[w] = inc;
     __syncthreads();
-    if (NW > 1) {
+    if constexpr (NW > 8) {
+        // warp 0 scans the warp totals; sh[NW + w] receives warp w's prefix
+        if (w == 0) {
+            M tot = lane < NW ? sh[lane] : ident(m);
+            M iw = tot;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                M o = FWD ? shfl_up(iw, d) : shfl_down(iw, d);
+                bool take = FWD ? lane >= d : lane + d < 32;
+                if (take) iw = comp(o, iw);
+            }
+            M xw = FWD ? shfl_up(iw, 1) : shfl_down(iw, 1);
+            if (FWD ? lane == 0 : lane == 31) xw = ident(m);
+            if (lane < NW) sh[NW + lane] = xw;
+        }
+        __syncthreads();
+        ex = comp(sh[NW + w], ex);
+    } else if constexpr (NW > 1) {
         M pre = ident(m);
         if (FWD) { for (int v = 0; v < w; v++) pre = comp(pre, sh[v]); }
         else { for (int v = NW - 1; v > w; v--) pre = comp(pre, sh[v]); }
@@ -200,7 +219,7 @@ __device__ __forceinline__ void tri_solve(double (&r)[SMAX], int a, int cnt, int
 // r'_i = (r_i - p2_i r'_{i-2}) - p1_i r'_{i-1};
 // x_i = ((r'_i - q1_i x_{i+1}) - q2_i x_{i+2}) * id_i.
 template <int SMAX, int T>
-__device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int n, const Tabs &tb, Map2 *sh) {
+__device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int n, const Tabs *__restrict__ tb, Map2 *sh) {
     // forward: state (r'_{i-1}, r'_{i-2}); local run plus the responses to
     // the incoming state's two components
     double s1 = 0.0, s2 = 0.0, e11 = 1.0, e12 = 0.0, e21 = 0.0, e22 = 1.0;   // e_k: response to unit c_k
@@ -208,8 +227,8 @@ __device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int
     for (int q = 0; q < SMAX; q++)
         if (q < cnt) {
             int i = a + q;
-            double p1 = i == 0 ? 0.0 : pen_f(tb.P1, tb.TF, n, i, 0);
-            double p2 = i < 2 ? 0.0 : pen_f(tb.P2, tb.TF, n, i, 1);
+            double p1 = i == 0 ? 0.0 : pen_f(tb->P1, tb->TF, n, i, 0);
+            double p2 = i < 2 ? 0.0 : pen_f(tb->P2, tb->TF, n, i, 1);
             double v = fma(-p1, s1, fma(-p2, s2, r[q]));
             double w1 = fma(-p1, e11, -p2 * e21);   // response of row i to c1
             double w2 = fma(-p1, e12, -p2 * e22);   // to c2
@@ -226,8 +245,8 @@ __device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int
     for (int q = 0; q < SMAX; q++)
         if (q < cnt) {
             int i = a + q;
-            double p1 = i == 0 ? 0.0 : pen_f(tb.P1, tb.TF, n, i, 0);
-            double p2 = i < 2 ? 0.0 : pen_f(tb.P2, tb.TF, n, i, 1);
+            double p1 = i == 0 ? 0.0 : pen_f(tb->P1, tb->TF, n, i, 0);
+            double p2 = i < 2 ? 0.0 : pen_f(tb->P2, tb->TF, n, i, 1);
             double w1 = fma(-p1, e11, -p2 * e21);
             double w2 = fma(-p1, e12, -p2 * e22);
             e21 = e11; e22 = e12; e11 = w1; e12 = w2;
@@ -240,9 +259,9 @@ __device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int
     for (int q = SMAX - 1; q >= 0; q--)
         if (q < cnt) {
             int i = a + q;
-            double q1 = i >= n - 1 ? 0.0 : pen_f(tb.Q1, tb.TF, n, i, 2);
-            double q2 = i >= n - 2 ? 0.0 : pen_f(tb.Q2, tb.TF, n, i, 3);
-            double id = pen_f(tb.IF, tb.TF, n, i, 4);
+            double q1 = i >= n - 1 ? 0.0 : pen_f(tb->Q1, tb->TF, n, i, 2);
+            double q2 = i >= n - 2 ? 0.0 : pen_f(tb->Q2, tb->TF, n, i, 3);
+            double id = pen_f(tb->IF, tb->TF, n, i, 4);
             double v = fma(-q2, x2, fma(-q1, x1, r[q])) * id;
             double w1 = fma(-q2, f21, -q1 * f11) * id;
             double w2 = fma(-q2, f22, -q1 * f12) * id;
@@ -258,9 +277,9 @@ __device__ __forceinline__ void pen_solve(double (&r)[SMAX], int a, int cnt, int
     for (int q = SMAX - 1; q >= 0; q--)
         if (q < cnt) {
             int i = a + q;
-            double q1 = i >= n - 1 ? 0.0 : pen_f(tb.Q1, tb.TF, n, i, 2);
-            double q2 = i >= n - 2 ? 0.0 : pen_f(tb.Q2, tb.TF, n, i, 3);
-            double id = pen_f(tb.IF, tb.TF, n, i, 4);
+            double q1 = i >= n - 1 ? 0.0 : pen_f(tb->Q1, tb->TF, n, i, 2);
+            double q2 = i >= n - 2 ? 0.0 : pen_f(tb->Q2, tb->TF, n, i, 3);
+            double id = pen_f(tb->IF, tb->TF, n, i, 4);
             double w1 = fma(-q2, f21, -q1 * f11) * id;
             double w2 = fma(-q2, f22, -q1 * f12) * id;
             f21 = f11; f22 = f12; f11 = w1; f12 = w2;
@@ -275,51 +294,51 @@ enum Op { OP_D1 = 0, OP_D2, OP_FILT, OP_GAUSS, OP_RHS, OP_HYPER };
 // DFDX src/derivCDopt6_radial.f:703-760, D2FDX2 :862-918,
 // Compact_Filter_X src/filters_nonperiodic.f:479-589 and
 // Gaussian_Filter_X :1108-1221 (symmetric reflection at both ends)
-__device__ __noinline__ double boundary_row(int op, int i, const double *X, int n, double fac, const K &k) {
+__device__ __noinline__ double boundary_row(int op, int i, const double *X, int n, double fac) {
     if (op == OP_D1) {
-        if (i >= 3 && i <= n - 4) return fac * (k.b1 * (X[i + 2] - X[i - 2]) + k.a1 * (X[i + 1] - X[i - 1]));
-        if (i == 2) return fac * (k.cl3 * (X[4] - X[0]) + k.cl4 * (X[3] - X[1]));
-        if (i == 1) return fac * (-k.cl1 * X[0] - 5.0e-1 * X[1] + X[2] + k.cl2 * X[3]);
+        if (i >= 3 && i <= n - 4) return fac * (c_k.b1 * (X[i + 2] - X[i - 2]) + c_k.a1 * (X[i + 1] - X[i - 1]));
+        if (i == 2) return fac * (c_k.cl3 * (X[4] - X[0]) + c_k.cl4 * (X[3] - X[1]));
+        if (i == 1) return fac * (-c_k.cl1 * X[0] - 5.0e-1 * X[1] + X[2] + c_k.cl2 * X[3]);
         if (i == 0) return fac * (-2.5 * X[0] + 2.0 * X[1] + 5.0e-1 * X[2]);
-        if (i == n - 3) return fac * (k.cl3 * (X[n - 1] - X[n - 5]) + k.cl4 * (X[n - 2] - X[n - 4]));
-        if (i == n - 2) return fac * (k.cl1 * X[n - 1] + 5.0e-1 * X[n - 2] - X[n - 3] - k.cl2 * X[n - 4]);
+        if (i == n - 3) return fac * (c_k.cl3 * (X[n - 1] - X[n - 5]) + c_k.cl4 * (X[n - 2] - X[n - 4]));
+        if (i == n - 2) return fac * (c_k.cl1 * X[n - 1] + 5.0e-1 * X[n - 2] - X[n - 3] - c_k.cl2 * X[n - 4]);
         return fac * (2.5 * X[n - 1] - 2.0 * X[n - 2] - 5.0e-1 * X[n - 3]);
     }
     if (op == OP_D2) {
         if (i >= 3 && i <= n - 4)
-            return fac * (k.b2 * (X[i + 2] + X[i - 2]) + k.a2 * (X[i + 1] + X[i - 1]) - k.d2 * X[i]);
-        if (i == 2) return fac * (k.cl5 * (X[0] - 2.0 * X[2] + X[4]) + k.cl6 * (X[1] - 2.0 * X[2] + X[3]));
+            return fac * (c_k.b2 * (X[i + 2] + X[i - 2]) + c_k.a2 * (X[i + 1] + X[i - 1]) - c_k.d2 * X[i]);
+        if (i == 2) return fac * (c_k.cl5 * (X[0] - 2.0 * X[2] + X[4]) + c_k.cl6 * (X[1] - 2.0 * X[2] + X[3]));
         if (i == 1) return fac * (1.2375 * X[0] - 3.0 * X[1] + 2.325 * X[2] - 6.0e-1 * X[3] + 3.75e-2 * X[4]);
         if (i == 0) return fac * (1.3e1 * X[0] - 2.7e1 * X[1] + 1.5e1 * X[2] - X[3]);
         if (i == n - 3)
-            return fac * (k.cl5 * (X[n - 1] - 2.0 * X[n - 3] + X[n - 5]) +
-                          k.cl6 * (X[n - 2] - 2.0 * X[n - 3] + X[n - 4]));
+            return fac * (c_k.cl5 * (X[n - 1] - 2.0 * X[n - 3] + X[n - 5]) +
+                          c_k.cl6 * (X[n - 2] - 2.0 * X[n - 3] + X[n - 4]));
         if (i == n - 2)
             return fac * (1.2375 * X[n - 1] - 3.0 * X[n - 2] + 2.325 * X[n - 3] - 6.0e-1 * X[n - 4] +
                           3.75e-2 * X[n - 5]);
         return fac * (1.3e1 * X[n - 1] - 2.7e1 * X[n - 2] + 1.5e1 * X[n - 3] - X[n - 4]);
     }
     if (op == OP_FILT) {
-        if (i == 0) return k.bc1[1] * X[0] + k.bc1[2] * X[1] + k.bc1[3] * X[2] + k.bc1[4] * X[3] + k.bc1[5] * X[4];
-        if (i == 1) return k.bc2[1] * X[0] + k.bc2[2] * X[1] + k.bc2[3] * X[2] + k.bc2[4] * X[3] + k.bc2[5] * X[4];
-        if (i == 2) return k.bc3[2] * X[4] + k.bc3[1] * X[3] + k.bc3[0] * X[2] + k.bc3[1] * X[1] + k.bc3[2] * X[0];
+        if (i == 0) return c_k.bc1[1] * X[0] + c_k.bc1[2] * X[1] + c_k.bc1[3] * X[2] + c_k.bc1[4] * X[3] + c_k.bc1[5] * X[4];
+        if (i == 1) return c_k.bc2[1] * X[0] + c_k.bc2[2] * X[1] + c_k.bc2[3] * X[2] + c_k.bc2[4] * X[3] + c_k.bc2[5] * X[4];
+        if (i == 2) return c_k.bc3[2] * X[4] + c_k.bc3[1] * X[3] + c_k.bc3[0] * X[2] + c_k.bc3[1] * X[1] + c_k.bc3[2] * X[0];
         if (i == 3)
-            return k.bc4[3] * X[6] + k.bc4[2] * X[5] + k.bc4[1] * X[4] + k.bc4[0] * X[3] + k.bc4[1] * X[2] +
-                   k.bc4[2] * X[1] + k.bc4[3] * X[0];
+            return c_k.bc4[3] * X[6] + c_k.bc4[2] * X[5] + c_k.bc4[1] * X[4] + c_k.bc4[0] * X[3] + c_k.bc4[1] * X[2] +
+                   c_k.bc4[2] * X[1] + c_k.bc4[3] * X[0];
         if (i == n - 1)
-            return k.bc1[1] * X[n - 1] + k.bc1[2] * X[n - 2] + k.bc1[3] * X[n - 3] + k.bc1[4] * X[n - 4] +
-                   k.bc1[5] * X[n - 5];
+            return c_k.bc1[1] * X[n - 1] + c_k.bc1[2] * X[n - 2] + c_k.bc1[3] * X[n - 3] + c_k.bc1[4] * X[n - 4] +
+                   c_k.bc1[5] * X[n - 5];
         if (i == n - 2)
-            return k.bc2[1] * X[n - 1] + k.bc2[2] * X[n - 2] + k.bc2[3] * X[n - 3] + k.bc2[4] * X[n - 4] +
-                   k.bc2[5] * X[n - 5];
+            return c_k.bc2[1] * X[n - 1] + c_k.bc2[2] * X[n - 2] + c_k.bc2[3] * X[n - 3] + c_k.bc2[4] * X[n - 4] +
+                   c_k.bc2[5] * X[n - 5];
         if (i == n - 3)
-            return k.bc3[2] * X[n - 5] + k.bc3[1] * X[n - 4] + k.bc3[0] * X[n - 3] + k.bc3[1] * X[n - 2] +
-                   k.bc3[2] * X[n - 1];
-        return k.bc4[3] * X[n - 7] + k.bc4[2] * X[n - 6] + k.bc4[1] * X[n - 5] + k.bc4[0] * X[n - 4] +
-               k.bc4[1] * X[n - 3] + k.bc4[2] * X[n - 2] + k.bc4[3] * X[n - 1];
+            return c_k.bc3[2] * X[n - 5] + c_k.bc3[1] * X[n - 4] + c_k.bc3[0] * X[n - 3] + c_k.bc3[1] * X[n - 2] +
+                   c_k.bc3[2] * X[n - 1];
+        return c_k.bc4[3] * X[n - 7] + c_k.bc4[2] * X[n - 6] + c_k.bc4[1] * X[n - 5] + c_k.bc4[0] * X[n - 4] +
+               c_k.bc4[1] * X[n - 3] + c_k.bc4[2] * X[n - 2] + c_k.bc4[3] * X[n - 1];
     }
     // Gaussian (a+b == b+a, so reflected pairs need no particular order)
-    const double *g = k.g;
+    const double *g = c_k.g;
     if (i == 0) return g[4] * (2.0 * X[4]) + g[3] * (2.0 * X[3]) + g[2] * (2.0 * X[2]) + g[1] * (2.0 * X[1]) + g[0] * X[0];
     if (i == n - 1)
         return g[4] * (2.0 * X[n - 5]) + g[3] * (2.0 * X[n - 4]) + g[2] * (2.0 * X[n - 3]) + g[1] * (2.0 * X[n - 2]) +
@@ -336,24 +355,24 @@ __device__ __noinline__ double boundary_row(int op, int i, const double *X, int 
 // explicit right-hand side of rows a..a+cnt-1 (interior rows inline)
 template <int SMAX>
 __device__ __forceinline__ void rhs_rows(double (&r)[SMAX], int op, const double *X, int a, int cnt, int n,
-                                         double fac, const K &k) {
+                                         double fac) {
 #pragma unroll
     for (int q = 0; q < SMAX; q++)
         if (q < cnt) {
             const int i = a + q;
             double w;
             if (i >= 4 && i <= n - 5) {
-                if (op == OP_D1) w = fac * (k.b1 * (X[i + 2] - X[i - 2]) + k.a1 * (X[i + 1] - X[i - 1]));
+                if (op == OP_D1) w = fac * (c_k.b1 * (X[i + 2] - X[i - 2]) + c_k.a1 * (X[i + 1] - X[i - 1]));
                 else if (op == OP_D2)
-                    w = fac * (k.b2 * (X[i + 2] + X[i - 2]) + k.a2 * (X[i + 1] + X[i - 1]) - k.d2 * X[i]);
+                    w = fac * (c_k.b2 * (X[i + 2] + X[i - 2]) + c_k.a2 * (X[i + 1] + X[i - 1]) - c_k.d2 * X[i]);
                 else if (op == OP_FILT)
-                    w = k.fa4 * (X[i + 4] + X[i - 4]) + k.fa3 * (X[i + 3] + X[i - 3]) + k.fa2 * (X[i + 2] + X[i - 2]) +
-                        k.fa1 * (X[i + 1] + X[i - 1]) + k.fa0 * X[i];
+                    w = c_k.fa4 * (X[i + 4] + X[i - 4]) + c_k.fa3 * (X[i + 3] + X[i - 3]) + c_k.fa2 * (X[i + 2] + X[i - 2]) +
+                        c_k.fa1 * (X[i + 1] + X[i - 1]) + c_k.fa0 * X[i];
                 else
-                    w = k.g[4] * (X[i + 4] + X[i - 4]) + k.g[3] * (X[i + 3] + X[i - 3]) +
-                        k.g[2] * (X[i + 2] + X[i - 2]) + k.g[1] * (X[i + 1] + X[i - 1]) + k.g[0] * X[i];
+                    w = c_k.g[4] * (X[i + 4] + X[i - 4]) + c_k.g[3] * (X[i + 3] + X[i - 3]) +
+                        c_k.g[2] * (X[i + 2] + X[i - 2]) + c_k.g[1] * (X[i + 1] + X[i - 1]) + c_k.g[0] * X[i];
             } else {
-                w = boundary_row(op, i, X, n, fac, k);
+                w = boundary_row(op, i, X, n, fac);
             }
             r[q] = w;
         }
@@ -387,7 +406,7 @@ struct Smem {
     double Y[N];          // line-operator result
     double Ru[N], Rr[N], Rs[N];   // dQ of the stage (u, rho, s)
     double Du[N];         // -du/dr (DFDX(u, -1)), reused by Hyper_RHS
-    Map2 sc[T / 32];      // scan scratch (also holds Map1 values)
+    Map2 sc[2 * (T / 32)];   // scan scratch (also holds Map1 values)
     double red[T / 32][4];
     int prob;
 };
@@ -398,14 +417,14 @@ struct Smem {
 // src/derivCDopt6_radial.f:772-784).  fac: cadd*sx*(n-1) (DFDX) or
 // (n-1)^2*sx^2 (D2FDX2).
 template <int T, int SMAX>
-__device__ __noinline__ void line_op(Smem<T, SMAX> &S, int op, int n, double fac, const K &k, const Tabs &tb) {
+__device__ __noinline__ void line_op(Smem<T, SMAX> &S, int op, int n, double fac, const Tabs *__restrict__ tb) {
     const int t = threadIdx.x, Sr = (n + T - 1) / T, a = t * Sr, cnt = max(0, min(Sr, n - a));
     double r[SMAX];
-    rhs_rows<SMAX>(r, op, S.X, a, cnt, n, fac, k);
+    rhs_rows<SMAX>(r, op, S.X, a, cnt, n, fac);
     if (op == OP_D1 || op == OP_D2) {
         const bool d1 = op == OP_D1;
-        tri_solve<SMAX, T>(r, a, cnt, n, d1 ? tb.L1 : tb.L2, d1 ? tb.I1 : tb.I2, d1 ? tb.U1 : tb.U2,
-                           d1 ? tb.T1 : tb.T2, reinterpret_cast<Map1 *>(S.sc));
+        tri_solve<SMAX, T>(r, a, cnt, n, d1 ? tb->L1 : tb->L2, d1 ? tb->I1 : tb->I2, d1 ? tb->U1 : tb->U2,
+                           d1 ? tb->T1 : tb->T2, reinterpret_cast<Map1 *>(S.sc));
     } else if (op == OP_FILT) {
         pen_solve<SMAX, T>(r, a, cnt, n, tb, S.sc);
     }
@@ -430,19 +449,19 @@ __device__ __forceinline__ void stage(Smem<T, SMAX> &S, int n, F f) {
 // Gauss(|d4|) * DX^5
 template <int T, int SMAX>
 __device__ __noinline__ void problem_hyper_core(Smem<T, SMAX> &S, const Geo &G, const double *u, double *hyp,
-                                                const K &k, const Tabs &tb) {
+                                                const Tabs *__restrict__ tb) {
     const int n = G.n;
     RAD_ROWS(T, n);
     stage(S, n, [&](int i) { return u[i]; });
-    line_op<T, SMAX>(S, OP_D2, n, G.fac2, k, tb);
+    line_op<T, SMAX>(S, OP_D2, n, G.fac2, tb);
     __syncthreads();                                        // every read of X is done
     for (int q = 0; q < cnt; q++) S.X[a + q] = S.Y[a + q];
     __syncthreads();
-    line_op<T, SMAX>(S, OP_D2, n, G.fac2, k, tb);
+    line_op<T, SMAX>(S, OP_D2, n, G.fac2, tb);
     __syncthreads();
     for (int q = 0; q < cnt; q++) S.X[a + q] = fabs(S.Y[a + q]);
     __syncthreads();
-    line_op<T, SMAX>(S, OP_GAUSS, n, 0.0, k, tb);
+    line_op<T, SMAX>(S, OP_GAUSS, n, 0.0, tb);
     const double DX5 = pow(G.DX, 5.0);
     for (int q = 0; q < cnt; q++) {
         hyp[a + q] = 1.0 * S.Y[a + q] * DX5;
@@ -456,18 +475,18 @@ __device__ __noinline__ void problem_hyper_core(Smem<T, SMAX> &S, const Geo &G, 
 // refreshes /HYPER/ (hyp).
 template <int T, int SMAX>
 __device__ __noinline__ void problem_rhs(Smem<T, SMAX> &S, const Geo &G, const double *u, const double *rho,
-                                         const double *s, double *hyp, double gam, int hyper, const K &k,
-                                         const Tabs &tb) {
+                                         const double *s, double *hyp, double gam, int hyper,
+                                         const Tabs *__restrict__ tb) {
     const int n = G.n;
     RAD_ROWS(T, n);
     // d rho/dt = -u d rho/dr  (DFDX(rho, Qrhs4, 1, -1): 0 + W)
     stage(S, n, [&](int i) { return rho[i]; });
-    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, tb);
     for (int q = 0; q < cnt; q++) S.Rr[a + q] = S.Y[a + q] * u[a + q];
     __syncthreads();
     // - rho/r^2 d(u r^2)/dr
     stage(S, n, [&](int i) { double rd = radius(i, G); return u[i] * rd * rd; });
-    line_op<T, SMAX>(S, OP_D1, n, G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, G.fac1, tb);
     for (int q = 0; q < cnt; q++) {
         const int i = a + q;
         double rd = radius(i, G);
@@ -476,25 +495,25 @@ __device__ __noinline__ void problem_rhs(Smem<T, SMAX> &S, const Geo &G, const d
     __syncthreads();
     // d u/dt = -u du/dr
     stage(S, n, [&](int i) { return u[i]; });
-    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, tb);
     for (int q = 0; q < cnt; q++) { S.Du[a + q] = S.Y[a + q]; S.Ru[a + q] = u[a + q] * S.Y[a + q]; }
     __syncthreads();
     // - (dP/dr)/rho,  P = s rho^gamma
     stage(S, n, [&](int i) { return s[i] * pow(rho[i], gam); });
-    line_op<T, SMAX>(S, OP_D1, n, G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, G.fac1, tb);
     for (int q = 0; q < cnt; q++) S.Ru[a + q] = S.Ru[a + q] - (S.Y[a + q] / rho[a + q]);
     __syncthreads();
     // d s/dt = -u ds/dr
     stage(S, n, [&](int i) { return s[i]; });
-    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, -G.fac1, tb);
     for (int q = 0; q < cnt; q++) S.Rs[a + q] = S.Y[a + q] * u[a + q];
     __syncthreads();
     if (!hyper) return;
-    problem_hyper_core<T, SMAX>(S, G, u, hyp, k, tb);
+    problem_hyper_core<T, SMAX>(S, G, u, hyp, tb);
     const double *bh = hyp, *vh = hyp + n;
     // 1/r^2 d/dr(r^2 2 nu du/dr)   (du/dr = -Du exactly: DFDX is odd in cadd)
     stage(S, n, [&](int i) { double rd = radius(i, G); return rd * rd * 2.0 * vh[i] * (-S.Du[i]); });
-    line_op<T, SMAX>(S, OP_D1, n, G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, G.fac1, tb);
     double qh[SMAX];                          // first Hyper_RHS term of this thread's rows
 #pragma unroll
     for (int q = 0; q < SMAX; q++)
@@ -505,7 +524,7 @@ __device__ __noinline__ void problem_rhs(Smem<T, SMAX> &S, const Geo &G, const d
         double rd = radius(i, G);
         return rd * rd * (bh[i] - (2.0 / 3.0) * vh[i]) * (-S.Du[i] + 2.0 * u[i] / rd);
     });
-    line_op<T, SMAX>(S, OP_D1, n, G.fac1, k, tb);
+    line_op<T, SMAX>(S, OP_D1, n, G.fac1, tb);
 #pragma unroll
     for (int q = 0; q < SMAX; q++)
         if (q < cnt) {
@@ -551,7 +570,7 @@ __constant__ double c_beta2[6] = {1.1584888181285561688e-1, 3.728769905165286491
 // Compute_CFL + Compute_Tstep (src/lddrk4_nonperiodic_sf.f:7-146, x term),
 // then LDDRK4 (:376-468; no Fix_Pressure: its radial source is not shipped).
 template <int T, int SMAX>
-__device__ __noinline__ void problem_step(Smem<T, SMAX> &S, const Batch &B, int p, const K &k, const Tabs &tb) {
+__device__ __noinline__ void problem_step(Smem<T, SMAX> &S, const Batch &B, int p, const Tabs *__restrict__ tb) {
     const int n = B.n[p];
     const Geo G = geo(n, B.xl[p]);
     const size_t o = (size_t)B.off[p];
@@ -591,7 +610,7 @@ __device__ __noinline__ void problem_step(Smem<T, SMAX> &S, const Batch &B, int 
             else if (B.rk_mode == 1) { al = c_alpha2[K]; be = c_beta2[K]; }
             else { al = 0.0; be = 0.0; }
             const bool first = K == 0;          // QW = 0 at the loop start and alpha(1) = 0
-            problem_rhs<T, SMAX>(S, G, u, rho, s, hyp, gam, B.hyper, k, tb);
+            problem_rhs<T, SMAX>(S, G, u, rho, s, hyp, gam, B.hyper, tb);
             // update, then filter u, rho, s in place (Compact_Filter x pass)
             for (int i = t; i < n; i += T) {
                 const double d0 = S.Ru[i], d1 = S.Rr[i], d2 = S.Rs[i];
@@ -607,7 +626,7 @@ __device__ __noinline__ void problem_step(Smem<T, SMAX> &S, const Batch &B, int 
             for (int f = 0; f < 3; f++) {
                 double *F = f == 0 ? u : (f == 1 ? rho : s);
                 stage(S, n, [&](int i) { return F[i]; });
-                line_op<T, SMAX>(S, OP_FILT, n, 0.0, k, tb);
+                line_op<T, SMAX>(S, OP_FILT, n, 0.0, tb);
                 for (int q = 0; q < cnt; q++) F[a + q] = S.Y[a + q];
                 __syncthreads();
             }
@@ -622,7 +641,7 @@ __device__ __noinline__ void problem_step(Smem<T, SMAX> &S, const Batch &B, int 
 // from the queue counter and run nsteps steps of each; a problem whose step
 // counter is 0 first gets the set-up Compute_hyper (src/main.f:100).
 template <int T, int SMAX>
-__global__ void __launch_bounds__(T) k_rad_steps(Batch B, K k, Tabs tb, int first, int last, int nsteps,
+__global__ void __launch_bounds__(T) k_rad_steps(Batch B, const Tabs *__restrict__ tb, int first, int last, int nsteps,
                                                    int *queue) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T, SMAX> &S = *reinterpret_cast<Smem<T, SMAX> *>(smem_raw);
@@ -635,15 +654,15 @@ __global__ void __launch_bounds__(T) k_rad_steps(Batch B, K k, Tabs tb, int firs
         const int p = B.order[idx];
         if (B.step[p] == 0) {
             const size_t o = (size_t)B.off[p];
-            problem_hyper_core<T, SMAX>(S, geo(B.n[p], B.xl[p]), B.Q + 3 * o, B.hyp + 2 * o, k, tb);
+            problem_hyper_core<T, SMAX>(S, geo(B.n[p], B.xl[p]), B.Q + 3 * o, B.hyp + 2 * o, tb);
         }
-        for (int it = 0; it < nsteps; it++) problem_step<T, SMAX>(S, B, p, k, tb);
+        for (int it = 0; it < nsteps; it++) problem_step<T, SMAX>(S, B, p, tb);
     }
 }
 
 // Per-operator kernel for the C ABI's line operators: one CTA per problem.
 template <int T, int SMAX>
-__global__ void __launch_bounds__(T) k_rad_op(Batch B, K k, Tabs tb, int op, const double *F, double *O1,
+__global__ void __launch_bounds__(T) k_rad_op(Batch B, const Tabs *__restrict__ tb, int op, const double *F, double *O1,
                                                 double *O2, int iadd, double cadd) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T, SMAX> &S = *reinterpret_cast<Smem<T, SMAX> *>(smem_raw);
@@ -654,7 +673,7 @@ __global__ void __launch_bounds__(T) k_rad_op(Batch B, K k, Tabs tb, int op, con
     RAD_ROWS(T, n);
     if (op == OP_RHS || op == OP_HYPER) {
         const double *u = F + 3 * o, *rho = u + n, *s = rho + n;
-        problem_rhs<T, SMAX>(S, G, u, rho, s, B.hyp + 2 * o, B.gamma, op == OP_HYPER ? B.hyper : 0, k, tb);
+        problem_rhs<T, SMAX>(S, G, u, rho, s, B.hyp + 2 * o, B.gamma, op == OP_HYPER ? B.hyper : 0, tb);
         double *R = O1 + 3 * o;
         for (int i = threadIdx.x; i < n; i += T) { R[i] = S.Ru[i]; R[n + i] = S.Rr[i]; R[2 * n + i] = S.Rs[i]; }
         return;
@@ -662,12 +681,12 @@ __global__ void __launch_bounds__(T) k_rad_op(Batch B, K k, Tabs tb, int op, con
     const double *f = F + o;
     stage(S, n, [&](int i) { return f[i]; });
     const double fac = op == OP_D1 ? cadd * (1.0 / B.xl[p]) * (double)(n - 1) : G.fac2;
-    line_op<T, SMAX>(S, op, n, fac, k, tb);
+    line_op<T, SMAX>(S, op, n, fac, tb);
     double *out = (op == OP_D2 ? O2 : O1) + o;
     for (int q = 0; q < cnt; q++) out[a + q] = (op == OP_D1 && iadd == 1) ? out[a + q] + S.Y[a + q] : S.Y[a + q];
     if (op == OP_D2 && iadd == 1) {
         __syncthreads();
-        line_op<T, SMAX>(S, OP_D1, n, 1.0 * (1.0 / B.xl[p]) * (double)(n - 1), k, tb);
+        line_op<T, SMAX>(S, OP_D1, n, 1.0 * (1.0 / B.xl[p]) * (double)(n - 1), tb);
         for (int q = 0; q < cnt; q++) O1[o + a + q] = S.Y[a + q];
     }
 }
@@ -794,6 +813,7 @@ struct st_radial {
     double *tabs = nullptr;         // all factor tables in one allocation
     K k{};
     Tabs tb{};
+    Tabs *dtb = nullptr;            // device copy of tb
     long long launches = 0;
 };
 
@@ -826,7 +846,7 @@ static int launch_steps(st_radial *h, int first, int last, int nsteps, int *queu
     RCUDA(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev));
     int grid = std::max(1, std::min(per_sm * nsm, last - first));
     h->launches++;
-    k_rad_steps<T, SMAX><<<grid, T, sm, st>>>(make_batch(h), h->k, h->tb, first, last, nsteps, queue);
+    k_rad_steps<T, SMAX><<<grid, T, sm, st>>>(make_batch(h), h->dtb, first, last, nsteps, queue);
     RCUDA(h, cudaGetLastError());
     return ST_OK;
 }
@@ -866,7 +886,7 @@ static int launch_op(st_radial *h, int op, const double *F, double *O1, double *
     const size_t sm = smem_bytes<T, SMAX>();
     RCUDA(h, cudaFuncSetAttribute(k_rad_op<T, SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     h->launches++;
-    k_rad_op<T, SMAX><<<h->nprob, T, sm, h->stream>>>(make_batch(h), h->k, h->tb, op, F, O1, O2, iadd, cadd);
+    k_rad_op<T, SMAX><<<h->nprob, T, sm, h->stream>>>(make_batch(h), h->dtb, op, F, O1, O2, iadd, cadd);
     RCUDA(h, cudaGetLastError());
     RCUDA(h, cudaStreamSynchronize(h->stream));
     return ST_OK;
@@ -976,6 +996,12 @@ int st_radial_create(const st_radial_params *p, int nprob, const int *n, const d
     h->tb.L2 = T0 + o_l2; h->tb.I2 = T0 + o_i2; h->tb.U2 = T0 + o_u2;
     h->tb.P1 = T0 + o_f[0]; h->tb.P2 = T0 + o_f[1]; h->tb.Q1 = T0 + o_f[2]; h->tb.Q2 = T0 + o_f[3]; h->tb.IF = T0 + o_f[4];
     h->tb.T1 = T0 + o_t1; h->tb.T2 = T0 + o_t2; h->tb.TF = T0 + o_tf;
+    if (cudaMalloc((void **)&h->dtb, sizeof(Tabs)) != cudaSuccess ||
+        cudaMemcpy(h->dtb, &h->tb, sizeof(Tabs), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_k, &h->k, sizeof(K)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(ST_E_CUDA, "uploading the radial constants");
+    }
     *out = h;
     return ST_OK;
 }
@@ -985,7 +1011,7 @@ int st_radial_destroy(st_radial *h) {
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->aux) cudaStreamSynchronize(h->aux);
-    void *ptrs[] = {h->tabs, h->off, h->n, h->order, h->step, h->queue, h->xl, h->time, h->Q, h->QW, h->hyp};
+    void *ptrs[] = {h->tabs, h->dtb, h->off, h->n, h->order, h->step, h->queue, h->xl, h->time, h->Q, h->QW, h->hyp};
     for (void *q : ptrs) if (q) cudaFree(q);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
