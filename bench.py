@@ -300,6 +300,89 @@ def run_radial(args, rank, world, local, dist):
     b.close()
 
 
+# ---------------------------------------------------------------- serving
+SRV_SIZES = (64, 96, 128, 192, 256)
+SRV_WEIGHTS = (0.3, 0.25, 0.2, 0.15, 0.1)
+
+
+def serving_requests(nreq, steps, rate, seed):
+    """Seeded Poisson stream: grid size by the weights above, blast pressure
+    ratio uniform in [10, 200], seeded turbulence (k0 = 8, M_t = 0.1)."""
+    import numpy as np
+    from shock_turbulence_b200 import default_params
+    from shock_turbulence_b200.initial import blast_in_turbulence
+    from shock_turbulence_b200.serving import Request
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        n = int(rng.choice(SRV_SIZES, p=SRV_WEIGHTS))
+        pr = float(rng.uniform(10.0, 200.0))
+        Q, Y = blast_in_turbulence(default_params(n), k0=8.0, mach_t=0.1, p_ratio=pr, radius_cells=4.0,
+                                   seed=int(rng.integers(1 << 30)))
+        out.append(Request(i, n, steps, Q, Y, arrival=t))
+    return out
+
+
+def run_serving(args, rank, world, local, dist):
+    """The serving configuration: Poisson arrivals (20 requests/s) of blast
+    cases of mixed grid sizes, 100 LDDRK4 steps each, admitted by a 150 GB HBM
+    budget, device-resident, stepped concurrently (one stream and one graph
+    per slot).  value = aggregate cell-steps/s over the run's makespan."""
+    steps = args.steps if "--steps" in sys.argv else 100
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        rate, el = oracle_rate(64, 2, 1, threads)
+        print(json.dumps({
+            "impl": "reference", "metric": "Mcell-steps/s (serving: mixed-size blast cases)", "value": rate,
+            "unit": UNIT, "n_gpus": args.gpus, "steps": 2, "warmup": 1, "ms_per_step": el / 2 * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "CPU oracle on a 64^3 case of the stream (one case at a time)"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"64^3 case, 1 warm-up + 2 steps, {threads} OpenMP threads"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    from shock_turbulence_b200.serving import Server, summarize
+    torch.cuda.set_device(local)
+    reqs = serving_requests(args.requests, steps, 20.0, seed=4 + rank)
+    srv = Server(hbm_budget=150e9)
+    # warm the slot kinds once (not timed): context creation, scratch pools, graphs
+    clocks = ClockSampler(gpu_smi_id(local))
+    clocks.start()
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    summ = summarize(res)
+    rate = max_over = summ["mcell_steps_per_s"]
+    if dist is not None:
+        from shock_turbulence_b200.replicas import max_over_ranks
+        max_over = max_over_ranks(summ["makespan_s"], dist, "cuda")
+        rate = world * sum(r.n ** 3 * r.steps for r in res) / max_over / 1e6
+    h2d = sum(6 * r.n ** 3 * 8 for r in res)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Mcell-steps/s (serving: mixed-size blast cases, 100 LDDRK4 steps each)", "value": rate,
+            "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded blast-in-turbulence requests)",
+            "config": {"workload": f"{args.requests} requests, Poisson arrivals at 20/s, grid sizes {SRV_SIZES} with "
+                                   f"weights {SRV_WEIGHTS}, pressure ratio uniform in [10, 200], 150 GB HBM budget",
+                       "p50_s": summ["p50_s"], "p99_s": summ["p99_s"], "mean_s": summ["mean_s"],
+                       "makespan_s": summ["makespan_s"], "slots_created": len(srv.slots),
+                       "sizes": [r.n for r in sorted(res, key=lambda r: r.rid)]},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": h2d / max(1, steps * len(res)),
+                    "d2h_bytes_per_step": h2d / max(1, steps * len(res)),
+                    "note": "time to solution includes each case's state upload and final download"},
+            "gpu_launches": None, "roofline": None, "cpu_baseline": None, "clocks": clk,
+            "wall_s": wall}), flush=True)
+    srv.close()
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -311,8 +394,10 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=96, help="grid of the CPU-oracle sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "radial"],
-                    help="blast3d: the 384^3 octant case; radial: the batch of 4096 1-D radial blasts")
+    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "radial", "serving"],
+                    help="blast3d: the 384^3 octant case; radial: the batch of 4096 1-D radial blasts; "
+                         "serving: a Poisson stream of mixed-size blast cases through the serving loop")
+    ap.add_argument("--requests", type=int, default=16, help="serving workload: number of requests")
     ap.add_argument("--nprob", type=int, default=4096, help="radial workload: number of problems")
     args = ap.parse_args()
     if args.workload == "radial" and "--steps" not in sys.argv:
@@ -333,6 +418,11 @@ def main():
 
     if args.workload == "radial":
         run_radial(args, rank, world, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    if args.workload == "serving":
+        run_serving(args, rank, world, local, dist)
         if dist is not None:
             dist.destroy_process_group()
         return

@@ -248,6 +248,19 @@ int  st_step(st_ctx *c, double *time, int *step);
 int  st_get_monitors(st_ctx *c, double out[10]);
 /* Synchronises the context stream. */
 int  st_sync(st_ctx *c);
+/* No reference counterpart: the main-loop step of st_step enqueued on the
+ * context stream without waiting (time advances in device memory; st_set_time
+ * sets it, st_get_time waits and reads it).  step is the caller's step
+ * counter (Compute_Tstep uses it); from step 2 on the step replays a CUDA
+ * graph captured on the first such call, so it costs one launch.  st_query
+ * returns 1 when the context's work has finished, 0 while it runs. */
+int  st_step_async(st_ctx *c, int step);
+int  st_get_time(st_ctx *c, double *time);
+int  st_set_time(st_ctx *c, double time);
+int  st_query(st_ctx *c);
+/* No reference counterpart: device bytes the context holds (COMMON mirrors,
+ * scratch pool, tables); the pool grows during the first steps. */
+int  st_memory(st_ctx *c, long long *bytes);
 
 /* ---- 1-D spherical-radial family, batched ---------------------------------
  * Many independent problems, each one run of the reference's radial program

@@ -45,6 +45,11 @@ SIGNATURES = {
     "st_step": [_ctx, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
     "st_get_monitors": [_ctx, _dp],
     "st_sync": [_ctx],
+    "st_step_async": [_ctx, ctypes.c_int],
+    "st_get_time": [_ctx, ctypes.POINTER(ctypes.c_double)],
+    "st_set_time": [_ctx, ctypes.c_double],
+    "st_query": [_ctx],
+    "st_memory": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
     "st_set_stream": [_ctx, ctypes.c_void_p],
     "st_get_stream": [_ctx, ctypes.POINTER(ctypes.c_void_p)],
     "st_profile": [_ctx, ctypes.c_int],

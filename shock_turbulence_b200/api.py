@@ -178,6 +178,25 @@ class Solver:
         self._check(self.lib.st_step(self._h, ctypes.byref(t), ctypes.byref(s)), "step")
         return t.value, s.value
 
+    def step_async(self, step):
+        """Enqueue one main-loop step without waiting (graph replay from step 2)."""
+        self._check(self.lib.st_step_async(self._h, int(step)), "st_step_async")
+
+    def get_time(self):
+        t = ctypes.c_double()
+        self._check(self.lib.st_get_time(self._h, ctypes.byref(t)), "st_get_time")
+        return t.value
+
+    def set_time(self, t):
+        self._check(self.lib.st_set_time(self._h, float(t)), "st_set_time")
+
+    def done(self):
+        """True when every operation enqueued on the context has finished."""
+        st = self.lib.st_query(self._h)
+        if st < 0:
+            self._check(st, "st_query")
+        return st == 1
+
     def monitors(self):
         out = np.zeros(10)
         self._check(self.lib.st_get_monitors(self._h, out.ctypes.data), "st_get_monitors")

@@ -224,6 +224,7 @@ int st_destroy(st_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &r : c->prec) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : c->evpool) cudaEventDestroy(e);
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     free_tables(c);
     double *arrs[] = {c->Q, c->dQ, c->QW, c->Y, c->drYi, c->rYW, c->gamma_eff, c->dscal};
     for (double *a : arrs) if (a) cudaFree(a);
@@ -670,6 +671,84 @@ int st_step(st_ctx *c, double *time, int *step) {
     *step = *step + 1;
     return ST_OK;
     API_END(c)
+}
+
+// the main-loop body without host synchronisation (dt and time stay on the device)
+static int enqueue_step(st_ctx *c, int step) {
+    ST_TRY(dev_compute_cfl(c, c->Q, false, nullptr, nullptr));
+    ST_TRY(dev_compute_tstep(c, c->Q, c->Y, step, true, 0.0));
+    ST_TRY(dev_lddrk4(c, true));
+    return ST_OK;
+}
+
+int st_step_async(st_ctx *c, int step) {
+    if (step < 0) return ST_E_ARG;
+    API_BEGIN(c)
+    // Compute_Tstep's branch depends on the step number only up to step 2;
+    // from then on every step is the same sequence of launches on the same
+    // buffers, captured once as a CUDA graph and replayed.
+    if (step < 2 || c->prof) return enqueue_step(c, step);
+    if (!c->step_graph) {
+        cudaGraph_t g = nullptr;
+        const long long l0 = c->launches;
+        ST_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(c, step);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->launches = l0;
+        if (rc != ST_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return fail(c, ST_E_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+        long long nk = 0;
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) nk++;
+        }
+        c->graph_kernels = nk;
+        e = cudaGraphInstantiate(&c->step_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { c->step_graph = nullptr; return fail(c, ST_E_CUDA, cudaGetErrorString(e)); }
+    }
+    ST_CUDA(c, cudaGraphLaunch(c->step_graph, c->stream));
+    c->launches += c->graph_kernels;
+    return ST_OK;
+    API_END(c)
+}
+
+int st_get_time(st_ctx *c, double *time) {
+    if (!time) return ST_E_ARG;
+    API_BEGIN(c)
+    return read_time(c, time);
+    API_END(c)
+}
+
+int st_set_time(st_ctx *c, double time) {
+    API_BEGIN(c)
+    c->hpinned[7] = time;
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + 7, c->hpinned + 7, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_memory(st_ctx *c, long long *bytes) {
+    if (!c || !bytes) return ST_E_ARG;
+    const size_t fb = c->dm.n3 * sizeof(double);
+    size_t b = 38 * fb + c->table_bytes + 16 * sizeof(double);   // COMMON mirrors, tables, scalars
+    for (auto &e : c->pool) b += (size_t)e.nf * fb;
+    *bytes = (long long)b;
+    return ST_OK;
+}
+
+int st_query(st_ctx *c) {
+    if (!c) return ST_E_ARG;
+    if (cudaSetDevice(c->dev) != cudaSuccess) return fail(c, ST_E_CUDA, "cudaSetDevice");
+    cudaError_t e = cudaStreamQuery(c->stream);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) { cudaGetLastError(); return 0; }
+    return fail(c, ST_E_CUDA, cudaGetErrorString(e));
 }
 
 int st_set_stream(st_ctx *c, void *stream) {

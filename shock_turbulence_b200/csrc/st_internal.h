@@ -110,6 +110,7 @@ struct st_ctx {
     st::TriTab tri[3][4];
     st::PenTab pen[3][2];
     std::vector<void *> table_allocs;
+    size_t table_bytes = 0;
     // COMMON blocks
     double *Q = nullptr, *dQ = nullptr, *QW = nullptr;
     double *Y = nullptr, *drYi = nullptr, *rYW = nullptr, *gamma_eff = nullptr;
@@ -128,6 +129,8 @@ struct st_ctx {
     cudaStream_t own_stream = nullptr;
     // instrumentation
     long long launches = 0;
+    cudaGraphExec_t step_graph = nullptr;   // captured main-loop step (st_step_async)
+    long long graph_kernels = 0;            // kernels in one replay of step_graph
     bool prof = false;
     struct ProfRec { const char *name; double bytes; cudaEvent_t a, b; };
     std::vector<ProfRec> prec;

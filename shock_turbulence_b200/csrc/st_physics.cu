@@ -860,9 +860,8 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
     // hyperviscous limits from the first step on (_mf) or the second (periodic)
     const bool use_hyper = c->p.hyper_param == 1 && step > (sf ? 1 : 0);
     if (use_hyper) {
-        const double inf = INFINITY;
-        double init[4] = {inf, inf, inf, inf};
-        ST_CUDA(c, cudaMemcpyAsync(c->dscal + 2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+        // minima start at +inf (a device fill, so that the step can be captured in a graph)
+        ST_TRY(dev_fill(c, c->dscal + 2, 4, INFINITY));
         if (sf) {
             int pi = prof_start(c, "k_tstep", 64.0 * c->dm.n3);
             k_tstep_sf<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, c->hyp[H_VISC], c->hyp[H_BETA],

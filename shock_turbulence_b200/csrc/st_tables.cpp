@@ -351,6 +351,7 @@ static const double *upload(st_ctx *c, const std::vector<double> &v, int *err) {
     void *p = nullptr;
     if (cudaMalloc(&p, v.size() * sizeof(double)) != cudaSuccess) { *err = 1; return nullptr; }
     c->table_allocs.push_back(p);
+    c->table_bytes += v.size() * sizeof(double);
     if (cudaMemcpy(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
         *err = 1;
     return (const double *)p;
