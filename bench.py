@@ -30,12 +30,15 @@ METRIC = "Mcell-steps/s (FP64 RHS+LDDRK4 step, 10 RK stages/step)"
 UNIT = "Mcell-steps/s"
 
 
-def make_params(n, device=0):
+def make_params(n, device=0, precision=0):
     from shock_turbulence_b200 import default_params
     # config: Re = 100 with the molecular viscous term added (re > 0),
     # Pr = 0.7, artificial viscosity on, CFL 0.5, bulk coefficient scale 1.75
     return default_params(n, re=100.0, re1=100.0, re2=100.0, pr=0.7, hyper_param=1, cfl_cal=0.5,
-                          c_beta_scale=1.75, device=device)
+                          c_beta_scale=1.75, device=device, precision=precision)
+
+
+METRIC_FP32 = "Mcell-steps/s (FP32-mode RHS+LDDRK4 step, 10 RK stages/step)"
 
 
 def make_state(p, seed):
@@ -349,7 +352,9 @@ def run_serving(args, rank, world, local, dist):
     from shock_turbulence_b200.serving import Server, summarize
     torch.cuda.set_device(local)
     reqs = serving_requests(args.requests, steps, 20.0, seed=4 + rank)
-    srv = Server(hbm_budget=150e9)
+    fp32 = args.precision == "fp32"
+    from shock_turbulence_b200.serving import _gpu_solver_factory
+    srv = Server(hbm_budget=150e9, make_solver=_gpu_solver_factory(precision=1 if fp32 else 0))
     # warm the slot kinds once (not timed): context creation, scratch pools, graphs
     clocks = ClockSampler(gpu_smi_id(local))
     clocks.start()
@@ -368,7 +373,8 @@ def run_serving(args, rank, world, local, dist):
         print(json.dumps({
             "metric": "Mcell-steps/s (serving: mixed-size blast cases, 100 LDDRK4 steps each)", "value": rate,
             "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 intermediates / f64 state" if fp32 else "f64",
             "data": "synthetic (seeded blast-in-turbulence requests)",
             "config": {"workload": f"{args.requests} requests, Poisson arrivals at 20/s, grid sizes {SRV_SIZES} with "
                                    f"weights {SRV_WEIGHTS}, pressure ratio uniform in [10, 200], 150 GB HBM budget",
@@ -383,6 +389,82 @@ def run_serving(args, rank, world, local, dist):
     srv.close()
 
 
+# ---------------------------------------------------------------- precision
+def run_precision(args, rank, world, local, dist):
+    """The precision configuration: the 384^3 blast case and a 512^3 periodic
+    turbulence box, each run in FP64 and in the FP32 mode from the same
+    initial state for `steps` steps (default 100); reports relative L2 and
+    Linf error per conserved field and the FP32/FP64 speed of each."""
+    steps = args.steps if "--steps" in sys.argv else 100
+    if args.impl == "reference" or rank != 0:
+        if args.impl == "reference" and rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the precision workload compares two GPU runs; "
+                                                                 "the CPU reference arm is the blast3d workload"}))
+        return
+    import torch
+    from shock_turbulence_b200 import PRECISION_FP32, PRECISION_FP64, Solver, periodic_params
+    from shock_turbulence_b200.initial import periodic_turbulence
+    from shock_turbulence_b200.precision import field_errors, worst
+    torch.cuda.set_device(local)
+    cases = []
+    n_blast = args.n
+    n_per = args.periodic_n
+    cases.append(("blast", n_blast, lambda prec: make_params(n_blast, device=local, precision=prec),
+                  lambda p: make_state(p, seed=1)))
+    cases.append(("periodic", n_per, lambda prec: periodic_params(n_per, device=local, precision=prec),
+                  lambda p: (periodic_turbulence(p, k0=8.0, urms=0.1, seed=3), None)))
+    out = {}
+    clocks = ClockSampler(gpu_smi_id(local))
+    clocks.start()
+    for name, n, mk, init in cases:
+        p64 = mk(PRECISION_FP64)
+        Q0, Y0 = init(p64)
+        res = {}
+        for prec in (PRECISION_FP64, PRECISION_FP32):
+            p = mk(prec)
+            s = Solver(p)
+            stream = torch.cuda.current_stream()
+            s._check(s.lib.st_set_stream(s._h, stream.cuda_stream), "st_set_stream")
+            s.set_state(Q0, Y0 if name == "blast" else None)
+            if name == "blast":
+                s.Compute_gamma(Y0)
+            s.Compute_hyper(Q0, Y0 if name == "blast" else None)
+            t, k = 0.0, 0
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                t, k = s.step(t, k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            Q, Y = s.get_state()
+            res[prec] = (Q, Y, t, ms)
+            s.close()
+            del s
+        Q64, Y64, t64, ms64 = res[PRECISION_FP64]
+        Q32, Y32, t32, ms32 = res[PRECISION_FP32]
+        errs = field_errors(Q32, Q64, Y32 if name == "blast" else None, Y64 if name == "blast" else None)
+        l2, linf = worst(errs)
+        out[name] = {"grid": n, "steps": steps, "fp64_ms_per_step": ms64 / steps, "fp32_ms_per_step": ms32 / steps,
+                     "fp64_mcell_steps_per_s": n ** 3 * steps / (ms64 / 1e3) / 1e6,
+                     "fp32_mcell_steps_per_s": n ** 3 * steps / (ms32 / 1e3) / 1e6,
+                     "speedup_fp32": ms64 / ms32, "time_fp64": t64, "time_fp32": t32,
+                     "errors": {k: {"l2_rel": v[0], "linf_rel": v[1]} for k, v in errs.items()},
+                     "worst_l2_rel": l2, "worst_linf_rel": linf}
+        del Q0, Y0, res
+    clk = clocks.stop()
+    b = out["blast"]
+    print(json.dumps({
+        "metric": METRIC_FP32, "value": b["fp32_mcell_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": 0, "ms_per_step": b["fp32_ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 intermediates / f64 state", "data": "synthetic",
+        "config": {"workload": f"precision: {n_blast}^3 blast and {n_per}^3 periodic box, FP64 and FP32-mode runs "
+                               f"from the same state, {steps} steps each; relative L2/Linf per conserved field",
+                   "cases": out},
+        "clocks": clk}), flush=True)
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -394,9 +476,13 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=96, help="grid of the CPU-oracle sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "radial", "serving"],
+    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "radial", "serving", "precision"],
                     help="blast3d: the 384^3 octant case; radial: the batch of 4096 1-D radial blasts; "
-                         "serving: a Poisson stream of mixed-size blast cases through the serving loop")
+                         "serving: a Poisson stream of mixed-size blast cases through the serving loop; "
+                         "precision: FP64 against FP32-mode runs of the 384^3 blast and a 512^3 periodic box")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="blast3d and serving: FP64, or the FP32 mode (float intermediates, double state)")
+    ap.add_argument("--periodic-n", type=int, default=512, help="precision workload: periodic box grid")
     ap.add_argument("--requests", type=int, default=16, help="serving workload: number of requests")
     ap.add_argument("--nprob", type=int, default=4096, help="radial workload: number of problems")
     args = ap.parse_args()
@@ -426,6 +512,11 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+    if args.workload == "precision":
+        run_precision(args, rank, world, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         run_reference(args, rank)
@@ -436,7 +527,8 @@ def main():
     from shock_turbulence_b200 import Solver
     from shock_turbulence_b200.replicas import aggregate_rate, max_over_ranks, replica_seed
     torch.cuda.set_device(local)
-    p = make_params(args.n, device=local)
+    fp32 = args.precision == "fp32"
+    p = make_params(args.n, device=local, precision=1 if fp32 else 0)
     Q, Y = make_state(p, seed=replica_seed(1, rank))
     s = Solver(p)
     stream = torch.cuda.current_stream()
@@ -533,11 +625,12 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC_FP32 if fp32 else METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 intermediates / f64 state" if fp32 else "f64",
             "data": "synthetic (seeded solenoidal turbulence + Gaussian blast)",
-            "config": {"workload": f"blast wave in isotropic turbulence, {args.n}^3 octant, FP64, two-species _mf "
+            "config": {"workload": f"blast wave in isotropic turbulence, {args.n}^3 octant, "
+                                   f"{'FP32 mode' if fp32 else 'FP64'}, two-species _mf "
                                    "physics (Y=1), Re=100 viscous term on, artificial viscosity on, CFL 0.5",
                        "grid": args.n, "cells": cells, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (one field is %.0f MB)" % (cells * 8 / 1e6),

@@ -74,10 +74,22 @@ typedef struct st_params {
                                    re its Reynolds number (re1 is ignored), and
                                    x_leng = period_x*(nx-1)/nx as Define_Param
                                    sets it (src/define_periodic_sf.f:42).      */
+    int    precision;           /* ST_PRECISION_FP64: every array in double
+                                   (the reference's REAL*8 build);
+                                   ST_PRECISION_FP32: the derivative, filter,
+                                   artificial-viscosity and RHS intermediates
+                                   (/GRAD/, /HYPER/, dQ, drYi and the scratch
+                                   fields) are stored in float, while the state
+                                   Q, Y, the LDDRK4 accumulators QW, rYW, the
+                                   compact filter of the state and the pressure
+                                   recovery (Fix_Pressure) stay double.  No
+                                   counterpart in the reference.               */
 } st_params;
 
 #define ST_FAMILY_MF        0
 #define ST_FAMILY_PERIODIC  1
+#define ST_PRECISION_FP64   0
+#define ST_PRECISION_FP32   1
 
 typedef struct st_ctx st_ctx;
 

@@ -18,17 +18,17 @@ struct OomError : std::runtime_error {
     OomError() : std::runtime_error("device scratch allocation failed") {}
 };
 
-double *scratch(st_ctx *c, int nf) {
+void *scratch_bytes(st_ctx *c, size_t bytes) {
     for (auto &e : c->pool)
-        if (!e.used && e.nf == nf) { e.used = true; return e.p; }
+        if (!e.used && e.bytes == bytes) { e.used = true; return e.p; }
     void *p = nullptr;
-    if (cudaMalloc(&p, (size_t)nf * c->dm.n3 * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
         cudaGetLastError();
         c->pool_oom = true;
         throw OomError();
     }
-    c->pool.push_back({(double *)p, nf, true});
-    return (double *)p;
+    c->pool.push_back({p, bytes, true});
+    return p;
 }
 
 int prof_start(st_ctx *c, const char *name, double bytes) {
@@ -48,7 +48,7 @@ void prof_stop(st_ctx *c, int idx) {
     if (idx >= 0) cudaEventRecord(c->prec[idx].b, c->stream);
 }
 
-void release(st_ctx *c, double *p) {
+void release(st_ctx *c, const void *p) {
     for (auto &e : c->pool)
         if (e.p == p) { e.used = false; return; }
 }
@@ -147,6 +147,7 @@ void st_default_params(st_params *p, int nx, int ny, int nz) {
     p->bulk_ratio = 0.0; p->t_ratio = 1.0;
     p->hyper_param = 1; p->rk_mode = 0; p->cfl_cal = 0.5; p->c_beta_scale = 1.0; p->device = 0;
     p->family = ST_FAMILY_MF;
+    p->precision = ST_PRECISION_FP64;
 }
 
 int st_create(const st_params *p, st_ctx **out) {
@@ -157,6 +158,7 @@ int st_create(const st_params *p, st_ctx **out) {
     if (p->device < 0 || p->device >= ndev) return ST_E_ARG;
     if (p->family != ST_FAMILY_MF && p->family != ST_FAMILY_PERIODIC) return ST_E_ARG;
     if (p->rk_mode != 0 && p->rk_mode != 1) return ST_E_ARG;
+    if (p->precision != ST_PRECISION_FP64 && p->precision != ST_PRECISION_FP32) return ST_E_ARG;
     const int n[3] = {p->nx, p->ny, p->nz};
     for (int d = 0; d < 3; d++)
         if (n[d] % kLanes != 0 || n[d] < kLanes || choose_seg(n[d]) == 0) return ST_E_UNSUPPORTED;
@@ -200,11 +202,20 @@ int st_create(const st_params *p, st_ctx **out) {
     const size_t b = c->dm.n3 * sizeof(double);
     auto al = [&](double **q, int nf) { return cudaMalloc((void **)q, nf * b) == cudaSuccess &&
                                               cudaMemset(*q, 0, nf * b) == cudaSuccess; };
-    bool ok = al(&c->Q, 5) && al(&c->dQ, 5) && al(&c->QW, 5) && al(&c->Y, 1) && al(&c->drYi, 1) &&
-              al(&c->rYW, 1) && al(&c->gamma_eff, 1);
-    for (int g = 0; g < 12 && ok; g++) ok = al(&c->grad[g], 1);
-    for (int h = 0; h < 4 && ok; h++) ok = al(&c->hyp[h], 1);
-    for (int h = 0; h < 3 && ok; h++) ok = al(&c->dYd[h], 1);
+    auto alf = [&](float **q, int nf) { return cudaMalloc((void **)q, nf * b / 2) == cudaSuccess &&
+                                               cudaMemset(*q, 0, nf * b / 2) == cudaSuccess; };
+    bool ok = al(&c->Q, 5) && al(&c->QW, 5) && al(&c->Y, 1) && al(&c->rYW, 1) && al(&c->gamma_eff, 1);
+    if (p->precision == ST_PRECISION_FP32) {
+        ok = ok && alf(&c->dQf, 5) && alf(&c->drYif, 1);
+        for (int g = 0; g < 12 && ok; g++) ok = alf(&c->gradf[g], 1);
+        for (int h = 0; h < 4 && ok; h++) ok = alf(&c->hypf[h], 1);
+        for (int h = 0; h < 3 && ok; h++) ok = alf(&c->dYdf[h], 1);
+    } else {
+        ok = ok && al(&c->dQ, 5) && al(&c->drYi, 1);
+        for (int g = 0; g < 12 && ok; g++) ok = al(&c->grad[g], 1);
+        for (int h = 0; h < 4 && ok; h++) ok = al(&c->hyp[h], 1);
+        for (int h = 0; h < 3 && ok; h++) ok = al(&c->dYd[h], 1);
+    }
     ok = ok && cudaMalloc((void **)&c->dscal, 16 * sizeof(double)) == cudaSuccess &&
          cudaMemset(c->dscal, 0, 16 * sizeof(double)) == cudaSuccess &&
          cudaMallocHost((void **)&c->hpinned, 16 * sizeof(double)) == cudaSuccess;
@@ -231,6 +242,11 @@ int st_destroy(st_ctx *c) {
     for (double *a : c->grad) if (a) cudaFree(a);
     for (double *a : c->hyp) if (a) cudaFree(a);
     for (double *a : c->dYd) if (a) cudaFree(a);
+    float *farrs[] = {c->dQf, c->drYif};
+    for (float *a : farrs) if (a) cudaFree(a);
+    for (float *a : c->gradf) if (a) cudaFree(a);
+    for (float *a : c->hypf) if (a) cudaFree(a);
+    for (float *a : c->dYdf) if (a) cudaFree(a);
     for (auto &e : c->pool) cudaFree(e.p);
     if (c->hpinned) cudaFreeHost(c->hpinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -255,9 +271,14 @@ int st_set_state(st_ctx *c, const double *Q, const double *Y) {
     // the periodic family has no species: its Y stays 1
     if (c->p.family != ST_FAMILY_PERIODIC) ST_CUDA(c, cudaMemcpyAsync(c->Y, Y, b, cudaMemcpyDefault, c->stream));
     ST_CUDA(c, cudaMemsetAsync(c->QW, 0, 5 * b, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(c->dQ, 0, 5 * b, c->stream));
+    if (fp32_mode(c)) {
+        ST_CUDA(c, cudaMemsetAsync(c->dQf, 0, 5 * b / 2, c->stream));
+        ST_CUDA(c, cudaMemsetAsync(c->drYif, 0, b / 2, c->stream));
+    } else {
+        ST_CUDA(c, cudaMemsetAsync(c->dQ, 0, 5 * b, c->stream));
+        ST_CUDA(c, cudaMemsetAsync(c->drYi, 0, b, c->stream));
+    }
     ST_CUDA(c, cudaMemsetAsync(c->rYW, 0, b, c->stream));
-    ST_CUDA(c, cudaMemsetAsync(c->drYi, 0, b, c->stream));
     ST_CUDA(c, cudaMemsetAsync(c->dscal + 7, 0, sizeof(double), c->stream));
     ST_CUDA(c, cudaStreamSynchronize(c->stream));
     return ST_OK;
@@ -295,18 +316,20 @@ int st_get_tstep(st_ctx *c, double *t) {
     API_END(c)
 }
 
-static double *common_ptr(st_ctx *c, const char *name, int *nf) {
+// COMMON array by name: a double array, or (FP32 mode) a float one in *pf
+static double *common_ptr(st_ctx *c, const char *name, int *nf, float **pf) {
     static const char *gn[12] = {"dux_dx", "duy_dx", "duz_dx", "dux_dy", "duy_dy", "duz_dy",
                                  "dux_dz", "duy_dz", "duz_dz", "dTdx", "dTdy", "dTdz"};
     static const char *hn[4] = {"beta_hyper", "visc_hyper", "k_hyper", "D_hyper"};
     *nf = 1;
-    for (int q = 0; q < 12; q++) if (!std::strcmp(name, gn[q])) return c->grad[q];
-    for (int q = 0; q < 4; q++) if (!std::strcmp(name, hn[q])) return c->hyp[q];
+    *pf = nullptr;
+    for (int q = 0; q < 12; q++) if (!std::strcmp(name, gn[q])) { *pf = c->gradf[q]; return c->grad[q]; }
+    for (int q = 0; q < 4; q++) if (!std::strcmp(name, hn[q])) { *pf = c->hypf[q]; return c->hyp[q]; }
     if (!std::strcmp(name, "gamma_eff")) return c->gamma_eff;
-    if (!std::strcmp(name, "drYi")) return c->drYi;
+    if (!std::strcmp(name, "drYi")) { *pf = c->drYif; return c->drYi; }
     if (!std::strcmp(name, "rYW")) return c->rYW;
     *nf = 5;
-    if (!std::strcmp(name, "dQ")) return c->dQ;
+    if (!std::strcmp(name, "dQ")) { *pf = c->dQf; return c->dQ; }
     if (!std::strcmp(name, "QW")) return c->QW;
     return nullptr;
 }
@@ -315,8 +338,16 @@ int st_get_common(st_ctx *c, const char *name, double *out) {
     if (!name || !out) return ST_E_ARG;
     API_BEGIN(c)
     int nf;
-    double *p = common_ptr(c, name, &nf);
-    if (!p) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    float *pf;
+    double *p = common_ptr(c, name, &nf, &pf);
+    if (!p && !pf) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    if (pf) {   // FP32 mode: widened on the device
+        Scratch t(c, nf);
+        ST_TRY(dev_to_double(c, pf, t, nf * c->dm.n3));
+        ST_CUDA(c, cudaMemcpyAsync(out, t, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
+        ST_CUDA(c, cudaStreamSynchronize(c->stream));
+        return ST_OK;
+    }
     ST_CUDA(c, cudaMemcpyAsync(out, p, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
     ST_CUDA(c, cudaStreamSynchronize(c->stream));
     return ST_OK;
@@ -327,8 +358,16 @@ int st_set_common(st_ctx *c, const char *name, const double *in) {
     if (!name || !in) return ST_E_ARG;
     API_BEGIN(c)
     int nf;
-    double *p = common_ptr(c, name, &nf);
-    if (!p) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    float *pf;
+    double *p = common_ptr(c, name, &nf, &pf);
+    if (!p && !pf) return fail(c, ST_E_ARG, std::string("unknown COMMON array ") + name);
+    if (pf) {   // FP32 mode: rounded to float on the device
+        Scratch t(c, nf);
+        ST_CUDA(c, cudaMemcpyAsync(t, in, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
+        ST_TRY(dev_to_float(c, t, pf, nf * c->dm.n3));
+        ST_CUDA(c, cudaStreamSynchronize(c->stream));
+        return ST_OK;
+    }
     ST_CUDA(c, cudaMemcpyAsync(p, in, nf * c->dm.n3 * 8, cudaMemcpyDefault, c->stream));
     ST_CUDA(c, cudaStreamSynchronize(c->stream));
     return ST_OK;
@@ -736,8 +775,11 @@ int st_set_time(st_ctx *c, double time) {
 int st_memory(st_ctx *c, long long *bytes) {
     if (!c || !bytes) return ST_E_ARG;
     const size_t fb = c->dm.n3 * sizeof(double);
-    size_t b = 38 * fb + c->table_bytes + 16 * sizeof(double);   // COMMON mirrors, tables, scalars
-    for (auto &e : c->pool) b += (size_t)e.nf * fb;
+    // COMMON mirrors (13 double state fields; 25 intermediate fields, float in
+    // the FP32 mode), tables, scalars and the scratch pool
+    const size_t ib = fp32_mode(c) ? fb / 2 : fb;
+    size_t b = 13 * fb + 25 * ib + c->table_bytes + 16 * sizeof(double);
+    for (auto &e : c->pool) b += e.bytes;
     *bytes = (long long)b;
     return ST_OK;
 }

@@ -74,11 +74,14 @@ enum ProdOp {
     PR_SPEC,         // a*b*c + a*c*k0*k1             (Species_RHS flux)
     PR_SPECT,        // (k0*d)*(a*b*c + a*c*k0b*k1)    (its energy counterpart)
 };
-struct Prod {
+template <class T>
+struct ProdT {
     int op;
-    const double *a, *b, *c, *d;
+    const T *a, *b, *c, *d;     // fields (double, or float in the FP32 mode)
     double k0, k1, k2;
 };
+using Prod = ProdT<double>;
+using ProdF = ProdT<float>;
 
 enum { G_DUX_DX, G_DUY_DX, G_DUZ_DX, G_DUX_DY, G_DUY_DY, G_DUZ_DY,
        G_DUX_DZ, G_DUY_DZ, G_DUZ_DZ, G_DTDX, G_DTDY, G_DTDZ };
@@ -117,8 +120,16 @@ struct st_ctx {
     double *grad[12] = {nullptr};
     double *hyp[4] = {nullptr};
     double *dYd[3] = {nullptr};
-    // scratch field pool
-    struct PoolEntry { double *p; int nf; bool used; };
+    // FP32 mode (precision ST_PRECISION_FP32): the same arrays in float; the
+    // double ones above stay unallocated (the state Q, QW, Y, rYW and
+    // gamma_eff are double in both modes)
+    float *dQf = nullptr, *drYif = nullptr;
+    float *gradf[12] = {nullptr};
+    float *hypf[4] = {nullptr};
+    float *dYdf[3] = {nullptr};
+    // scratch field pool (entries of any byte size; float and double requests
+    // of the same size share entries)
+    struct PoolEntry { void *p; size_t bytes; bool used; };
     std::vector<PoolEntry> pool;
     bool pool_oom = false;
     // device scalars (reductions, dt)
@@ -164,24 +175,39 @@ void free_tables(st_ctx *c);
 void fill_consts(Consts &k);
 
 // scratch pool
-double *scratch(st_ctx *c, int nfields = 1);   // nfields contiguous N^3 fields
-void release(st_ctx *c, double *p);
-struct Scratch {                                 // RAII helper
-    st_ctx *c; double *p;
-    explicit Scratch(st_ctx *cc, int nf = 1) : c(cc), p(scratch(cc, nf)) {}
-    ~Scratch() { release(c, p); }
-    Scratch(const Scratch &) = delete;
-    Scratch &operator=(const Scratch &) = delete;
-    operator double *() const { return p; }
+void *scratch_bytes(st_ctx *c, size_t bytes);
+inline double *scratch(st_ctx *c, int nfields = 1) {   // nfields contiguous N^3 double fields
+    return (double *)scratch_bytes(c, (size_t)nfields * c->dm.n3 * sizeof(double));
+}
+template <class R>
+inline R *scratch_t(st_ctx *c, int nfields) { return (R *)scratch_bytes(c, (size_t)nfields * c->dm.n3 * sizeof(R)); }
+void release(st_ctx *c, const void *p);
+template <class R>
+struct ScratchT {                                // RAII helper
+    st_ctx *c; R *p;
+    explicit ScratchT(st_ctx *cc, int nf = 1) : c(cc), p(scratch_t<R>(cc, nf)) {}
+    ~ScratchT() { release(c, p); }
+    ScratchT(const ScratchT &) = delete;
+    ScratchT &operator=(const ScratchT &) = delete;
+    operator R *() const { return p; }
 };
+using Scratch = ScratchT<double>;
+inline bool fp32_mode(const st_ctx *c) { return c->p.precision == ST_PRECISION_FP32; }
 
 // line operators on device arrays (st_kernels.cu)
 int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd);
 int dev_dfd_prod(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int iadd, double cadd);
+// FP32-field variants (FP32 mode): same operators, float inputs and outputs
+int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd, double cadd);
+int dev_dfd_prod_f(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd);
+int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd);
+int dev_gauss_f(st_ctx *c, int dir, const float *F, float *Fg);
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd);
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0);
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg);
 int dev_fill(st_ctx *c, double *x, size_t n, double v);
+int dev_to_float(st_ctx *c, const double *x, float *y, size_t n);
+int dev_to_double(st_ctx *c, const float *x, double *y, size_t n);
 int dev_tridiagonal(st_ctx *c, const double *A, const double *B, const double *C, double *R,
                     int n, int lot, int nper);
 int dev_pentadiagonal(st_ctx *c, const double *A, const double *B, const double *C,

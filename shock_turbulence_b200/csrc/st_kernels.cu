@@ -6,11 +6,15 @@
 namespace st {
 
 static int launch_line(st_ctx *c, OpKind op, const LineArgs &a) {
-    return a.cyc ? launch_line_cyc(c, op, a) : launch_line_t<false>(c, op, a);
+    return a.cyc ? launch_line_cyc(c, op, a) : launch_line_t<false, double>(c, op, a);
+}
+static int launch_line(st_ctx *c, OpKind op, const LineArgsF &a) {
+    return a.cyc ? launch_line_cyc_f32(c, op, a) : launch_line_f32(c, op, a);
 }
 
-static LineArgs make_args(st_ctx *c, int dir) {
-    LineArgs a{};
+template <class T = double>
+static LineArgsT<T> make_args(st_ctx *c, int dir) {
+    LineArgsT<T> a{};
     a.geo.dir = dir;
     a.geo.n = c->dm.n[dir];
     a.geo.My = c->dm.n[1];
@@ -61,6 +65,42 @@ int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg) {
     LineArgs a = make_args(c, dir);
     a.F = plain(F); a.O1 = Fg;
+    return launch_line(c, OP_GAUSS, a);
+}
+
+// ---- FP32-field variants (the FP32 mode's derivative and Gaussian passes) ----
+static ProdF plain_f(const float *F) {
+    ProdF p{};
+    p.op = PR_A;
+    p.a = F;
+    return p;
+}
+
+int dev_dfd_prod_f(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd) {
+    LineArgsF a = make_args<float>(c, dir);
+    a.F = F; a.O1 = dF; a.asym = asym; a.iadd = iadd;
+    a.fac1 = cadd * c->s1[dir] * (double)(a.geo.n - 1);
+    a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
+    return launch_line(c, OP_D1, a);
+}
+
+int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd, double cadd) {
+    return dev_dfd_prod_f(c, dir, asym, plain_f(F), dF, iadd, cadd);
+}
+
+int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd) {
+    LineArgsF a = make_args<float>(c, dir);
+    a.F = plain_f(F); a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;
+    a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
+    a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];
+    a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
+    a.t2 = c->tri[dir][asym ? K_D2A : K_D2S];
+    return launch_line(c, OP_D2, a);
+}
+
+int dev_gauss_f(st_ctx *c, int dir, const float *F, float *Fg) {
+    LineArgsF a = make_args<float>(c, dir);
+    a.F = plain_f(F); a.O1 = Fg;
     return launch_line(c, OP_GAUSS, a);
 }
 

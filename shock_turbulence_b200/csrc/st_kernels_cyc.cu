@@ -4,6 +4,6 @@
 
 namespace st {
 
-int launch_line_cyc(st_ctx *c, OpKind op, const LineArgs &a) { return launch_line_t<true>(c, op, a); }
+int launch_line_cyc(st_ctx *c, OpKind op, const LineArgs &a) { return launch_line_t<true, double>(c, op, a); }
 
 }  // namespace st

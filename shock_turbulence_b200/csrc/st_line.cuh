@@ -39,23 +39,28 @@ struct LineGeo {
     }
 };
 
-template <int OP>
-__device__ __forceinline__ double prod_eval(const Prod &P, size_t i) {
+// The producer's fields are double or float (FP32 mode); values are
+// converted to double as they are loaded and every operation is in double.
+template <class T>
+__device__ __forceinline__ double ld(const T *p) { return (double)__ldg(p); }
+
+template <int OP, class T>
+__device__ __forceinline__ double prod_eval(const ProdT<T> &P, size_t i) {
     if constexpr (OP == PR_MUL) {
-        return __ldg(P.a + i) * __ldg(P.b + i);
+        return ld(P.a + i) * ld(P.b + i);
     } else if constexpr (OP == PR_ADDMUL) {
-        return (__ldg(P.a + i) + __ldg(P.b + i)) * __ldg(P.c + i);
+        return (ld(P.a + i) + ld(P.b + i)) * ld(P.c + i);
     } else if constexpr (OP == PR_MULMUL) {
-        return __ldg(P.c + i) * (__ldg(P.a + i) * __ldg(P.b + i));
+        return ld(P.c + i) * (ld(P.a + i) * ld(P.b + i));
     } else if constexpr (OP == PR_SPEC) {
-        double a = __ldg(P.a + i), b = __ldg(P.b + i), c = __ldg(P.c + i);
+        double a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i);
         return a * b * c + a * c * P.k0 * P.k1;
     } else if constexpr (OP == PR_SPECT) {
-        double a = __ldg(P.a + i), b = __ldg(P.b + i), c = __ldg(P.c + i), d = __ldg(P.d + i);
+        double a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i), d = ld(P.d + i);
         double fl = a * b * c + a * c * P.k0 * P.k1;
         return P.k2 * d * fl;
     } else {
-        return __ldg(P.a + i);
+        return ld(P.a + i);
     }
 }
 
@@ -67,8 +72,8 @@ __device__ __forceinline__ int halo_row(int row, int n, int cyc) {
 }
 
 // rows a-H .. a+S+H-1 of this lane's line into v
-template <int S, int H, int OP>
-__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const Prod &F, const ColMap &m, int lane,
+template <int S, int H, int OP, class T>
+__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const ProdT<T> &F, const ColMap &m, int lane,
                                           int a, int n, int cyc) {
     const size_t p = m.base + (size_t)lane * m.lstride;
 #pragma unroll
@@ -78,19 +83,19 @@ __device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const Prod &F,
     }
 }
 
-template <int S, int N>
-__device__ __forceinline__ void store_rows(const double (&r)[N], double *__restrict__ O, const ColMap &m,
+template <int S, int N, class T>
+__device__ __forceinline__ void store_rows(const double (&r)[N], T *__restrict__ O, const ColMap &m,
                                            int lane, int a, int add) {
-    double *p = O + m.base + (size_t)lane * m.lstride + (size_t)a * m.rstride;
+    T *p = O + m.base + (size_t)lane * m.lstride + (size_t)a * m.rstride;
     if (add) {
         double prev[S];
 #pragma unroll
-        for (int t = 0; t < S; t++) prev[t] = p[(size_t)t * m.rstride];
+        for (int t = 0; t < S; t++) prev[t] = (double)p[(size_t)t * m.rstride];
 #pragma unroll
-        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = prev[t] + r[t];
+        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = (T)(prev[t] + r[t]);
     } else {
 #pragma unroll
-        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = r[t];
+        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = (T)r[t];
     }
 }
 
@@ -214,10 +219,10 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
 // the reference formulas term by term (Fortran evaluates left to right).
 // Boundary rows belong to the first/last segment only: those warps re-read
 // the few rows they need from global memory (warp-uniform branch).
-template <int OP>
+template <int OP, class T = double>
 struct RowReader {
     const double *tile;       // shared tile row (y lines) or null
-    const Prod *F;            // global producer (x, z lines)
+    const ProdT<T> *F;        // global producer (x, z lines)
     size_t base, rstride;
     __device__ __forceinline__ double operator()(int row) const {
         return tile ? tile[row] : prod_eval<OP>(*F, base + (size_t)row * rstride);
@@ -229,16 +234,18 @@ struct RowReader {
 // are copied with 16-byte coalesced accesses into a [32][n+1] tile (odd
 // stride: lane l reading row r of line l hits bank (l*(n+1)+r) mod 32, all
 // distinct), so that each thread reads its segment conflict-free.
-template <int OP>
-__device__ __forceinline__ void ytile_load(double *tile, const Prod &F, size_t base, int n) {
+template <int OP, class T>
+__device__ __forceinline__ void ytile_load(double *tile, const ProdT<T> &F, size_t base, int n) {
     const int half = kLanes * n / 2;
-    if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
-        const double2 *src = reinterpret_cast<const double2 *>(F.a + base);
-        for (int q = threadIdx.x; q < half; q += blockDim.x) {
-            double2 d = __ldg(src + q);
-            int e = 2 * q, line = e / n, row = e - line * n;
-            tile[line * (n + 1) + row] = d.x;
-            tile[line * (n + 1) + row + 1] = d.y;
+    if (sizeof(T) == 8 && OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
+        if constexpr (sizeof(T) == 8) {
+            const double2 *src = reinterpret_cast<const double2 *>(F.a + base);
+            for (int q = threadIdx.x; q < half; q += blockDim.x) {
+                double2 d = __ldg(src + q);
+                int e = 2 * q, line = e / n, row = e - line * n;
+                tile[line * (n + 1) + row] = d.x;
+                tile[line * (n + 1) + row + 1] = d.y;
+            }
         }
     } else {
         for (int q = threadIdx.x; q < 2 * half; q += blockDim.x) {
@@ -247,27 +254,30 @@ __device__ __forceinline__ void ytile_load(double *tile, const Prod &F, size_t b
         }
     }
 }
-__device__ __forceinline__ void ytile_store(const double *tile, double *__restrict__ O, size_t base, int n,
+template <class T>
+__device__ __forceinline__ void ytile_store(const double *tile, T *__restrict__ O, size_t base, int n,
                                             int add) {
-    if (reinterpret_cast<uintptr_t>(O + base) & 15) {
+    if (sizeof(T) != 8 || (reinterpret_cast<uintptr_t>(O + base) & 15)) {
         for (int q = threadIdx.x; q < kLanes * n; q += blockDim.x) {
             int line = q / n, row = q - line * n;
             double v = tile[line * (n + 1) + row];
-            O[base + q] = add ? O[base + q] + v : v;
+            O[base + q] = (T)(add ? (double)O[base + q] + v : v);
         }
         return;
     }
-    double2 *dst = reinterpret_cast<double2 *>(O + base);
-    const int half = kLanes * n / 2;
-    for (int q = threadIdx.x; q < half; q += blockDim.x) {
-        int e = 2 * q, line = e / n, row = e - line * n;
-        double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
-        if (add) {
-            double2 o = dst[q];
-            d.x = o.x + d.x;
-            d.y = o.y + d.y;
+    if constexpr (sizeof(T) == 8) {
+        double2 *dst = reinterpret_cast<double2 *>(O + base);
+        const int half = kLanes * n / 2;
+        for (int q = threadIdx.x; q < half; q += blockDim.x) {
+            int e = 2 * q, line = e / n, row = e - line * n;
+            double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
+            if (add) {
+                double2 o = dst[q];
+                d.x = o.x + d.x;
+                d.y = o.y + d.y;
+            }
+            dst[q] = d;
         }
-        dst[q] = d;
     }
 }
 template <int S, int H>

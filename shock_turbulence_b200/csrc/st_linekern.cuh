@@ -11,9 +11,12 @@
 
 namespace st {
 
-struct LineArgs {
-    Prod F;
-    double *O1, *O2;
+// T: element type of the fields read and written (double, or float in the
+// FP32 mode); the stencils and solves always run in double.
+template <class T>
+struct LineArgsT {
+    ProdT<T> F;
+    T *O1, *O2;
     LineGeo geo;
     int S, P;
     double fac1, fac2;
@@ -23,6 +26,8 @@ struct LineArgs {
     PenTab p;
     Consts K;
 };
+using LineArgs = LineArgsT<double>;
+using LineArgsF = LineArgsT<float>;
 
 // Every line kernel is instantiated for x/z lines (YT = false: direct
 // coalesced row accesses) and for y lines (YT = true: staged through a
@@ -32,17 +37,17 @@ struct LineArgs {
     extern __shared__ double tile[];                                                   \
     const int lane = threadIdx.x & (kLanes - 1), s = threadIdx.x / kLanes, n = a.geo.n, row0 = s * S; \
     const ColMap m = a.geo.map(blockIdx.x);                                            \
-    const RowReader<OP> rd = YT ? RowReader<OP>{tile + lane * (n + 1), nullptr, 0, 0}  \
-                                : RowReader<OP>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
+    const RowReader<OP, T> rd = YT ? RowReader<OP, T>{tile + lane * (n + 1), nullptr, 0, 0}  \
+                                   : RowReader<OP, T>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
 
-template <int S, int H, bool YT, int OP>
-__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const Prod &F,
+template <int S, int H, bool YT, int OP, class T>
+__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const ProdT<T> &F,
                                          const ColMap &m, int lane, int a, int n, int cyc) {
     if (YT) ytile_rows<S, H>(v, tile, lane, a, n, cyc);
     else load_rows<S, H, OP>(v, F, m, lane, a, n, cyc);
 }
-template <int S, bool YT, int N>
-__device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, double *O, const ColMap &m,
+template <int S, bool YT, int N, class T>
+__device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, T *O, const ColMap &m,
                                          int lane, int a, int n, int add) {
     if (YT) {
         __syncthreads();                 // every thread has finished reading the tile
@@ -55,8 +60,8 @@ __device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, dou
 }
 
 // DF*_sym/_asym and the periodic DF*: O1 (=|+=) cadd * dF/ds
-template <int S, bool YT, int OP, bool CYC>
-__global__ void __launch_bounds__(512, 2) k_dfd(LineArgs a) {
+template <int S, bool YT, int OP, bool CYC, class T>
+__global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
     double v[S + 4];
@@ -70,8 +75,8 @@ __global__ void __launch_bounds__(512, 2) k_dfd(LineArgs a) {
 // D2F*2_sym/_asym and the periodic D2F*2: O2 = d2F/ds2; if iadd, O1 = dF/ds
 // (cadd = 1).  The first
 // derivative re-reads the rows (the CTA's lines are still in L2).
-template <int S, bool YT, bool CYC>
-__global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgs a) {
+template <int S, bool YT, bool CYC, class T>
+__global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
@@ -99,8 +104,8 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgs a) {
 // F.  O1 may alias F: every read of
 // F (including the boundary re-reads) happens before the solve's first
 // barrier and every write after its last one.
-template <int S, bool YT, bool CYC>
-__global__ void __launch_bounds__(512, 2) k_filter(LineArgs a) {
+template <int S, bool YT, bool CYC, class T>
+__global__ void __launch_bounds__(512, 2) k_filter(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
@@ -114,8 +119,8 @@ __global__ void __launch_bounds__(512, 2) k_filter(LineArgs a) {
 
 // Gaussian_Filter_X/Y/Z (both families): O1 = explicit 9-point Gaussian of F
 // (O1 != F)
-template <int S, bool YT, bool CYC>
-__global__ void __launch_bounds__(512, 2) k_gauss(LineArgs a) {
+template <int S, bool YT, bool CYC, class T>
+__global__ void __launch_bounds__(512, 2) k_gauss(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;
@@ -139,8 +144,8 @@ static void set_smem(size_t bytes) {
     }
 }
 
-template <int S, bool YT, bool CYC>
-static void launch_SY(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
+template <int S, bool YT, bool CYC, class T>
+static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t st) {
     const size_t nlines = c->dm.n3 / (size_t)a.geo.n;
     dim3 grid((unsigned)(nlines / kLanes)), block(kLanes * a.P);
     const size_t smem = YT ? (size_t)kLanes * (a.geo.n + 1) * sizeof(double) : 0;
@@ -148,37 +153,42 @@ static void launch_SY(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) 
     const double n3 = (double)c->dm.n3;
     // inputs: 1 field, or every field a producer expression reads
     static const int nin[6] = {1, 2, 3, 3, 3, 4};
-    double b = 8.0 * nin[a.F.op] + 8.0;          // + one output
-    if (op == OP_D1 && a.iadd) b += 8.0;           // read-modify-write
-    if (op == OP_D2 && a.iadd) b += 8.0;           // second output
+    const double es = (double)sizeof(T);
+    double b = es * nin[a.F.op] + es;              // + one output
+    if (op == OP_D1 && a.iadd) b += es;            // read-modify-write
+    if (op == OP_D2 && a.iadd) b += es;            // second output
     static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
     int pi = prof_start(c, names[op], b * n3);
     switch (op) {
         case OP_D1:
             switch (a.F.op) {
-#define PCASE(o_) case o_: set_smem<k_dfd<S, YT, o_, CYC>>(smem); k_dfd<S, YT, o_, CYC><<<grid, block, smem, st>>>(a); break;
+#define PCASE(o_) case o_: set_smem<k_dfd<S, YT, o_, CYC, T>>(smem); k_dfd<S, YT, o_, CYC, T><<<grid, block, smem, st>>>(a); break;
                 PCASE(PR_A) PCASE(PR_MUL) PCASE(PR_ADDMUL) PCASE(PR_MULMUL) PCASE(PR_SPEC) PCASE(PR_SPECT)
 #undef PCASE
             }
             break;
-        case OP_D2: set_smem<k_d2fd2<S, YT, CYC>>(smem); k_d2fd2<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
-        case OP_FILTER: set_smem<k_filter<S, YT, CYC>>(smem); k_filter<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
-        case OP_GAUSS: set_smem<k_gauss<S, YT, CYC>>(smem); k_gauss<S, YT, CYC><<<grid, block, smem, st>>>(a); break;
+        case OP_D2: set_smem<k_d2fd2<S, YT, CYC, T>>(smem); k_d2fd2<S, YT, CYC, T><<<grid, block, smem, st>>>(a); break;
+        case OP_FILTER:
+            if constexpr (sizeof(T) == 8) {   // the compact filter acts on the FP64 state only
+                set_smem<k_filter<S, YT, CYC, T>>(smem); k_filter<S, YT, CYC, T><<<grid, block, smem, st>>>(a);
+            }
+            break;
+        case OP_GAUSS: set_smem<k_gauss<S, YT, CYC, T>>(smem); k_gauss<S, YT, CYC, T><<<grid, block, smem, st>>>(a); break;
     }
     prof_stop(c, pi);
 }
 
-template <int S, bool CYC>
-static void launch_S(st_ctx *c, OpKind op, const LineArgs &a, cudaStream_t st) {
-    if (a.geo.dir == 1) launch_SY<S, true, CYC>(c, op, a, st);
-    else launch_SY<S, false, CYC>(c, op, a, st);
+template <int S, bool CYC, class T>
+static void launch_S(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t st) {
+    if (a.geo.dir == 1) launch_SY<S, true, CYC, T>(c, op, a, st);
+    else launch_SY<S, false, CYC, T>(c, op, a, st);
 }
 
 // all line-operator launches of one family (CYC: periodic lines)
-template <bool CYC>
-static int launch_line_t(st_ctx *c, OpKind op, const LineArgs &a) {
+template <bool CYC, class T>
+static int launch_line_t(st_ctx *c, OpKind op, const LineArgsT<T> &a) {
     switch (a.S) {
-#define CASE(s_) case s_: launch_S<s_, CYC>(c, op, a, c->stream); break;
+#define CASE(s_) case s_: launch_S<s_, CYC, T>(c, op, a, c->stream); break;
         CASE(2) CASE(3) CASE(4) CASE(6) CASE(8) CASE(12) CASE(16)
 #undef CASE
         default: return fail(c, ST_E_UNSUPPORTED, "unsupported line segmentation");
@@ -188,7 +198,11 @@ static int launch_line_t(st_ctx *c, OpKind op, const LineArgs &a) {
 }
 
 
-// periodic-line launches, instantiated in st_kernels_cyc.cu
+// launches of the other instantiations, each in its own translation unit:
+// periodic lines (st_kernels_cyc.cu), FP32 fields (st_kernels_f32.cu) and
+// both (st_kernels_cyc_f32.cu)
 int launch_line_cyc(st_ctx *c, OpKind op, const LineArgs &a);
+int launch_line_f32(st_ctx *c, OpKind op, const LineArgsF &a);
+int launch_line_cyc_f32(st_ctx *c, OpKind op, const LineArgsF &a);
 
 }  // namespace st

@@ -29,13 +29,57 @@ static int pfor(st_ctx *c, size_t n, Fn fn) {
 #define PFOR(c, n, ...) ST_TRY(pfor((c), (n), [=] __device__(size_t p) __VA_ARGS__))
 
 // producer expressions evaluated by the derivative kernels while loading
-static Prod pr_mul(const double *a, const double *b) { Prod p{}; p.op = PR_MUL; p.a = a; p.b = b; return p; }
-static Prod pr_addmul(const double *a, const double *b, const double *c) {
-    Prod p{}; p.op = PR_ADDMUL; p.a = a; p.b = b; p.c = c; return p;
+template <class R>
+static ProdT<R> pr_mul(const R *a, const R *b) { ProdT<R> p{}; p.op = PR_MUL; p.a = a; p.b = b; return p; }
+template <class R>
+static ProdT<R> pr_addmul(const R *a, const R *b, const R *c) {
+    ProdT<R> p{}; p.op = PR_ADDMUL; p.a = a; p.b = b; p.c = c; return p;
 }
-static Prod pr_mulmul(const double *a, const double *b, const double *c) {
-    Prod p{}; p.op = PR_MULMUL; p.a = a; p.b = b; p.c = c; return p;
+template <class R>
+static ProdT<R> pr_mulmul(const R *a, const R *b, const R *c) {
+    ProdT<R> p{}; p.op = PR_MULMUL; p.a = a; p.b = b; p.c = c; return p;
 }
+
+// Line operators by field type: double arrays, or float arrays in the FP32
+// mode (the kernels compute in double either way; only storage differs).
+static int dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
+    return dev_dfd(c, dir, asym, F, dF, iadd, cadd);
+}
+static int dfd(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd, double cadd) {
+    return dev_dfd_f(c, dir, asym, F, dF, iadd, cadd);
+}
+static int dfd(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int iadd, double cadd) {
+    return dev_dfd_prod(c, dir, asym, F, dF, iadd, cadd);
+}
+static int dfd(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd) {
+    return dev_dfd_prod_f(c, dir, asym, F, dF, iadd, cadd);
+}
+static int d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
+    return dev_d2fd2(c, dir, asym, F, dF, d2F, iadd);
+}
+static int d2fd2(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd) {
+    return dev_d2fd2_f(c, dir, asym, F, dF, d2F, iadd);
+}
+static int gauss(st_ctx *c, int dir, const double *F, double *Fg) { return dev_gauss(c, dir, F, Fg); }
+static int gauss(st_ctx *c, int dir, const float *F, float *Fg) { return dev_gauss_f(c, dir, F, Fg); }
+
+// COMMON arrays of the intermediate type R
+template <class R> struct Store;
+template <> struct Store<double> {
+    static double **grad(st_ctx *c) { return c->grad; }
+    static double **hyp(st_ctx *c) { return c->hyp; }
+    static double **dYd(st_ctx *c) { return c->dYd; }
+    static double *dQ(st_ctx *c) { return c->dQ; }
+    static double *drYi(st_ctx *c) { return c->drYi; }
+};
+template <> struct Store<float> {
+    static float **grad(st_ctx *c) { return c->gradf; }
+    static float **hyp(st_ctx *c) { return c->hypf; }
+    static float **dYd(st_ctx *c) { return c->dYdf; }
+    static float *dQ(st_ctx *c) { return c->dQf; }
+    static float *drYi(st_ctx *c) { return c->drYif; }
+};
+template <class R> constexpr bool is_fp64() { return sizeof(R) == sizeof(double); }
 
 struct Phys {
     double g1, g2, eps, vis_exp, Re1_inv, Re2_inv, Pr_inv, Sc_inv, bulk;
@@ -69,16 +113,25 @@ __device__ __forceinline__ void viscosity(const Phys &f, double T, double Y, dou
     dmu = pow(fac1 * T, fac2) * num / den * f.vis_exp * fac1;
 }
 
-// contiguous multi-field scratch (n fields)
-struct ScratchN {
-    st_ctx *c; std::vector<double *> f;
-    ScratchN(st_ctx *cc, int n) : c(cc) { for (int i = 0; i < n; i++) f.push_back(scratch(cc)); }
-    ~ScratchN() { for (double *p : f) release(c, p); }
-    double *operator[](int i) const { return f[i]; }
+// n separate scratch fields
+template <class R>
+struct ScratchNT {
+    st_ctx *c; std::vector<R *> f;
+    ScratchNT(st_ctx *cc, int n) : c(cc) { for (int i = 0; i < n; i++) f.push_back(scratch_t<R>(cc, 1)); }
+    ~ScratchNT() { for (R *p : f) release(c, p); }
+    R *operator[](int i) const { return f[i]; }
 };
 
 int dev_fill(st_ctx *c, double *x, size_t n, double v) {
     PFOR(c, n, { x[p] = v; });
+    return ST_OK;
+}
+int dev_to_float(st_ctx *c, const double *x, float *y, size_t n) {
+    PFOR(c, n, { y[p] = (float)x[p]; });
+    return ST_OK;
+}
+int dev_to_double(st_ctx *c, const float *x, double *y, size_t n) {
+    PFOR(c, n, { y[p] = (double)x[p]; });
     return ST_OK;
 }
 
@@ -108,36 +161,45 @@ int dev_compute_gamma(st_ctx *c, const double *Y) {
 //  - when the molecular viscous term is not added (Re <= 0, the reference
 //    build, src/rhsv_sym_mf.f:1420-1424) the Qvisc work, whose only consumer
 //    is that sum, is skipped; the /GRAD/ first derivatives are still formed.
-int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
+//
+// R is the storage type of every field except the state: double, or float in
+// the FP32 mode.  Qr is the state in that type (Q itself in FP64); the
+// derivative operands come from Qr, the pointwise thermodynamics from Q.
+template <class R>
+static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     const size_t n3 = c->dm.n3;
     const Phys f = phys(c);
     // src/rhsv_periodic_sf.f:1381 adds Qvisc unconditionally
     const bool visc = c->p.re > 0.0 || c->p.family == ST_FAMILY_PERIODIC;
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    double *Gxx = c->grad[G_DUX_DX], *Gyx = c->grad[G_DUY_DX], *Gzx = c->grad[G_DUZ_DX];
-    double *Gxy = c->grad[G_DUX_DY], *Gyy = c->grad[G_DUY_DY], *Gzy = c->grad[G_DUZ_DY];
-    double *Gxz = c->grad[G_DUX_DZ], *Gyz = c->grad[G_DUY_DZ], *Gzz = c->grad[G_DUZ_DZ];
-    double *GTx = c->grad[G_DTDX], *GTy = c->grad[G_DTDY], *GTz = c->grad[G_DTDZ];
-    Scratch sQcx(c, 5), sQcy(c, 5), sQcz(c, 5), sQv(c, 5);
-    double *Qcx = sQcx, *Qcy = sQcy, *Qcz = sQcz, *Qv = sQv;
-    ScratchN s(c, 17);
-    double *Vs = s[0], *P = s[1], *T = s[2], *u = s[3], *v = s[4], *w = s[5], *mu = s[6], *dmu = s[7];
-    double *Flux = s[8], *FF = s[9], *dF = s[10], *dFz = s[11], *U4 = s[12], *U5 = s[13], *Tdy = s[14];
-    double *Tdz = s[15], *T2 = s[16];
+    const R *q1r = Qr, *q2r = Qr + n3, *q3r = Qr + 2 * n3, *q4r = Qr + 3 * n3, *q5r = Qr + 4 * n3;
+    R **G = Store<R>::grad(c);
+    R *Gxx = G[G_DUX_DX], *Gyx = G[G_DUY_DX], *Gzx = G[G_DUZ_DX];
+    R *Gxy = G[G_DUX_DY], *Gyy = G[G_DUY_DY], *Gzy = G[G_DUZ_DY];
+    R *Gxz = G[G_DUX_DZ], *Gyz = G[G_DUY_DZ], *Gzz = G[G_DUZ_DZ];
+    R *GTx = G[G_DTDX], *GTy = G[G_DTDY], *GTz = G[G_DTDZ];
+    ScratchT<R> sQcx(c, 5), sQcy(c, 5), sQcz(c, 5), sQv(c, 5);
+    R *Qcx = sQcx, *Qcy = sQcy, *Qcz = sQcz, *Qv = sQv;
+    ScratchNT<R> s(c, 17);
+    R *Vs = s[0], *P = s[1], *T = s[2], *u = s[3], *v = s[4], *w = s[5], *mu = s[6], *dmu = s[7];
+    R *Flux = s[8], *FF = s[9], *dF = s[10], *dFz = s[11], *U4 = s[12], *U5 = s[13], *Tdy = s[14];
+    R *Tdz = s[15], *T2 = s[16];
     const double *g = c->gamma_eff;
 
     // ---- RHS_x (src/rhsv_sym_mf.f:37-481)
     PFOR(c, n3, {
-        thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs[p], P[p], T[p]);
-        u[p] = Q1[p] * Vs[p];
+        double vs, pp, tt;
+        thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], vs, pp, tt);
+        Vs[p] = vs; P[p] = pp; T[p] = tt;
+        u[p] = Q1[p] * vs;
     });
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q4, u), Qcx + 3 * n3, 0, -1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_addmul(Q5, P, u), Qcx + 4 * n3, 0, -1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 0, pr_mul(Q1, u), Qcx, 0, -5.0e-1));
-    ST_TRY(dev_dfd(c, 0, 0, P, Qcx, 1, -1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q2, u), Qcx + n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q3, u), Qcx + 2 * n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd(c, 0, 1, Q1, FF, 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(q4r, u), Qcx + 3 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 0, 1, pr_addmul(q5r, P, u), Qcx + 4 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 0, 0, pr_mul(q1r, u), Qcx, 0, -5.0e-1));
+    ST_TRY(dfd(c, 0, 0, P, Qcx, 1, -1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(q2r, u), Qcx + n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 0, 1, pr_mul(q3r, u), Qcx + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 0, 1, q1r, FF, 0, 1.0));
     PFOR(c, n3, {
         double m, dm;
         v[p] = Q2[p] * Vs[p];
@@ -152,31 +214,31 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     });
     if (visc) {
         const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
-        ST_TRY(dev_d2fd2(c, 0, 0, T, GTx, dF, 1));
+        ST_TRY(d2fd2(c, 0, 0, T, GTx, dF, 1));
         PFOR(c, n3, { Qv[4 * n3 + p] = Pri * (mu[p] * dF[p] + dmu[p] * GTx[p] * GTx[p]); });
-        ST_TRY(dev_d2fd2(c, 0, 1, u, Gxx, dF, 1));
+        ST_TRY(d2fd2(c, 0, 1, u, Gxx, dF, 1));
         PFOR(c, n3, {
             double fac2 = fac1 * mu[p] * dF[p];
             Qv[p] = fac2;
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac2;
         });
-        ST_TRY(dev_d2fd2(c, 0, 0, v, Gyx, dF, 1));
+        ST_TRY(d2fd2(c, 0, 0, v, Gyx, dF, 1));
         PFOR(c, n3, {
             double fac2 = mu[p] * dF[p];
             Qv[n3 + p] = fac2;
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + v[p] * fac2;
         });
-        ST_TRY(dev_d2fd2(c, 0, 0, w, Gzx, dF, 1));
+        ST_TRY(d2fd2(c, 0, 0, w, Gzx, dF, 1));
         PFOR(c, n3, {
             double fac2 = mu[p] * dF[p];
             Qv[2 * n3 + p] = fac2;
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + w[p] * fac2;
         });
     } else {
-        ST_TRY(dev_dfd(c, 0, 0, T, GTx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 1, u, Gxx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 0, v, Gyx, 0, 1.0));
-        ST_TRY(dev_dfd(c, 0, 0, w, Gzx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, T, GTx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 1, u, Gxx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, v, Gyx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, w, Gzx, 0, 1.0));
     }
     PFOR(c, n3, {
         double fac2 = -5.0e-1 * Q4[p] * u[p];
@@ -187,20 +249,20 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
 
     // ---- RHS_yz (src/rhsv_sym_mf.f:492-1428)
     // d(rho v)/dy and d(rho w)/dz with iadd=0, cadd=-1: Qconv(4) = 0 - d(.) exactly
-    ST_TRY(dev_dfd(c, 1, 1, Q2, Qcy + 3 * n3, 0, -1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q1, v), Qcy, 0, -5.0e-1));
-    ST_TRY(dev_dfd_prod(c, 1, 0, pr_mul(Q2, v), Qcy + n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd(c, 1, 0, P, Qcy + n3, 1, -1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q3, v), Qcy + 2 * n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_addmul(Q5, P, v), Qcy + 4 * n3, 0, -1.0));
-    ST_TRY(dev_dfd(c, 2, 1, Q3, Qcz + 3 * n3, 0, -1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q1, w), Qcz, 0, -5.0e-1));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q2, w), Qcz + n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd_prod(c, 2, 0, pr_mul(Q3, w), Qcz + 2 * n3, 0, -5.0e-1));
-    ST_TRY(dev_dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_addmul(Q5, P, w), Qcz + 4 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 1, 1, q2r, Qcy + 3 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(q1r, v), Qcy, 0, -5.0e-1));
+    ST_TRY(dfd(c, 1, 0, pr_mul(q2r, v), Qcy + n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 1, 0, P, Qcy + n3, 1, -1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(q3r, v), Qcy + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 1, 1, pr_addmul(q5r, P, v), Qcy + 4 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 2, 1, q3r, Qcz + 3 * n3, 0, -1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mul(q1r, w), Qcz, 0, -5.0e-1));
+    ST_TRY(dfd(c, 2, 1, pr_mul(q2r, w), Qcz + n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 2, 0, pr_mul(q3r, w), Qcz + 2 * n3, 0, -5.0e-1));
+    ST_TRY(dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
+    ST_TRY(dfd(c, 2, 1, pr_addmul(q5r, P, w), Qcz + 4 * n3, 0, -1.0));
     // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
-    const double *dFy = Qcy + 3 * n3, *dFzz = Qcz + 3 * n3;
+    const R *dFy = Qcy + 3 * n3, *dFzz = Qcz + 3 * n3;
     PFOR(c, n3, {
         double fac2 = -5.0e-1 * (-dFy[p]);
         Qcy[p] = Qcy[p] + fac2 * u[p];
@@ -213,8 +275,8 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     });
     if (visc) {
         const double Pri = f.Pr_inv;
-        ST_TRY(dev_d2fd2(c, 1, 0, T, GTy, U5, 1));
-        ST_TRY(dev_d2fd2(c, 2, 0, T, GTz, Flux, 1));
+        ST_TRY(d2fd2(c, 1, 0, T, GTy, U5, 1));
+        ST_TRY(d2fd2(c, 2, 0, T, GTz, Flux, 1));
         PFOR(c, n3, {
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + Pri * (mu[p] * (U5[p] + Flux[p]) +
                                                     dmu[p] * (GTy[p] * GTy[p] + GTz[p] * GTz[p]));
@@ -222,19 +284,19 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
             Tdy[p] = dmu[p] * GTy[p];
             Tdz[p] = dmu[p] * GTz[p];
         });
-        ST_TRY(dev_d2fd2(c, 1, 0, u, Gxy, U5, 1));
-        ST_TRY(dev_d2fd2(c, 1, 1, v, Gyy, dF, 1));
-        ST_TRY(dev_d2fd2(c, 1, 0, w, Gzy, T2, 1));
+        ST_TRY(d2fd2(c, 1, 0, u, Gxy, U5, 1));
+        ST_TRY(d2fd2(c, 1, 1, v, Gyy, dF, 1));
+        ST_TRY(d2fd2(c, 1, 0, w, Gzy, T2, 1));
     } else {
-        ST_TRY(dev_dfd(c, 1, 0, T, GTy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 0, T, GTz, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 0, u, Gxy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, v, Gyy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 0, w, Gzy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, T, GTy, 0, 1.0));
+        ST_TRY(dfd(c, 2, 0, T, GTz, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, u, Gxy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, v, Gyy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, w, Gzy, 0, 1.0));
     }
-    ST_TRY(dev_dfd(c, 2, 0, u, Gxz, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, v, Gyz, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 1, w, Gzz, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, u, Gxz, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, v, Gyz, 0, 1.0));
+    ST_TRY(dfd(c, 2, 1, w, Gzz, 0, 1.0));
     {
         const double fac1 = f.bulk + 4.0 / 3.0;
         PFOR(c, n3, {
@@ -259,8 +321,8 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     }
     if (visc) {
         const double fac1 = f.bulk - 2.0 / 3.0, fac2 = f.bulk + 4.0 / 3.0, fac3 = f.bulk + 1.0 / 3.0;
-        ST_TRY(dev_d2fd2(c, 2, 1, w, nullptr, T2, 0));
-        ST_TRY(dev_dfd(c, 1, 0, Gzz, U5, 0, 1.0));
+        ST_TRY(d2fd2(c, 2, 1, w, nullptr, T2, 0));
+        ST_TRY(dfd(c, 1, 0, Gzz, U5, 0, 1.0));
         PFOR(c, n3, {
             double tmp1 = Gxx[p];
             double dil = tmp1 + Gyy[p] + Gzz[p];
@@ -273,8 +335,8 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
                              mu[p] * (2.0 * (tmp1 * tmp1 + Gyy[p] * Gyy[p] + Gzz[p] * Gzz[p]) + fac1 * dil * dil);
         });
-        ST_TRY(dev_d2fd2(c, 2, 0, u, nullptr, dF, 0));
-        ST_TRY(dev_d2fd2(c, 2, 0, v, nullptr, U5, 0));
+        ST_TRY(d2fd2(c, 2, 0, u, nullptr, dF, 0));
+        ST_TRY(d2fd2(c, 2, 0, v, nullptr, U5, 0));
         PFOR(c, n3, {
             double tmp1 = Gyx[p] + Gxy[p];
             double tmp2 = Gzx[p] + Gxz[p];
@@ -288,14 +350,15 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
             Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
                              mu[p] * (tmp1 * tmp1 + tmp2 * tmp2 + tmp3 * tmp3);
         });
-        ST_TRY(dev_dfd(c, 1, 0, Gxx, U4, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 0, Gxx, U5, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, Gyx, Tdy, 0, 1.0));
-        ST_TRY(dev_dfd(c, 2, 1, Gzx, Tdz, 0, 1.0));
-        ST_TRY(dev_dfd(c, 1, 1, Gyz, T2, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, Gxx, U4, 0, 1.0));
+        ST_TRY(dfd(c, 2, 0, Gxx, U5, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, Gyx, Tdy, 0, 1.0));
+        ST_TRY(dfd(c, 2, 1, Gzx, Tdz, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, Gyz, T2, 0, 1.0));
     }
     {
         const double fac3 = f.bulk + 1.0 / 3.0;
+        const bool fp64 = is_fp64<R>();
         PFOR(c, n3, {
             if (visc) {
                 double fac_X = fac3 * mu[p] * (Tdy[p] + Tdz[p]);
@@ -306,10 +369,14 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
                 Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
                 Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z;
             }
-            // velocities back to momenta, (m/rho)*rho as the reference does
-            Q1[p] = u[p] * Q4[p];
-            Q2[p] = v[p] * Q4[p];
-            Q3[p] = w[p] * Q4[p];
+            // velocities back to momenta, (m/rho)*rho as the reference does;
+            // the FP32 mode keeps the double momenta instead of rounding them
+            // through the float velocities
+            if (fp64) {
+                Q1[p] = u[p] * Q4[p];
+                Q2[p] = v[p] * Q4[p];
+                Q3[p] = w[p] * Q4[p];
+            }
             for (int l = 0; l < 5; l++) {
                 size_t q = l * n3 + p;
                 double r = Qcx[q] + Qcy[q] + Qcz[q];
@@ -321,25 +388,40 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     return ST_OK;
 }
 
+// Gaussian_Filter src/filters_sym.f:1046-1071
+template <class R>
+static int gaussian_filter_t(st_ctx *c, const R *F, R *Fg, int nvar) {
+    const size_t n3 = c->dm.n3;
+    ScratchT<R> tmp(c);
+    R *t = tmp;
+    for (int l = 0; l < nvar; l++) {
+        ST_TRY(gauss(c, 0, F + l * n3, Fg + l * n3));
+        ST_TRY(gauss(c, 1, Fg + l * n3, t));
+        ST_TRY(gauss(c, 2, t, Fg + l * n3));
+    }
+    return ST_OK;
+}
+
 // ---- artificial viscosity -----------------------------------------------------
 // Compute_Laplacian src/hyper_dynamic_sym_mf.f:41-65
-static int laplacian(st_ctx *c, const double *S, double *d2S) {
-    Scratch dS(c), t1(c), t2(c);
-    double *pt1 = t1, *pt2 = t2;
+template <class R>
+static int laplacian(st_ctx *c, const R *S, R *d2S) {
+    ScratchT<R> dS(c), t1(c), t2(c);
+    R *pt1 = t1, *pt2 = t2;
     if (c->p.family == ST_FAMILY_PERIODIC) {
         // Compute_Laplacian src/hyper_dynamic.f:41-58 (second derivatives)
-        ST_TRY(dev_d2fd2(c, 0, 0, S, nullptr, t1, 0));
-        ST_TRY(dev_d2fd2(c, 1, 0, S, nullptr, t2, 0));
-        ST_TRY(dev_d2fd2(c, 2, 0, S, nullptr, d2S, 0));
+        ST_TRY(d2fd2(c, 0, 0, S, (R *)nullptr, (R *)t1, 0));
+        ST_TRY(d2fd2(c, 1, 0, S, (R *)nullptr, (R *)t2, 0));
+        ST_TRY(d2fd2(c, 2, 0, S, (R *)nullptr, d2S, 0));
         PFOR(c, c->dm.n3, { d2S[p] = d2S[p] + pt1[p] + pt2[p]; });
         return ST_OK;
     }
-    ST_TRY(dev_dfd(c, 0, 0, S, dS, 0, 1.0));
-    ST_TRY(dev_dfd(c, 0, 1, dS, t1, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, S, dS, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 1, dS, t2, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, S, dS, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 1, dS, d2S, 0, 1.0));
+    ST_TRY(dfd(c, 0, 0, S, (R *)dS, 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, (const R *)dS, (R *)t1, 0, 1.0));
+    ST_TRY(dfd(c, 1, 0, S, (R *)dS, 0, 1.0));
+    ST_TRY(dfd(c, 1, 1, (const R *)dS, (R *)t2, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, S, (R *)dS, 0, 1.0));
+    ST_TRY(dfd(c, 2, 1, (const R *)dS, d2S, 0, 1.0));
     PFOR(c, c->dm.n3, { d2S[p] = d2S[p] + pt1[p] + pt2[p]; });
     return ST_OK;
 }
@@ -353,30 +435,32 @@ static int laplacian(st_ctx *c, const double *S, double *d2S) {
 // eta = (rho|d4S|, fac3|d4e|, rho|d4S|) and applies the coefficients after the
 // filter.  The third field equals the first, so its filtered value is the
 // first one's (same input, same arithmetic) and is filtered once.
+template <class R>
 static int compute_hyper_sf(st_ctx *c, const double *Q) {
     const size_t n3 = c->dm.n3;
     const double gam = c->p.gamma1;
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    ScratchN s(c, 14);
-    double *U1 = s[0], *U2 = s[1], *U3 = s[2], *W1 = s[3], *W2 = s[4], *W3 = s[5], *Dl = s[6];
-    double *Cbeta = s[7], *S = s[8], *e = s[9], *T = s[10], *d2 = s[11], *d4S = s[12], *d4e = s[13];
+    ScratchNT<R> s(c, 14);
+    R *U1 = s[0], *U2 = s[1], *U3 = s[2], *W1 = s[3], *W2 = s[4], *W3 = s[5], *Dl = s[6];
+    R *Cbeta = s[7], *S = s[8], *e = s[9], *T = s[10], *d2 = s[11], *d4S = s[12], *d4e = s[13];
     PFOR(c, n3, {
         double t = 1.0 / Q4[p];
         U1[p] = Q1[p] * t; U2[p] = Q2[p] * t; U3[p] = Q3[p] * t;
     });
-    ST_TRY(dev_dfd(c, 1, 0, U3, W1, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, U2, W1, 1, -1.0));
-    ST_TRY(dev_dfd(c, 0, 0, U3, W2, 0, -1.0));
-    ST_TRY(dev_dfd(c, 2, 0, U1, W2, 1, 1.0));
-    ST_TRY(dev_dfd(c, 0, 0, U2, W3, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, U1, W3, 1, -1.0));
-    ST_TRY(dev_dfd(c, 0, 0, U1, Dl, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, U2, Dl, 1, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, U3, Dl, 1, 1.0));
-    const double *G0 = c->grad[0], *G1 = c->grad[1], *G2 = c->grad[2], *G3 = c->grad[3], *G4 = c->grad[4],
-                 *G5 = c->grad[5], *G6 = c->grad[6], *G7 = c->grad[7], *G8 = c->grad[8];
+    ST_TRY(dfd(c, 1, 0, U3, W1, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, U2, W1, 1, -1.0));
+    ST_TRY(dfd(c, 0, 0, U3, W2, 0, -1.0));
+    ST_TRY(dfd(c, 2, 0, U1, W2, 1, 1.0));
+    ST_TRY(dfd(c, 0, 0, U2, W3, 0, 1.0));
+    ST_TRY(dfd(c, 1, 0, U1, W3, 1, -1.0));
+    ST_TRY(dfd(c, 0, 0, U1, Dl, 0, 1.0));
+    ST_TRY(dfd(c, 1, 0, U2, Dl, 1, 1.0));
+    ST_TRY(dfd(c, 2, 0, U3, Dl, 1, 1.0));
+    R *const *Gr = Store<R>::grad(c);
+    const R *G0 = Gr[0], *G1 = Gr[1], *G2 = Gr[2], *G3 = Gr[3], *G4 = Gr[4], *G5 = Gr[5], *G6 = Gr[6],
+            *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
-    double *P = U1, *Vs = U2;   // the velocities are dead from here on
+    R *P = U1, *Vs = U2;   // the velocities are dead from here on
     PFOR(c, n3, {
         double eps = 1.0e-7, fac2 = 10.0;
         double dil = Dl[p];
@@ -401,17 +485,18 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     ST_TRY(laplacian(c, d2, d4S));
     ST_TRY(laplacian(c, e, d2));
     ST_TRY(laplacian(c, d2, d4e));
-    Scratch etas(c, 4);
-    double *eta = etas, *etag = eta + 2 * n3;   // [rho|d4S|, fac3|d4e|] and their filtered values
+    ScratchT<R> etas(c, 4);
+    R *eta = etas, *etag = eta + 2 * n3;   // [rho|d4S|, fac3|d4e|] and their filtered values
     PFOR(c, n3, {
         double fac3 = (Q4[p] / T[p]) * sqrt(gam * P[p] * Vs[p]);
         eta[p] = Q4[p] * fabs(d4S[p]);
         eta[n3 + p] = fac3 * fabs(d4e[p]);
     });
-    ST_TRY(dev_gaussian_filter(c, eta, etag, 2));
+    ST_TRY(gaussian_filter_t<R>(c, eta, etag, 2));
     const double DX6 = pow(c->DX, 6.0), DX5 = pow(c->DX, 5.0);
     const double C_mu = 2.0e-3, C_k = 1.0e-2;
-    double *hb = c->hyp[H_BETA], *hv = c->hyp[H_VISC], *hk = c->hyp[H_K];
+    R **H = Store<R>::hyp(c);
+    R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K];
     PFOR(c, n3, {
         hb[p] = Cbeta[p] * etag[p] * DX6;
         hv[p] = C_mu * etag[p] * DX6;
@@ -420,19 +505,22 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     return ST_OK;
 }
 
-int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
-    if (c->p.family == ST_FAMILY_PERIODIC) return compute_hyper_sf(c, Q);
+// Yr: the mass fraction in the type R (Y itself in FP64)
+template <class R>
+static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R *Yr) {
+    if (c->p.family == ST_FAMILY_PERIODIC) return compute_hyper_sf<R>(c, Q);
     const size_t n3 = c->dm.n3;
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    ScratchN s(c, 10);
-    double *Cbeta = s[0], *S = s[1], *e = s[2], *P = s[3], *T = s[4], *Vs = s[5], *d2 = s[6];
-    double *d4S = s[7], *d4e = s[8], *d4Y = s[9];
-    Scratch etas(c, 10);
-    double *eta = etas, *etag = eta + 5 * n3;
+    ScratchNT<R> s(c, 10);
+    R *Cbeta = s[0], *S = s[1], *e = s[2], *P = s[3], *T = s[4], *Vs = s[5], *d2 = s[6];
+    R *d4S = s[7], *d4e = s[8], *d4Y = s[9];
+    ScratchT<R> etas(c, 10);
+    R *eta = etas, *etag = eta + 5 * n3;
     const double *g = c->gamma_eff;
-    const double *G0 = c->grad[0], *G1 = c->grad[1], *G2 = c->grad[2], *G3 = c->grad[3], *G4 = c->grad[4],
-                 *G5 = c->grad[5], *G6 = c->grad[6], *G7 = c->grad[7], *G8 = c->grad[8];
+    R *const *Gr = Store<R>::grad(c);
+    const R *G0 = Gr[0], *G1 = Gr[1], *G2 = Gr[2], *G3 = Gr[3], *G4 = Gr[4], *G5 = Gr[5], *G6 = Gr[6],
+            *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
     {
         PFOR(c, n3, {
@@ -453,17 +541,19 @@ int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
             double fac1 = g[p] - 1.0;
             double fac3 = f.g1 / (f.g1 - 1.0);
             fac3 = fac3 * 1.0 / (Y[p] + f.eps * (1.0 - Y[p]));
-            Vs[p] = 1.0 / Q4[p];
-            P[p] = fac1 * (Q5[p] - 5.0e-1 * Vs[p] * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
-            T[p] = fac3 * Vs[p] * P[p];
-            e[p] = Vs[p] * (Q5[p] - 5.0e-1 * Vs[p] * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+            double vs = 1.0 / Q4[p];
+            double pp = fac1 * (Q5[p] - 5.0e-1 * vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+            Vs[p] = vs;
+            P[p] = pp;
+            T[p] = fac3 * vs * pp;
+            e[p] = vs * (Q5[p] - 5.0e-1 * vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
             S[p] = sqrt(5.0e-1 * (s1 * s1 + s5 * s5 + s9 * s9 + 2.0 * (s2 * s4 + s3 * s7 + s6 * s8)));
         });
         ST_TRY(laplacian(c, S, d2));
         ST_TRY(laplacian(c, d2, d4S));
         ST_TRY(laplacian(c, e, d2));
         ST_TRY(laplacian(c, d2, d4e));
-        ST_TRY(laplacian(c, Y, d2));
+        ST_TRY(laplacian(c, Yr, d2));
         ST_TRY(laplacian(c, d2, d4Y));
         const double C_mu = 2.0e-3, C_k = 1.0e-2;
         PFOR(c, n3, {
@@ -478,10 +568,11 @@ int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
             double tmp2 = (Y[p] < 0.0) ? 0.0 : 1.0;
             eta[3 * n3 + p] = cs * ((Y[p] - 1.0) * tmp1 - Y[p] * (1.0 - tmp2));
         });
-        ST_TRY(dev_gaussian_filter(c, eta, etag, 5));
+        ST_TRY(gaussian_filter_t<R>(c, eta, etag, 5));
         const double DX6 = pow(c->DX, 6.0), DX5 = pow(c->DX, 5.0), DX = c->DX;
         const double C_D = 1.0e-4, C_Y = 100.0;
-        double *hb = c->hyp[H_BETA], *hv = c->hyp[H_VISC], *hk = c->hyp[H_K], *hd = c->hyp[H_D];
+        R **H = Store<R>::hyp(c);
+        R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K], *hd = H[H_D];
         PFOR(c, n3, {
             hb[p] = etag[2 * n3 + p] * DX6;
             hv[p] = etag[p] * DX6;
@@ -496,21 +587,24 @@ int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
 // is accumulated by the derivative kernels themselves in the reference's
 // x, y, z order (iadd), so dF*/dE* are never stored; fluxes that are products
 // of stored fields are formed by the derivative kernels while loading.
-int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
+template <class R>
+static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, const R *Yr) {
     if (c->p.hyper_param == 0) return ST_OK;
     const size_t n3 = c->dm.n3;
-    ST_TRY(dev_compute_hyper(c, Q, Y));
+    ST_TRY(compute_hyper_t<R>(c, Q, Y, Yr));
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3;
-    ScratchN s(c, 9);
-    double *U1 = s[0], *U2 = s[1], *U3 = s[2], *dila = s[3], *S1 = s[4], *S2 = s[5], *S3 = s[6];
-    double *Flux = s[7], *Flux2 = s[8];
-    Scratch Qhs(c, 5);
-    double *Qh = Qhs;   // Qh(:,:,:,4) stays zero and is never added
-    double *h1 = Qh, *h2 = Qh + n3, *h3 = Qh + 2 * n3, *h5 = Qh + 4 * n3;
-    const double *G0 = c->grad[0], *G1 = c->grad[1], *G2 = c->grad[2], *G3 = c->grad[3], *G4 = c->grad[4],
-                 *G5 = c->grad[5], *G6 = c->grad[6], *G7 = c->grad[7], *G8 = c->grad[8];
-    const double *GTx = c->grad[G_DTDX], *GTy = c->grad[G_DTDY], *GTz = c->grad[G_DTDZ];
-    const double *vh = c->hyp[H_VISC], *bh = c->hyp[H_BETA], *kh = c->hyp[H_K];
+    ScratchNT<R> s(c, 9);
+    R *U1 = s[0], *U2 = s[1], *U3 = s[2], *dila = s[3], *S1 = s[4], *S2 = s[5], *S3 = s[6];
+    R *Flux = s[7], *Flux2 = s[8];
+    ScratchT<R> Qhs(c, 5);
+    R *Qh = Qhs;   // Qh(:,:,:,4) stays zero and is never added
+    R *h1 = Qh, *h2 = Qh + n3, *h3 = Qh + 2 * n3, *h5 = Qh + 4 * n3;
+    R *const *Gr = Store<R>::grad(c);
+    const R *G0 = Gr[0], *G1 = Gr[1], *G2 = Gr[2], *G3 = Gr[3], *G4 = Gr[4], *G5 = Gr[5], *G6 = Gr[6],
+            *G7 = Gr[7], *G8 = Gr[8];
+    const R *GTx = Gr[G_DTDX], *GTy = Gr[G_DTDY], *GTz = Gr[G_DTDZ];
+    R *const *H = Store<R>::hyp(c);
+    const R *vh = H[H_VISC], *bh = H[H_BETA], *kh = H[H_K];
     PFOR(c, n3, {
         U1[p] = Q1[p] / Q4[p];
         U2[p] = Q2[p] / Q4[p];
@@ -523,31 +617,31 @@ int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
         Flux2[p] = 2.0 * vh[p] * G4[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
     });
     // x momentum: Qh1 = dFx + dFy + dFz, Qh5 = dEx + dEy + dEz
-    ST_TRY(dev_dfd(c, 0, 0, Flux, h1, 0, 1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(U1, Flux), h5, 0, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(vh, S1), h1, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mulmul(vh, S1, U1), h5, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(vh, S2), h1, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mulmul(vh, S2, U1), h5, 1, 1.0));
+    ST_TRY(dfd(c, 0, 0, Flux, h1, 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(U1, Flux), h5, 0, 1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(vh, S1), h1, 1, 1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mulmul(vh, S1, U1), h5, 1, 1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mul(vh, S2), h1, 1, 1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S2, U1), h5, 1, 1.0));
     // y momentum (x, y, z accumulation order)
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(vh, S1), h2, 0, 1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mulmul(vh, S1, U2), h5, 1, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, Flux2, h2, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(U2, Flux2), h5, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(vh, S1), h2, 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S1, U2), h5, 1, 1.0));
+    ST_TRY(dfd(c, 1, 0, Flux2, h2, 1, 1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(U2, Flux2), h5, 1, 1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
     // z momentum
     PFOR(c, n3, { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mulmul(vh, S3, U3), h5, 1, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, Flux, h3, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(U3, Flux), h5, 1, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mulmul(vh, S3, U3), h5, 1, 1.0));
+    ST_TRY(dfd(c, 2, 0, Flux, h3, 1, 1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mul(U3, Flux), h5, 1, 1.0));
     // artificial heat flux
-    ST_TRY(dev_dfd_prod(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 0, pr_mul(kh, GTz), h5, 1, 1.0));
+    ST_TRY(dfd(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
+    ST_TRY(dfd(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
+    ST_TRY(dfd(c, 2, 0, pr_mul(kh, GTz), h5, 1, 1.0));
     PFOR(c, n3, {
         for (int l = 0; l < 5; l++)
             if (l != 3) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] + Qh[l * n3 + p];
@@ -558,41 +652,46 @@ int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
 // Species_RHS src/species_rhs_sym.f:9-207.  Yrhs accumulates the three
 // convective derivatives in x, y, z order, then adds Ydiff, as
 // Yrhs = Yconvx + Yconvy + Yconvz + Ydiff does.
-int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+template <class R>
+static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const double *Y, const R *Yr,
+                         R *Yrhs) {
     if (c->p.hyper_param == 0) return ST_OK;
     const size_t n3 = c->dm.n3;
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
-    ScratchN s(c, 2);
-    double *Yd = s[0], *T = s[1];
-    const double *Dh = c->hyp[H_D];
+    const R *q1r = Qr, *q2r = Qr + n3, *q3r = Qr + 2 * n3, *q4r = Qr + 3 * n3;
+    ScratchNT<R> s(c, 2);
+    R *Yd = s[0], *T = s[1];
+    R *const *dYd = Store<R>::dYd(c);
+    const R *Dh = Store<R>::hyp(c)[H_D];
     const double *g = c->gamma_eff;
     PFOR(c, n3, {
         double Vs, P, Tt;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, P, Tt);
         T[p] = Tt;
     });
-    ST_TRY(dev_dfd(c, 0, 0, Y, c->dYd[0], 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, Y, c->dYd[1], 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, Y, c->dYd[2], 0, 1.0));
-    ST_TRY(dev_dfd_prod(c, 0, 1, pr_mul(Q1, Y), Yrhs, 0, -1.0));
-    ST_TRY(dev_dfd_prod(c, 1, 1, pr_mul(Q2, Y), Yrhs, 1, -1.0));
-    ST_TRY(dev_dfd_prod(c, 2, 1, pr_mul(Q3, Y), Yrhs, 1, -1.0));
+    ST_TRY(dfd(c, 0, 0, Yr, dYd[0], 0, 1.0));
+    ST_TRY(dfd(c, 1, 0, Yr, dYd[1], 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, Yr, dYd[2], 0, 1.0));
+    ST_TRY(dfd(c, 0, 1, pr_mul(q1r, Yr), Yrhs, 0, -1.0));
+    ST_TRY(dfd(c, 1, 1, pr_mul(q2r, Yr), Yrhs, 1, -1.0));
+    ST_TRY(dfd(c, 2, 1, pr_mul(q3r, Yr), Yrhs, 1, -1.0));
     const double cst = 1.0 - f.eps * f.g2 * (f.g1 - 1.0) / (f.g1 * (f.g2 - 1.0));
     for (int d = 0; d < 3; d++) {
-        Prod fl{};
-        fl.op = PR_SPEC; fl.a = Q4; fl.b = Dh; fl.c = c->dYd[d]; fl.k0 = f.Re1_inv; fl.k1 = f.Sc_inv;
-        Prod ft = fl;
+        ProdT<R> fl{};
+        fl.op = PR_SPEC; fl.a = q4r; fl.b = Dh; fl.c = dYd[d]; fl.k0 = f.Re1_inv; fl.k1 = f.Sc_inv;
+        ProdT<R> ft = fl;
         ft.op = PR_SPECT; ft.d = T; ft.k2 = cst;
-        ST_TRY(dev_dfd_prod(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
-        ST_TRY(dev_dfd_prod(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
+        ST_TRY(dfd(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
+        ST_TRY(dfd(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
     }
     PFOR(c, n3, { Yrhs[p] = Yrhs[p] + Yd[p]; });
     return ST_OK;
 }
 
 // bc_RHS src/bc_mf.f:11-463 (active face blocks)
-int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+template <class R>
+static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     const size_t n3 = c->dm.n3;
     const int Mx = c->dm.n[0], My = c->dm.n[1], Mz = c->dm.n[2];
     Phys f = phys(c);
@@ -605,17 +704,18 @@ int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs
         if (k == 0) Q3[p] = 0.0;
         if (j == 0) Q2[p] = 0.0;
     });
-    ScratchN s(c, 4);
-    double *P = s[0], *dPx = s[1], *dPy = s[2], *dPz = s[3];
+    ScratchNT<R> s(c, 4);
+    R *P = s[0], *dPx = s[1], *dPy = s[2], *dPz = s[3];
     PFOR(c, n3, {
         double Vs, Pp, T;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, Pp, T);
         P[p] = Pp;
     });
-    ST_TRY(dev_dfd(c, 0, 0, P, dPx, 0, 1.0));
-    ST_TRY(dev_dfd(c, 1, 0, P, dPy, 0, 1.0));
-    ST_TRY(dev_dfd(c, 2, 0, P, dPz, 0, 1.0));
-    const double *Gxx = c->grad[G_DUX_DX], *Gyy = c->grad[G_DUY_DY], *Gzz = c->grad[G_DUZ_DZ];
+    ST_TRY(dfd(c, 0, 0, P, dPx, 0, 1.0));
+    ST_TRY(dfd(c, 1, 0, P, dPy, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, P, dPz, 0, 1.0));
+    R *const *Gr = Store<R>::grad(c);
+    const R *Gxx = Gr[G_DUX_DX], *Gyy = Gr[G_DUY_DY], *Gzz = Gr[G_DUZ_DZ];
     // faces in the reference order x, y, z (later faces overwrite edges)
     for (int face = 0; face < 3; face++) {
         size_t nf = face == 0 ? (size_t)My * Mz : face == 1 ? (size_t)Mx * Mz : (size_t)Mx * My;
@@ -654,7 +754,8 @@ int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs
 }
 
 // Sponge_Forcing src/sponge_mf.f:7-127
-int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+template <class R>
+static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     const size_t n3 = c->dm.n3;
     const int Mx = c->dm.n[0], My = c->dm.n[1], Mz = c->dm.n[2];
     const double g1 = c->p.gamma1;
@@ -686,6 +787,69 @@ int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double
     return ST_OK;
 }
 
+// ---- entry points on double arrays -----------------------------------------------
+// In the FP32 mode the caller's double arrays are rounded to float copies,
+// the float form runs, and accumulated outputs are widened back.
+int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
+    if (!fp32_mode(c)) return rhs_t<double>(c, Q, Q, Qrhs, Y);
+    const size_t n3 = c->dm.n3;
+    ScratchT<float> Qs(c, 5), Rs(c, 5);
+    ST_TRY(dev_to_float(c, Q, Qs, 5 * n3));
+    ST_TRY(rhs_t<float>(c, Q, Qs, Rs, Y));
+    return dev_to_double(c, Rs, Qrhs, 5 * n3);
+}
+
+int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
+    if (!fp32_mode(c)) return compute_hyper_t<double>(c, Q, Y, Y);
+    ScratchT<float> Ys(c, 1);
+    ST_TRY(dev_to_float(c, Y, Ys, c->dm.n3));
+    return compute_hyper_t<float>(c, Q, Y, Ys);
+}
+
+int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
+    if (!fp32_mode(c)) return hyper_rhs_t<double>(c, Q, Qrhs, Y, Y);
+    const size_t n3 = c->dm.n3;
+    ScratchT<float> Ys(c, 1), Rs(c, 5);
+    ST_TRY(dev_to_float(c, Y, Ys, n3));
+    ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
+    ST_TRY(hyper_rhs_t<float>(c, Q, Rs, Y, Ys));
+    return dev_to_double(c, Rs, Qrhs, 5 * n3);
+}
+
+int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    if (!fp32_mode(c)) return species_rhs_t<double>(c, Q, Q, Qrhs, Y, Y, Yrhs);
+    const size_t n3 = c->dm.n3;
+    ScratchT<float> Qs(c, 5), Ys(c, 1), Rs(c, 5), YRs(c, 1);
+    ST_TRY(dev_to_float(c, Q, Qs, 5 * n3));
+    ST_TRY(dev_to_float(c, Y, Ys, n3));
+    ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
+    ST_TRY(species_rhs_t<float>(c, Q, Qs, Rs, Y, Ys, YRs));
+    ST_TRY(dev_to_double(c, Rs, Qrhs, 5 * n3));
+    return dev_to_double(c, YRs, Yrhs, n3);
+}
+
+int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    if (!fp32_mode(c)) return bc_rhs_t<double>(c, Q, Qrhs, Y, Yrhs);
+    const size_t n3 = c->dm.n3;
+    ScratchT<float> Rs(c, 5), YRs(c, 1);
+    ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
+    ST_TRY(dev_to_float(c, Yrhs, YRs, n3));
+    ST_TRY(bc_rhs_t<float>(c, Q, Rs, Y, YRs));
+    ST_TRY(dev_to_double(c, Rs, Qrhs, 5 * n3));
+    return dev_to_double(c, YRs, Yrhs, n3);
+}
+
+int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    if (!fp32_mode(c)) return sponge_t<double>(c, Q, Qrhs, Y, Yrhs);
+    const size_t n3 = c->dm.n3;
+    ScratchT<float> Rs(c, 5), YRs(c, 1);
+    ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
+    ST_TRY(dev_to_float(c, Yrhs, YRs, n3));
+    ST_TRY(sponge_t<float>(c, Q, Rs, Y, YRs));
+    ST_TRY(dev_to_double(c, Rs, Qrhs, 5 * n3));
+    return dev_to_double(c, YRs, Yrhs, n3);
+}
+
 // Fix_Pressure pproc/pproc_mf.f:190-233; periodic family
 // src/lddrk4_periodic_sf.f:436-473 (base pressure 0.71463, gamma_eff = gamma)
 int dev_fix_pressure(st_ctx *c, double *Q) {
@@ -714,16 +878,8 @@ int dev_compact_filter(st_ctx *c, const double *F, double *F0, int nvar) {
     return ST_OK;
 }
 
-// Gaussian_Filter src/filters_sym.f:1046-1071
 int dev_gaussian_filter(st_ctx *c, const double *F, double *Fg, int nvar) {
-    const size_t n3 = c->dm.n3;
-    Scratch tmp(c);
-    for (int l = 0; l < nvar; l++) {
-        ST_TRY(dev_gauss(c, 0, F + l * n3, Fg + l * n3));
-        ST_TRY(dev_gauss(c, 1, Fg + l * n3, tmp));
-        ST_TRY(dev_gauss(c, 2, tmp, Fg + l * n3));
-    }
-    return ST_OK;
+    return gaussian_filter_t<double>(c, F, Fg, nvar);
 }
 
 // ---- reductions ----------------------------------------------------------------
@@ -759,8 +915,9 @@ __global__ void k_cfl(const double *Q, const double *g, size_t n3, double DX, do
 }
 
 // Compute_Tstep hyperviscous limits src/lddrk4_nonperiodic_mf.f:100-145 -> out[2..5] minima
-__global__ void k_tstep(const double *Q, const double *Y, const double *g, const double *vh, const double *bh,
-                        const double *kh, const double *Dh, size_t n3, double del, double g1, double g2,
+template <class R>
+__global__ void k_tstep(const double *Q, const double *Y, const double *g, const R *vh, const R *bh,
+                        const R *kh, const R *Dh, size_t n3, double del, double g1, double g2,
                         double eps, double *out) {
     double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY, m6 = INFINITY;
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
@@ -772,10 +929,10 @@ __global__ void k_tstep(const double *Q, const double *Y, const double *g, const
         double T = g1 * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3));
         T = T / (double)fac1;
         double q4 = Q[3 * n3 + p];
-        double w3 = q4 * pow(del, 2.0) / vh[p];
-        double w4 = q4 * pow(del, 2.0) / bh[p];
-        double w5 = q4 * pow(del * tmp2, 2.0) / (kh[p] * T);
-        double w6 = pow(del, 2.0) / Dh[p];
+        double w3 = q4 * pow(del, 2.0) / (double)vh[p];
+        double w4 = q4 * pow(del, 2.0) / (double)bh[p];
+        double w5 = q4 * pow(del * tmp2, 2.0) / ((double)kh[p] * T);
+        double w6 = pow(del, 2.0) / (double)Dh[p];
         m3 = fmin(m3, w3); m4 = fmin(m4, w4); m5 = fmin(m5, w5); m6 = fmin(m6, w6);
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -792,7 +949,8 @@ __global__ void k_tstep(const double *Q, const double *Y, const double *g, const
 
 // Compute_Tstep of the periodic family, src/lddrk4_periodic_sf.f:105-135:
 // single-fluid temperature, no diffusivity limit (out[5] stays +inf)
-__global__ void k_tstep_sf(const double *Q, const double *vh, const double *bh, const double *kh, size_t n3,
+template <class R>
+__global__ void k_tstep_sf(const double *Q, const R *vh, const R *bh, const R *kh, size_t n3,
                            double del, double gam, double *out) {
     double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY;
     const double fac = gam * (gam - 1.0);
@@ -801,9 +959,9 @@ __global__ void k_tstep_sf(const double *Q, const double *vh, const double *bh, 
         double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p], q5 = Q[4 * n3 + p];
         double tmp2 = sqrt(fac * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3)));
         double T = gam * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3));
-        double w3 = q4 * pow(del, 2.0) / vh[p];
-        double w4 = q4 * pow(del, 2.0) / bh[p];
-        double w5 = q4 * pow(del * tmp2, 2.0) / ((kh[p]) * T);
+        double w3 = q4 * pow(del, 2.0) / (double)vh[p];
+        double w4 = q4 * pow(del, 2.0) / (double)bh[p];
+        double w5 = q4 * pow(del * tmp2, 2.0) / ((double)kh[p] * T);
         m3 = fmin(m3, w3); m4 = fmin(m4, w4); m5 = fmin(m5, w5);
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -854,6 +1012,25 @@ int dev_compute_cfl(st_ctx *c, const double *Q, bool to_host, double *stab, doub
 
 // dt lands in dscal[6] (device); the context's host copy is refreshed only
 // when the caller asks for it.
+template <class R>
+static int tstep_hyper(st_ctx *c, const double *Q, const double *Y, bool sf) {
+    R *const *H = Store<R>::hyp(c);
+    if (sf) {
+        int pi = prof_start(c, "k_tstep", (40.0 + 3 * sizeof(R)) * c->dm.n3);
+        k_tstep_sf<R><<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, H[H_VISC], H[H_BETA], H[H_K], c->dm.n3,
+                                                                   c->DX, c->p.gamma1, c->dscal);
+        prof_stop(c, pi);
+    } else {
+        int pi = prof_start(c, "k_tstep", (56.0 + 4 * sizeof(R)) * c->dm.n3);
+        k_tstep<R><<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(
+            Q, Y, c->gamma_eff, H[H_VISC], H[H_BETA], H[H_K], H[H_D], c->dm.n3, c->DX, c->p.gamma1, c->p.gamma2,
+            c->p.epsilon, c->dscal);
+        prof_stop(c, pi);
+    }
+    ST_CUDA(c, cudaGetLastError());
+    return ST_OK;
+}
+
 int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, bool resv_on_device,
                       double cfl_resv_host) {
     const bool sf = c->p.family == ST_FAMILY_PERIODIC;
@@ -862,20 +1039,7 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
     if (use_hyper) {
         // minima start at +inf (a device fill, so that the step can be captured in a graph)
         ST_TRY(dev_fill(c, c->dscal + 2, 4, INFINITY));
-        if (sf) {
-            int pi = prof_start(c, "k_tstep", 64.0 * c->dm.n3);
-            k_tstep_sf<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, c->hyp[H_VISC], c->hyp[H_BETA],
-                                                                    c->hyp[H_K], c->dm.n3, c->DX,
-                                                                    c->p.gamma1, c->dscal);
-            prof_stop(c, pi);
-        } else {
-            int pi = prof_start(c, "k_tstep", 88.0 * c->dm.n3);
-            k_tstep<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(
-                Q, Y, c->gamma_eff, c->hyp[H_VISC], c->hyp[H_BETA], c->hyp[H_K], c->hyp[H_D], c->dm.n3, c->DX,
-                c->p.gamma1, c->p.gamma2, c->p.epsilon, c->dscal);
-            prof_stop(c, pi);
-        }
-        ST_CUDA(c, cudaGetLastError());
+        ST_TRY(fp32_mode(c) ? tstep_hyper<float>(c, Q, Y, sf) : tstep_hyper<double>(c, Q, Y, sf));
     }
     c->launches++;
     const double f = sf ? (double)0.2f : 0.2;
@@ -897,6 +1061,34 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
 // build, i.e. zero: rk_mode 0; rk_mode 1 takes the commented-out HHM 4-6
 // values of src/header:267-276).  Each stage: RHS, Hyper_RHS, update,
 // Compact_Filter (Q = Qf), Fix_Pressure.
+// The state in the intermediate type R: the state arrays themselves in FP64;
+// float copies, refreshed before each stage, in the FP32 mode.
+template <class R> struct StateCopy;
+template <> struct StateCopy<double> {
+    StateCopy(st_ctx *) {}
+    const double *q(const double *Q) const { return Q; }
+    const double *y(const double *Y) const { return Y; }
+};
+template <> struct StateCopy<float> {
+    ScratchT<float> qs, ys;
+    explicit StateCopy(st_ctx *c) : qs(c, 5), ys(c, 1) {}
+    const float *q(const double *) const { return qs; }
+    const float *y(const double *) const { return ys; }
+};
+template <class R>
+static int refresh(st_ctx *c, StateCopy<R> &sc, const double *Q, const double *Y, bool with_y) {
+    if constexpr (!is_fp64<R>()) {
+        const size_t n3 = c->dm.n3;
+        float *qs = sc.qs, *ys = sc.ys;
+        PFOR(c, n3, {
+            for (int l = 0; l < 5; l++) qs[l * n3 + p] = (float)Q[l * n3 + p];
+            if (with_y) ys[p] = (float)Y[p];
+        });
+    }
+    return ST_OK;
+}
+
+template <class R>
 static int lddrk4_sf(st_ctx *c) {
     static const double alpha1[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
                                      -2.016477077503357e+00, -1.056444269767207e+00};
@@ -911,6 +1103,7 @@ static int lddrk4_sf(st_ctx *c) {
     const size_t n3 = c->dm.n3;
     Scratch Qfs(c, 5);
     double *Qf = Qfs;
+    StateCopy<R> sc(c);
     const double *dtp = c->dscal + 6;
     double *timep = c->dscal + 7;
     for (int loop = 0; loop < 2; loop++) {
@@ -921,9 +1114,11 @@ static int lddrk4_sf(st_ctx *c) {
             else if (c->p.rk_mode == 1) { al = alpha2[K]; be = beta2[K]; }
             else { al = 0.0; be = 0.0; }
             const bool first = K == 0;
-            double *Q = c->Q, *dQ = c->dQ, *QW = c->QW;
-            ST_TRY(dev_rhs(c, Q, dQ, c->Y));
-            ST_TRY(dev_hyper_rhs(c, Q, dQ, c->Y));
+            double *Q = c->Q, *QW = c->QW;
+            R *dQ = Store<R>::dQ(c);
+            ST_TRY(refresh<R>(c, sc, Q, c->Y, false));
+            ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, c->Y));
+            ST_TRY(hyper_rhs_t<R>(c, Q, dQ, c->Y, sc.y(c->Y)));
             PFOR(c, n3, {
                 double dt = *dtp;
                 for (int l = 0; l < 5; l++) {
@@ -945,8 +1140,8 @@ static int lddrk4_sf(st_ctx *c) {
     return ST_OK;
 }
 
-int dev_lddrk4(st_ctx *c, bool) {
-    if (c->p.family == ST_FAMILY_PERIODIC) return lddrk4_sf(c);
+template <class R>
+static int lddrk4_mf(st_ctx *c) {
     static const double alpha1[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
                                      -2.016477077503357e+00, -1.056444269767207e+00};
     static const double beta1[5] = {1.028639988104959e-01, 7.408540575766301e-01, 7.426530946683799e-01,
@@ -954,6 +1149,7 @@ int dev_lddrk4(st_ctx *c, bool) {
     const size_t n3 = c->dm.n3;
     Scratch rYs(c), Qfs(c, 5);
     double *rY = rYs, *Qf = Qfs;
+    StateCopy<R> sc(c);
     const double *dtp = c->dscal + 6;
     double *timep = c->dscal + 7;
     for (int loop = 0; loop < 2; loop++) {
@@ -961,13 +1157,15 @@ int dev_lddrk4(st_ctx *c, bool) {
             const bool real = loop == 0 || c->p.rk_mode == 1;
             const double al = real ? alpha1[K] : 0.0, be = real ? beta1[K] : 0.0;
             const bool first = K == 0;
-            double *Q = c->Q, *dQ = c->dQ, *QW = c->QW, *Y = c->Y, *drYi = c->drYi, *rYW = c->rYW;
+            double *Q = c->Q, *QW = c->QW, *Y = c->Y, *rYW = c->rYW;
+            R *dQ = Store<R>::dQ(c), *drYi = Store<R>::drYi(c);
+            ST_TRY(refresh<R>(c, sc, Q, Y, true));
             ST_TRY(dev_compute_gamma(c, Y));
-            ST_TRY(dev_rhs(c, Q, dQ, Y));
-            ST_TRY(dev_hyper_rhs(c, Q, dQ, Y));
-            ST_TRY(dev_species_rhs(c, Q, dQ, Y, drYi));
-            ST_TRY(dev_bc_rhs(c, Q, dQ, Y, drYi));
-            ST_TRY(dev_sponge(c, Q, dQ, Y, drYi));
+            ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, Y));
+            ST_TRY(hyper_rhs_t<R>(c, Q, dQ, Y, sc.y(Y)));
+            ST_TRY(species_rhs_t<R>(c, Q, sc.q(Q), dQ, Y, sc.y(Y), drYi));
+            ST_TRY(bc_rhs_t<R>(c, Q, dQ, Y, drYi));
+            ST_TRY(sponge_t<R>(c, Q, dQ, Y, drYi));
             PFOR(c, n3, {
                 double dt = *dtp;
                 double ry = Q[3 * n3 + p] * Y[p];
@@ -1005,6 +1203,12 @@ int dev_lddrk4(st_ctx *c, bool) {
         PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
     }
     return ST_OK;
+}
+
+int dev_lddrk4(st_ctx *c, bool) {
+    const bool f32 = fp32_mode(c);
+    if (c->p.family == ST_FAMILY_PERIODIC) return f32 ? lddrk4_sf<float>(c) : lddrk4_sf<double>(c);
+    return f32 ? lddrk4_mf<float>(c) : lddrk4_mf<double>(c);
 }
 
 // monitoring sums (Compute_Mom/KE/Mass/Energy/Entropy), two-pass block sums

@@ -24,11 +24,14 @@ class StParams(ctypes.Structure):
         ("c_beta_scale", ctypes.c_double),
         ("device", ctypes.c_int),
         ("family", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
 FAMILY_MF = 0          # two-species symmetric octant (src/main_mf.f)
 FAMILY_PERIODIC = 1    # single-fluid triply periodic box (src/main.f)
+PRECISION_FP64 = 0     # every array in double (the reference's REAL*8 build)
+PRECISION_FP32 = 1     # float intermediates; double state, accumulators, state filter, pressure recovery
 
 
 def default_params(nx, ny=None, nz=None, length=2.0 * math.pi, **kw):
@@ -54,6 +57,7 @@ def default_params(nx, ny=None, nz=None, length=2.0 * math.pi, **kw):
     p.c_beta_scale = 1.0
     p.device = 0
     p.family = FAMILY_MF
+    p.precision = PRECISION_FP64
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(f"st_params has no field {k!r}")
