@@ -162,6 +162,9 @@ int st_create(const st_params *p, st_ctx **out) {
     const int n[3] = {p->nx, p->ny, p->nz};
     for (int d = 0; d < 3; d++)
         if (n[d] % kLanes != 0 || n[d] < kLanes || choose_seg(n[d]) == 0) return ST_E_UNSUPPORTED;
+    // FP32 mode: a CTA of the line kernels owns 32 lines (two per thread)
+    if (p->precision == ST_PRECISION_FP32 && (p->ny % (2 * kLanes) != 0 || (p->nx * p->nz) % (2 * kLanes) != 0))
+        return ST_E_UNSUPPORTED;
     st_ctx *c = new (std::nothrow) st_ctx();
     if (!c) return ST_E_NOMEM;
     c->p = *p;

@@ -25,17 +25,20 @@ int choose_seg(int n);
 // Row tables of a constant-coefficient tridiagonal system, factorised as the
 // reference's tridiagonal_serial does (src/tridiagonal.f90:264-287), plus the
 // carry tables of the segmented solve.
-struct TriTab {
-    const double *l;    // forward multiplier of row i (row 0: 0)
-    const double *g;    // response of the forward value of row i to the carry-in
-    const double *up;   // upper diagonal c_i
-    const double *id;   // 1 / (b'_i + tiny)   (last row: 1 / b'_n)
-    const double *h;    // response of x_i to the carry from the right
-    const double *wf;   // [P][P]: carry into segment s = sum_{s'<s} wf[s'][s] * A_{s'}
-    const double *wb;   // [P][P]: carry into segment s = sum_{s'>s} wb[s'][s] * B_{s'}
-    int kf, kb;         // segments back/ahead whose carry weight is >= 1e-20
-    const double *cyc;  // periodic family: [n][2] corner correction (see st_tables.cpp), else null
+// A: arithmetic type of the solve (double; float for the FP32 mode's kernels).
+template <class A>
+struct TriTabT {
+    const A *l;    // forward multiplier of row i (row 0: 0)
+    const A *g;    // response of the forward value of row i to the carry-in
+    const A *up;   // upper diagonal c_i
+    const A *id;   // 1 / (b'_i + tiny)   (last row: 1 / b'_n)
+    const A *h;    // response of x_i to the carry from the right
+    const A *wf;   // [P][P]: carry into segment s = sum_{s'<s} wf[s'][s] * A_{s'}
+    const A *wb;   // [P][P]: carry into segment s = sum_{s'>s} wb[s'][s] * B_{s'}
+    int kf, kb;    // segments back/ahead whose carry weight can change a result of type A
+    const A *cyc;  // periodic family: [n][2] corner correction (see st_tables.cpp), else null
 };
+using TriTab = TriTabT<double>;
 
 // Same for the pentadiagonal systems of the compact filter
 // (pentadiagonal_serial, src/pentadiagonal.f90:319-374); carries are
@@ -111,6 +114,7 @@ struct st_ctx {
     st::Consts k;
     // tables [dir][kind]
     st::TriTab tri[3][4];
+    st::TriTabT<float> trif[3][4];   // FP32 mode: the same factors rounded to float
     st::PenTab pen[3][2];
     std::vector<void *> table_allocs;
     size_t table_bytes = 0;

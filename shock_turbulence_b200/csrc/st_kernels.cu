@@ -68,7 +68,7 @@ int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg) {
     return launch_line(c, OP_GAUSS, a);
 }
 
-// ---- FP32-field variants (the FP32 mode's derivative and Gaussian passes) ----
+// ---- FP32 mode (float fields and arithmetic, two lines per thread) ----------
 static ProdF plain_f(const float *F) {
     ProdF p{};
     p.op = PR_A;
@@ -76,11 +76,21 @@ static ProdF plain_f(const float *F) {
     return p;
 }
 
+// the kernels access a thread's two lines with one 8-byte load or store
+static int check_f2(st_ctx *c, const ProdF &F, const float *O1, const float *O2) {
+    const void *ptrs[6] = {F.a, F.b, F.c, F.d, O1, O2};
+    for (const void *p : ptrs)
+        if (reinterpret_cast<uintptr_t>(p) & 7)
+            return fail(c, ST_E_ARG, "FP32 line operators need 8-byte aligned fields");
+    return ST_OK;
+}
+
 int dev_dfd_prod_f(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd) {
+    ST_TRY(check_f2(c, F, dF, nullptr));
     LineArgsF a = make_args<float>(c, dir);
     a.F = F; a.O1 = dF; a.asym = asym; a.iadd = iadd;
     a.fac1 = cadd * c->s1[dir] * (double)(a.geo.n - 1);
-    a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
+    a.t1 = c->trif[dir][asym ? K_D1A : K_D1S];
     return launch_line(c, OP_D1, a);
 }
 
@@ -91,14 +101,16 @@ int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd,
 int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd) {
     LineArgsF a = make_args<float>(c, dir);
     a.F = plain_f(F); a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;
+    ST_TRY(check_f2(c, a.F, dF, d2F));
     a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
     a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];
-    a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
-    a.t2 = c->tri[dir][asym ? K_D2A : K_D2S];
+    a.t1 = c->trif[dir][asym ? K_D1A : K_D1S];
+    a.t2 = c->trif[dir][asym ? K_D2A : K_D2S];
     return launch_line(c, OP_D2, a);
 }
 
 int dev_gauss_f(st_ctx *c, int dir, const float *F, float *Fg) {
+    ST_TRY(check_f2(c, plain_f(F), Fg, nullptr));
     LineArgsF a = make_args<float>(c, dir);
     a.F = plain_f(F); a.O1 = Fg;
     return launch_line(c, OP_GAUSS, a);

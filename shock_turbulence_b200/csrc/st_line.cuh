@@ -14,38 +14,84 @@
 //  - segments exchange their end values through shared memory once per
 //    recurrence direction; the carry into each segment is a fixed linear
 //    combination of those values (tables wf/wb, mf/mb).
+//
+// FP32 mode: fields are float and the solves run in float, and a thread
+// works on TWO neighbouring lines (lanes 2l, 2l+1 of a 32-line CTA) through a
+// two-lane value type F2: one 8-byte access covers both lines' row, the LU
+// table value of a row is loaded once for both, and the two recurrences give
+// the dependent chains twice the independent work.
 #pragma once
 #include "st_internal.h"
 
 namespace st {
 
-// element (lane, row) of a CTA's 32 lines is base + lane*lstride + row*rstride
+// two float lines at one row
+struct F2 {
+    float x, y;
+    F2() = default;
+    __host__ __device__ constexpr F2(float a, float b) : x(a), y(b) {}
+    __host__ __device__ F2(double v) : x((float)v), y((float)v) {}   // a constant on both lines
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.x, -a.y); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ F2 operator*(float k, F2 a) { return F2(k * a.x, k * a.y); }
+__device__ __forceinline__ F2 operator*(F2 a, float k) { return F2(a.x * k, a.y * k); }
+__device__ __forceinline__ F2 operator*(double k, F2 a) { return (float)k * a; }
+__device__ __forceinline__ F2 operator*(F2 a, double k) { return a * (float)k; }
+// k*b + c with one rounding (the solves' explicit fma)
+__device__ __forceinline__ double vfma(double k, double b, double c) { return fma(k, b, c); }
+__device__ __forceinline__ F2 vfma(float k, F2 b, F2 c) { return F2(fmaf(k, b.x, c.x), fmaf(k, b.y, c.y)); }
+
+// storage type T -> value type V of a thread's lines, its scalar A, lines per thread W
+template <class T> struct Val;
+template <> struct Val<double> { using V = double; using A = double; static constexpr int W = 1; };
+template <> struct Val<float> { using V = F2; using A = float; static constexpr int W = 2; };
+
+// element (lane, row) of a CTA's lines is base + lane*W*lstride + row*rstride
 struct ColMap {
     size_t base, lstride, rstride;
 };
 struct LineGeo {
     int dir, n, My, Mz;
+    // W lines per thread: a CTA owns kLanes*W lines
+    template <int W>
     __device__ __forceinline__ ColMap map(unsigned blk) const {
+        constexpr int NL = kLanes * W;
         ColMap m;
-        const size_t sMy = My, sMz = Mz, jb = My / kLanes;
-        if (dir == 0) {            // lines (j,k): 32 consecutive j at one k
-            m.base = (blk % jb) * kLanes + sMy * (blk / jb); m.lstride = 1; m.rstride = sMy * sMz;
-        } else if (dir == 1) {     // lines (k,i): 32 consecutive lines, each contiguous
-            m.base = sMy * (size_t)blk * kLanes; m.lstride = sMy; m.rstride = 1;
-        } else {                   // lines (j,i): 32 consecutive j at one i
-            m.base = (blk % jb) * kLanes + sMy * sMz * (blk / jb); m.lstride = 1; m.rstride = sMy;
+        const size_t sMy = My, sMz = Mz, jb = My / NL;
+        if (dir == 0) {            // lines (j,k): NL consecutive j at one k
+            m.base = (blk % jb) * NL + sMy * (blk / jb); m.lstride = 1; m.rstride = sMy * sMz;
+        } else if (dir == 1) {     // lines (k,i): NL consecutive lines, each contiguous
+            m.base = sMy * (size_t)blk * NL; m.lstride = sMy; m.rstride = 1;
+        } else {                   // lines (j,i): NL consecutive j at one i
+            m.base = (blk % jb) * NL + sMy * sMz * (blk / jb); m.lstride = 1; m.rstride = sMy;
         }
         return m;
     }
 };
 
-// The producer's fields are double or float (FP32 mode); values are
-// converted to double as they are loaded and every operation is in double.
-template <class T>
-__device__ __forceinline__ double ld(const T *p) { return (double)__ldg(p); }
+// Loads of one value: a double (a float field read in double), a float, or
+// the two float lines at p and p+1 (8-byte aligned) as one F2.
+template <class V, class T> struct Ld;
+template <class T> struct Ld<double, T> {
+    __device__ __forceinline__ static double get(const T *p) { return (double)__ldg(p); }
+};
+template <> struct Ld<float, float> {
+    __device__ __forceinline__ static float get(const float *p) { return __ldg(p); }
+};
+template <> struct Ld<F2, float> {
+    __device__ __forceinline__ static F2 get(const float *p) {
+        float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+        return F2(v.x, v.y);
+    }
+};
 
-template <int OP, class T>
-__device__ __forceinline__ double prod_eval(const ProdT<T> &P, size_t i) {
+template <int OP, class V = double, class T>
+__device__ __forceinline__ V prod_eval(const ProdT<T> &P, size_t i) {
+    using A = typename Val<T>::A;
+    auto ld = [&](const T *p) { return Ld<V, T>::get(p); };
     if constexpr (OP == PR_MUL) {
         return ld(P.a + i) * ld(P.b + i);
     } else if constexpr (OP == PR_ADDMUL) {
@@ -53,12 +99,12 @@ __device__ __forceinline__ double prod_eval(const ProdT<T> &P, size_t i) {
     } else if constexpr (OP == PR_MULMUL) {
         return ld(P.c + i) * (ld(P.a + i) * ld(P.b + i));
     } else if constexpr (OP == PR_SPEC) {
-        double a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i);
-        return a * b * c + a * c * P.k0 * P.k1;
+        V a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i);
+        return a * b * c + a * c * (A)P.k0 * (A)P.k1;
     } else if constexpr (OP == PR_SPECT) {
-        double a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i), d = ld(P.d + i);
-        double fl = a * b * c + a * c * P.k0 * P.k1;
-        return P.k2 * d * fl;
+        V a = ld(P.a + i), b = ld(P.b + i), c = ld(P.c + i), d = ld(P.d + i);
+        V fl = a * b * c + a * c * (A)P.k0 * (A)P.k1;
+        return (A)P.k2 * d * fl;
     } else {
         return ld(P.a + i);
     }
@@ -71,50 +117,66 @@ __device__ __forceinline__ int halo_row(int row, int n, int cyc) {
     return row < 0 ? (cyc ? row + n : 0) : (row > n - 1 ? (cyc ? row - n : n - 1) : row);
 }
 
-// rows a-H .. a+S+H-1 of this lane's line into v
-template <int S, int H, int OP, class T>
-__device__ __forceinline__ void load_rows(double (&v)[S + 2 * H], const ProdT<T> &F, const ColMap &m, int lane,
+// rows a-H .. a+S+H-1 of this lane's line(s) into v (x and z lines: the W
+// lines of a thread are neighbours in memory, lstride = 1)
+template <int S, int H, int OP, class T, class V>
+__device__ __forceinline__ void load_rows(V (&v)[S + 2 * H], const ProdT<T> &F, const ColMap &m, int lane,
                                           int a, int n, int cyc) {
-    const size_t p = m.base + (size_t)lane * m.lstride;
+    const size_t p = m.base + (size_t)lane * Val<T>::W * m.lstride;
 #pragma unroll
     for (int q = 0; q < S + 2 * H; q++) {
         int row = halo_row(a - H + q, n, cyc);
-        v[q] = prod_eval<OP>(F, p + (size_t)row * m.rstride);
+        v[q] = prod_eval<OP, V>(F, p + (size_t)row * m.rstride);
     }
 }
 
-template <int S, int N, class T>
-__device__ __forceinline__ void store_rows(const double (&r)[N], T *__restrict__ O, const ColMap &m,
+// plain (not read-only-path) load and store of one value
+__device__ __forceinline__ double ldp(const double *p) { return *p; }
+__device__ __forceinline__ F2 ldp2(const float *p) {
+    float2 v = *reinterpret_cast<const float2 *>(p);
+    return F2(v.x, v.y);
+}
+__device__ __forceinline__ void stv(double *p, double v) { *p = v; }
+__device__ __forceinline__ void stv(float *p, double v) { *p = (float)v; }
+__device__ __forceinline__ void stv(float *p, F2 v) { *reinterpret_cast<float2 *>(p) = make_float2(v.x, v.y); }
+
+template <int S, int N, class T, class V>
+__device__ __forceinline__ void store_rows(const V (&r)[N], T *__restrict__ O, const ColMap &m,
                                            int lane, int a, int add) {
-    T *p = O + m.base + (size_t)lane * m.lstride + (size_t)a * m.rstride;
+    T *p = O + m.base + (size_t)lane * Val<T>::W * m.lstride + (size_t)a * m.rstride;
     if (add) {
-        double prev[S];
+        V prev[S];
 #pragma unroll
-        for (int t = 0; t < S; t++) prev[t] = (double)p[(size_t)t * m.rstride];
+        for (int t = 0; t < S; t++) {
+            if constexpr (Val<T>::W == 2) prev[t] = ldp2(p + (size_t)t * m.rstride);
+            else prev[t] = (double)p[(size_t)t * m.rstride];
+        }
 #pragma unroll
-        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = (T)(prev[t] + r[t]);
+        for (int t = 0; t < S; t++) stv(p + (size_t)t * m.rstride, prev[t] + r[t]);
     } else {
 #pragma unroll
-        for (int t = 0; t < S; t++) p[(size_t)t * m.rstride] = (T)r[t];
+        for (int t = 0; t < S; t++) stv(p + (size_t)t * m.rstride, r[t]);
     }
 }
 
 // shared buffers for the segment end values of one solve, and the corner
 // values of a periodic line (rows 0, 1, n-2, n-1 of the banded solution)
-struct CarryBuf {
-    double a[kMaxSeg][kLanes][2];
-    double b[kMaxSeg][kLanes][2];
-    double cy[kLanes][4];
+template <class V>
+struct CarryBufT {
+    V a[kMaxSeg][kLanes][2];
+    V b[kMaxSeg][kLanes][2];
+    V cy[kLanes][4];
 };
+using CarryBuf = CarryBufT<double>;
 
 // ---- periodic lines: corner correction after the banded solve ------------
 // x_i = y_i - sum_k K_ik y_{j_k} with the corner rows j = {0, n-1} (K = 2,
 // tridiagonal) or {0, 1, n-2, n-1} (K = 4, pentadiagonal); the table holds
 // -K row-major.  The first and last segments publish the corner values; the
 // barrier also orders them after every read of the previous solve's cy.
-template <int S, int N, int KC>
-__device__ __forceinline__ void cyc_fix(double (&r)[N], const double *__restrict__ Kt, int s, int P, int lane,
-                                        CarryBuf &cb) {
+template <int S, int N, int KC, class V, class A>
+__device__ __forceinline__ void cyc_fix(V (&r)[N], const A *__restrict__ Kt, int s, int P, int lane,
+                                        CarryBufT<V> &cb) {
     if (KC == 2) {
         if (s == 0) cb.cy[lane][0] = r[0];
         if (s == P - 1) cb.cy[lane][1] = r[S - 1];
@@ -123,15 +185,15 @@ __device__ __forceinline__ void cyc_fix(double (&r)[N], const double *__restrict
         if (s == P - 1) { cb.cy[lane][2] = r[S - 2]; cb.cy[lane][3] = r[S - 1]; }
     }
     __syncthreads();
-    double y[KC];
+    V y[KC];
 #pragma unroll
     for (int k = 0; k < KC; k++) y[k] = cb.cy[lane][k];
-    const double *kr = Kt + (size_t)s * S * KC;
+    const A *kr = Kt + (size_t)s * S * KC;
 #pragma unroll
     for (int t = 0; t < S; t++) {
-        double v = r[t];
+        V v = r[t];
 #pragma unroll
-        for (int k = 0; k < KC; k++) v = fma(__ldg(kr + t * KC + k), y[k], v);
+        for (int k = 0; k < KC; k++) v = vfma(__ldg(kr + t * KC + k), y[k], v);
         r[t] = v;
     }
 }
@@ -141,28 +203,28 @@ __device__ __forceinline__ void cyc_fix(double (&r)[N], const double *__restrict
 // x_i = (r'_i - c_i x_{i+1}) / (b'_i + tiny) of tridiagonal_serial
 // (src/tridiagonal.f90:274-284) per segment with zero carries, then the
 // carry corrections.  Caller guarantees cb is free (synchronised).
-template <int S, int N>
-__device__ __forceinline__ void tri_solve(double (&r)[N], const TriTab &T, int s, int P, int lane,
-                                          CarryBuf &cb) {
+template <int S, int N, class V, class A>
+__device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s, int P, int lane,
+                                          CarryBufT<V> &cb) {
     const int a = s * S;
 #pragma unroll
     for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * __ldg(T.l + a + t);
     cb.a[s][lane][0] = r[S - 1];
     __syncthreads();
-    double cin = 0.0;
-    for (int sp = max(0, s - T.kf); sp < s; sp++) cin = fma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
+    V cin = V(0.0);
+    for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
 #pragma unroll
-    for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g + a + t), cin, r[t]);
+    for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
     r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
 #pragma unroll
     for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
     cb.b[s][lane][0] = r[0];
     __syncthreads();
-    double ein = 0.0;
+    V ein = V(0.0);
     for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
-        ein = fma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
+        ein = vfma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
 #pragma unroll
-    for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.h + a + t), ein, r[t]);
+    for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.h + a + t), ein, r[t]);
 }
 
 // ---- segmented constant-coefficient pentadiagonal solve ------------------
@@ -219,26 +281,33 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
 // the reference formulas term by term (Fortran evaluates left to right).
 // Boundary rows belong to the first/last segment only: those warps re-read
 // the few rows they need from global memory (warp-uniform branch).
-template <int OP, class T = double>
+template <int OP, class T = double, class V = double>
 struct RowReader {
-    const double *tile;       // shared tile row (y lines) or null
+    using A = typename Val<T>::A;
+    const A *tile;            // shared tile row of the thread's (first) line (y lines) or null
     const ProdT<T> *F;        // global producer (x, z lines)
     size_t base, rstride;
-    __device__ __forceinline__ double operator()(int row) const {
-        return tile ? tile[row] : prod_eval<OP>(*F, base + (size_t)row * rstride);
+    int tstride;              // tile distance between a thread's two lines (W = 2)
+    __device__ __forceinline__ V operator()(int row) const {
+        if constexpr (Val<T>::W == 2) {
+            return tile ? V(tile[row], tile[row + tstride]) : prod_eval<OP, V>(*F, base + (size_t)row * rstride);
+        } else {
+            return tile ? tile[row] : prod_eval<OP, V>(*F, base + (size_t)row * rstride);
+        }
     }
 };
 
 // ---- y lines: staging through shared memory ------------------------------
-// The 32 lines of a y CTA are one contiguous block of 32*n doubles.  They
-// are copied with 16-byte coalesced accesses into a [32][n+1] tile (odd
-// stride: lane l reading row r of line l hits bank (l*(n+1)+r) mod 32, all
-// distinct), so that each thread reads its segment conflict-free.
+// The NL = kLanes*W lines of a y CTA are one contiguous block of NL*n values.
+// They are copied with 16-byte coalesced accesses into an [NL][n+1] tile of
+// the arithmetic type (odd stride: the lines of a half-warp start in distinct
+// banks), so that each thread reads its segment conflict-free.
 template <int OP, class T>
-__device__ __forceinline__ void ytile_load(double *tile, const ProdT<T> &F, size_t base, int n) {
-    const int half = kLanes * n / 2;
-    if (sizeof(T) == 8 && OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
-        if constexpr (sizeof(T) == 8) {
+__device__ __forceinline__ void ytile_load(typename Val<T>::A *tile, const ProdT<T> &F, size_t base, int n) {
+    constexpr int NL = kLanes * Val<T>::W;
+    if constexpr (sizeof(T) == 8) {
+        const int half = NL * n / 2;
+        if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
             const double2 *src = reinterpret_cast<const double2 *>(F.a + base);
             for (int q = threadIdx.x; q < half; q += blockDim.x) {
                 double2 d = __ldg(src + q);
@@ -246,60 +315,103 @@ __device__ __forceinline__ void ytile_load(double *tile, const ProdT<T> &F, size
                 tile[line * (n + 1) + row] = d.x;
                 tile[line * (n + 1) + row + 1] = d.y;
             }
+            return;
         }
     } else {
-        for (int q = threadIdx.x; q < 2 * half; q += blockDim.x) {
-            int line = q / n, row = q - line * n;
-            tile[line * (n + 1) + row] = prod_eval<OP>(F, base + q);
+        if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
+            const float4 *src = reinterpret_cast<const float4 *>(F.a + base);
+            for (int q = threadIdx.x; q < NL * n / 4; q += blockDim.x) {
+                float4 d = __ldg(src + q);
+                int e = 4 * q, line = e / n, row = e - line * n;   // n % 4 == 0: one line
+                float *t = tile + line * (n + 1) + row;
+                t[0] = d.x; t[1] = d.y; t[2] = d.z; t[3] = d.w;
+            }
+            return;
         }
+    }
+    using A = typename Val<T>::A;
+    for (int q = threadIdx.x; q < NL * n; q += blockDim.x) {
+        int line = q / n, row = q - line * n;
+        tile[line * (n + 1) + row] = prod_eval<OP, A>(F, base + q);
     }
 }
 template <class T>
-__device__ __forceinline__ void ytile_store(const double *tile, T *__restrict__ O, size_t base, int n,
+__device__ __forceinline__ void ytile_store(const typename Val<T>::A *tile, T *__restrict__ O, size_t base, int n,
                                             int add) {
-    if (sizeof(T) != 8 || (reinterpret_cast<uintptr_t>(O + base) & 15)) {
-        for (int q = threadIdx.x; q < kLanes * n; q += blockDim.x) {
-            int line = q / n, row = q - line * n;
-            double v = tile[line * (n + 1) + row];
-            O[base + q] = (T)(add ? (double)O[base + q] + v : v);
-        }
-        return;
-    }
+    constexpr int NL = kLanes * Val<T>::W;
     if constexpr (sizeof(T) == 8) {
-        double2 *dst = reinterpret_cast<double2 *>(O + base);
-        const int half = kLanes * n / 2;
-        for (int q = threadIdx.x; q < half; q += blockDim.x) {
-            int e = 2 * q, line = e / n, row = e - line * n;
-            double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
-            if (add) {
-                double2 o = dst[q];
-                d.x = o.x + d.x;
-                d.y = o.y + d.y;
+        if (!(reinterpret_cast<uintptr_t>(O + base) & 15)) {
+            double2 *dst = reinterpret_cast<double2 *>(O + base);
+            const int half = NL * n / 2;
+            for (int q = threadIdx.x; q < half; q += blockDim.x) {
+                int e = 2 * q, line = e / n, row = e - line * n;
+                double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
+                if (add) {
+                    double2 o = dst[q];
+                    d.x = o.x + d.x;
+                    d.y = o.y + d.y;
+                }
+                dst[q] = d;
             }
-            dst[q] = d;
+            return;
+        }
+    } else {
+        if (!(reinterpret_cast<uintptr_t>(O + base) & 15)) {
+            float4 *dst = reinterpret_cast<float4 *>(O + base);
+            for (int q = threadIdx.x; q < NL * n / 4; q += blockDim.x) {
+                int e = 4 * q, line = e / n, row = e - line * n;
+                const float *t = tile + line * (n + 1) + row;
+                float4 d = make_float4(t[0], t[1], t[2], t[3]);
+                if (add) {
+                    float4 o = dst[q];
+                    d.x = o.x + d.x; d.y = o.y + d.y; d.z = o.z + d.z; d.w = o.w + d.w;
+                }
+                dst[q] = d;
+            }
+            return;
         }
     }
+    for (int q = threadIdx.x; q < NL * n; q += blockDim.x) {
+        int line = q / n, row = q - line * n;
+        auto v = tile[line * (n + 1) + row];
+        O[base + q] = (T)(add ? (T)O[base + q] + v : v);
+    }
 }
-template <int S, int H>
-__device__ __forceinline__ void ytile_rows(double (&v)[S + 2 * H], const double *tile, int lane, int a, int n,
-                                           int cyc) {
-    const double *p = tile + lane * (n + 1);
+// rows of the thread's line(s) from the tile; W = 2: lines 2*lane and 2*lane+1
+template <int S, int H, class V, class A>
+__device__ __forceinline__ void ytile_rows(V (&v)[S + 2 * H], const A *tile, int lane, int a, int n, int cyc) {
+    if constexpr (sizeof(V) == 2 * sizeof(A)) {
+        const A *p = tile + 2 * lane * (n + 1);
 #pragma unroll
-    for (int q = 0; q < S + 2 * H; q++) v[q] = p[halo_row(a - H + q, n, cyc)];
+        for (int q = 0; q < S + 2 * H; q++) {
+            int row = halo_row(a - H + q, n, cyc);
+            v[q] = V(p[row], p[row + n + 1]);
+        }
+    } else {
+        const A *p = tile + lane * (n + 1);
+#pragma unroll
+        for (int q = 0; q < S + 2 * H; q++) v[q] = p[halo_row(a - H + q, n, cyc)];
+    }
 }
-template <int S, int N>
-__device__ __forceinline__ void ytile_put(double *tile, const double (&r)[N], int lane, int a, int n) {
-    double *p = tile + lane * (n + 1) + a;
+template <int S, int N, class V, class A>
+__device__ __forceinline__ void ytile_put(A *tile, const V (&r)[N], int lane, int a, int n) {
+    if constexpr (sizeof(V) == 2 * sizeof(A)) {
+        A *p = tile + 2 * lane * (n + 1) + a;
 #pragma unroll
-    for (int t = 0; t < S; t++) p[t] = r[t];
+        for (int t = 0; t < S; t++) { p[t] = r[t].x; p[t + n + 1] = r[t].y; }
+    } else {
+        A *p = tile + lane * (n + 1) + a;
+#pragma unroll
+        for (int t = 0; t < S; t++) p[t] = r[t];
+    }
 }
 
 // DFDX_sym/_asym RHS, src/derivCDopt6_sym_tri.f:458-514,
 // src/derivCDopt6_asym_tri.f:461-516  (H = 2).  Periodic DFDX,
 // src/derivCDopt6_periodic.f:205-248: the interior formula on every row with
 // wrapped halos (its f(i+-3) weight c1 is zero for the FDL3DI set).
-template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
+template <int S, int H, class RD, class V>
+__device__ __forceinline__ void rhs_d1(V (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
                                        const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
@@ -325,8 +437,8 @@ __device__ __forceinline__ void rhs_d1(double (&v)[S + 2 * H], int a, int n, int
 // src/derivCDopt6_asym_tri.f:588-643  (H = 2).  Periodic D2FDX2,
 // src/derivCDopt6_periodic.f:316-370, with zero f(i+-3) weight and centre
 // weight 2(a2+b2).
-template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_d2(double (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
+template <int S, int H, class RD, class V>
+__device__ __forceinline__ void rhs_d2(V (&v)[S + 2 * H], int a, int n, int asym, int cyc, double fac,
                                        const Consts &K, const RD &F) {
 #pragma unroll
     for (int t = 0; t < S; t++) {
@@ -401,8 +513,8 @@ __device__ __forceinline__ void rhs_filter(double (&v)[S + 2 * H], int a, int n,
 // Gaussian_Filter_X, src/filters_sym.f:1119-1212: explicit, symmetric low end,
 // last four points copied  (H = 4).  Periodic family,
 // src/filters_periodic.f:601-675: interior formula, wrapped halos.
-template <int S, int H, class RD>
-__device__ __forceinline__ void rhs_gauss(double (&v)[S + 2 * H], int a, int n, int cyc, const Consts &K,
+template <int S, int H, class RD, class V>
+__device__ __forceinline__ void rhs_gauss(V (&v)[S + 2 * H], int a, int n, int cyc, const Consts &K,
                                           const RD &F) {
     const double *g = K.ga;
 #pragma unroll

@@ -11,8 +11,9 @@
 
 namespace st {
 
-// T: element type of the fields read and written (double, or float in the
-// FP32 mode); the stencils and solves always run in double.
+// T: element type of the fields read and written and of the arithmetic:
+// double, or float in the FP32 mode, whose kernels give each thread two
+// neighbouring lines (value type F2, 32 lines per CTA).
 template <class T>
 struct LineArgsT {
     ProdT<T> F;
@@ -22,7 +23,7 @@ struct LineArgsT {
     double fac1, fac2;
     int asym, iadd;
     int cyc;            // periodic family: wrapped halos, corner correction (selects the CYC kernels)
-    TriTab t1, t2;
+    TriTabT<T> t1, t2;
     PenTab p;
     Consts K;
 };
@@ -33,27 +34,32 @@ using LineArgsF = LineArgsT<float>;
 // coalesced row accesses) and for y lines (YT = true: staged through a
 // shared [32][n+1] tile).
 #define LINE_PROLOGUE                                                                  \
-    __shared__ CarryBuf cb;                                                            \
-    extern __shared__ double tile[];                                                   \
+    using V = typename Val<T>::V;                                                      \
+    using A = typename Val<T>::A;                                                      \
+    constexpr int W = Val<T>::W;                                                       \
+    __shared__ CarryBufT<V> cb;                                                        \
+    extern __shared__ __align__(16) unsigned char smem_raw[];                          \
+    A *tile = reinterpret_cast<A *>(smem_raw);                                         \
     const int lane = threadIdx.x & (kLanes - 1), s = threadIdx.x / kLanes, n = a.geo.n, row0 = s * S; \
-    const ColMap m = a.geo.map(blockIdx.x);                                            \
-    const RowReader<OP, T> rd = YT ? RowReader<OP, T>{tile + lane * (n + 1), nullptr, 0, 0}  \
-                                   : RowReader<OP, T>{nullptr, &a.F, m.base + (size_t)lane * m.lstride, m.rstride};
+    const ColMap m = a.geo.template map<W>(blockIdx.x);                                \
+    const RowReader<OP, T, V> rd = YT ? RowReader<OP, T, V>{tile + W * lane * (n + 1), nullptr, 0, 0, n + 1} \
+                                      : RowReader<OP, T, V>{nullptr, &a.F, m.base + (size_t)lane * W * m.lstride, \
+                                                            m.rstride, 0};
 
-template <int S, int H, bool YT, int OP, class T>
-__device__ __forceinline__ void get_rows(double (&v)[S + 2 * H], const double *tile, const ProdT<T> &F,
+template <int S, int H, bool YT, int OP, class T, class V, class A>
+__device__ __forceinline__ void get_rows(V (&v)[S + 2 * H], const A *tile, const ProdT<T> &F,
                                          const ColMap &m, int lane, int a, int n, int cyc) {
     if (YT) ytile_rows<S, H>(v, tile, lane, a, n, cyc);
     else load_rows<S, H, OP>(v, F, m, lane, a, n, cyc);
 }
-template <int S, bool YT, int N, class T>
-__device__ __forceinline__ void put_rows(const double (&v)[N], double *tile, T *O, const ColMap &m,
+template <int S, bool YT, int N, class T, class V, class A>
+__device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const ColMap &m,
                                          int lane, int a, int n, int add) {
     if (YT) {
         __syncthreads();                 // every thread has finished reading the tile
         ytile_put<S>(tile, v, lane, a, n);
         __syncthreads();
-        ytile_store(tile, O, m.base, n, add);
+        ytile_store<T>(tile, O, m.base, n, add);
     } else {
         store_rows<S>(v, O, m, lane, a, add);
     }
@@ -64,7 +70,7 @@ template <int S, bool YT, int OP, bool CYC, class T>
 __global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
-    double v[S + 4];
+    V v[S + 4];
     get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
     rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
@@ -81,7 +87,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
     LINE_PROLOGUE
     {
         if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
-        double v[S + 4];
+        V v[S + 4];
         get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
         rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
@@ -91,7 +97,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
     if (a.iadd) {
         __syncthreads();   // carry buffers and tile are reused
         if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
-        double v[S + 4];
+        V v[S + 4];
         get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
         rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
         tri_solve<S>(v, a.t1, s, a.P, lane, cb);
@@ -125,7 +131,7 @@ __global__ void __launch_bounds__(512, 2) k_gauss(LineArgsT<T> a) {
     LINE_PROLOGUE
     (void)cb;
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
-    double v[S + 8];
+    V v[S + 8];
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
     rhs_gauss<S, 4>(v, row0, n, CYC, a.K, rd);
     put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
@@ -147,8 +153,9 @@ static void set_smem(size_t bytes) {
 template <int S, bool YT, bool CYC, class T>
 static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t st) {
     const size_t nlines = c->dm.n3 / (size_t)a.geo.n;
-    dim3 grid((unsigned)(nlines / kLanes)), block(kLanes * a.P);
-    const size_t smem = YT ? (size_t)kLanes * (a.geo.n + 1) * sizeof(double) : 0;
+    constexpr int NL = kLanes * Val<T>::W;
+    dim3 grid((unsigned)(nlines / NL)), block(kLanes * a.P);
+    const size_t smem = YT ? (size_t)NL * (a.geo.n + 1) * sizeof(T) : 0;
     // algorithmic bytes: every input and output field touched once
     const double n3 = (double)c->dm.n3;
     // inputs: 1 field, or every field a producer expression reads

@@ -215,7 +215,7 @@ struct PenHost {
 // size of the solution, so the device loops stop at the farthest segment
 // whose weight (max norm of the 2x2 block for pentadiagonal carries) is at
 // least that large.
-static int carry_span(const std::vector<double> &w, int P, int blk, bool fwd) {
+static int carry_span(const std::vector<double> &w, int P, int blk, bool fwd, double floor = 1e-20) {
     int span = 0;
     for (int s = 0; s < P; s++)
         for (int sp = 0; sp < P; sp++) {
@@ -223,7 +223,7 @@ static int carry_span(const std::vector<double> &w, int P, int blk, bool fwd) {
             if (dist <= 0) continue;
             double m = 0.0;
             for (int q = 0; q < blk; q++) m = std::fmax(m, std::fabs(w[((size_t)sp * P + s) * blk + q]));
-            if (m >= 1e-20 && dist > span) span = dist;
+            if (m >= floor && dist > span) span = dist;
         }
     return span;
 }
@@ -356,6 +356,35 @@ static const double *upload(st_ctx *c, const std::vector<double> &v, int *err) {
         *err = 1;
     return (const double *)p;
 }
+static const float *upload_f(st_ctx *c, const std::vector<double> &v, int *err) {
+    std::vector<float> f(v.begin(), v.end());
+    void *p = nullptr;
+    if (cudaMalloc(&p, f.size() * sizeof(float)) != cudaSuccess) { *err = 1; return nullptr; }
+    c->table_allocs.push_back(p);
+    c->table_bytes += f.size() * sizeof(float);
+    if (cudaMemcpy(p, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) *err = 1;
+    return (const float *)p;
+}
+
+// The FP32 mode's tridiagonal factors: the double tables rounded to float.
+// Carry weights below 1e-12 cannot change a float result of the size of the
+// solution (float epsilon 6e-8 times the few segment end values they scale).
+static void upload_tri(st_ctx *c, st::TriTab &t, st::TriTabT<float> &tf, const TriHost &h,
+                       const std::vector<double> *K, int P, int *err) {
+    t.l = upload(c, h.l, err); t.g = upload(c, h.g, err); t.up = upload(c, h.up, err);
+    t.id = upload(c, h.id, err); t.h = upload(c, h.h, err);
+    t.wf = upload(c, h.wf, err); t.wb = upload(c, h.wb, err);
+    t.kf = h.kf; t.kb = h.kb;
+    t.cyc = K ? upload(c, *K, err) : nullptr;
+    tf = st::TriTabT<float>{};
+    if (c->p.precision != ST_PRECISION_FP32) return;
+    tf.l = upload_f(c, h.l, err); tf.g = upload_f(c, h.g, err); tf.up = upload_f(c, h.up, err);
+    tf.id = upload_f(c, h.id, err); tf.h = upload_f(c, h.h, err);
+    tf.wf = upload_f(c, h.wf, err); tf.wb = upload_f(c, h.wb, err);
+    tf.kf = carry_span(h.wf, P, 1, true, 1e-12);
+    tf.kb = carry_span(h.wb, P, 1, false, 1e-12);
+    tf.cyc = K ? upload_f(c, *K, err) : nullptr;
+}
 
 // Periodic family: every derivative and filter kind of a direction gets the
 // cyclic tables (the periodic routines have no sym/asym variants).  The FDL3DI
@@ -373,12 +402,8 @@ static int build_tables_periodic(st_ctx *c) {
             TriHost h = tri_tables(M[1], M[2], M[3], n, c->seg[d]);
             std::vector<double> K = cyclic_correction(n, 0.0, al, 2);
             for (int asym = 0; asym < 2; asym++) {
-                TriTab &t = c->tri[d][(order - 1) * 2 + asym];
-                t.l = upload(c, h.l, &err); t.g = upload(c, h.g, &err); t.up = upload(c, h.up, &err);
-                t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
-                t.wf = upload(c, h.wf, &err); t.wb = upload(c, h.wb, &err);
-                t.kf = h.kf; t.kb = h.kb;
-                t.cyc = upload(c, K, &err);
+                const int kind = (order - 1) * 2 + asym;
+                upload_tri(c, c->tri[d][kind], c->trif[d][kind], h, &K, n / c->seg[d], &err);
             }
         }
         std::vector<double> M[5];
@@ -409,12 +434,7 @@ int build_tables(st_ctx *c) {
             std::vector<double> a, b, cc;
             deriv_lhs(n, kind < 2 ? 1 : 2, kind & 1, a, b, cc);
             TriHost h = tri_tables(a, b, cc, n, c->seg[d]);
-            TriTab &t = c->tri[d][kind];
-            t.l = upload(c, h.l, &err); t.g = upload(c, h.g, &err); t.up = upload(c, h.up, &err);
-            t.id = upload(c, h.id, &err); t.h = upload(c, h.h, &err);
-            t.wf = upload(c, h.wf, &err); t.wb = upload(c, h.wb, &err);
-            t.kf = h.kf; t.kb = h.kb;
-            t.cyc = nullptr;
+            upload_tri(c, c->tri[d][kind], c->trif[d][kind], h, nullptr, n / c->seg[d], &err);
         }
         for (int kind = 0; kind < 2; kind++) {
             std::vector<double> M[5];

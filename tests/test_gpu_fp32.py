@@ -104,8 +104,8 @@ def test_steps_vs_oracle(oracle_mod):
 def test_rhs_operator_vs_fp64():
     """One RHS + Hyper_RHS evaluation through the per-operator entry points."""
     from shock_turbulence_b200 import Solver
-    p64 = default_params(48, re=100.0)
-    p32 = default_params(48, re=100.0, precision=PRECISION_FP32)
+    p64 = default_params(32, 64, 32, re=100.0)
+    p32 = default_params(32, 64, 32, re=100.0, precision=PRECISION_FP32)
     Q, Y = blast(p64, seed=9)
     out = []
     for p in (p64, p32):
@@ -141,3 +141,13 @@ def test_bad_precision_rejected():
     from shock_turbulence_b200 import Solver, StError
     with pytest.raises(StError):
         Solver(default_params(32, precision=7))
+
+
+def test_fp32_needs_32_lines():
+    """The FP32 kernels give a CTA 32 lines (two per thread): ny must be a
+    multiple of 32; 48 is rejected as unsupported, not run on another path."""
+    from shock_turbulence_b200 import Solver, StError
+    with pytest.raises(StError) as e:
+        Solver(default_params(32, 48, 32, precision=PRECISION_FP32))
+    assert e.value.status == -4
+    Solver(default_params(32, 48, 32)).close()    # the FP64 path takes it
