@@ -780,6 +780,10 @@ static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrh
             return 0.0;
         };
         double s = sig(i + 1, sx, lx) + sig(j + 1, sy, ly) + sig(k + 1, sz, lz);
+        // outside the sponge shell the forcing is 0*(...): the right-hand
+        // sides keep their values (up to the sign of a zero), so those cells
+        // are not touched
+        if (s == 0.0) return;
         double Qref[5] = {0.0, 0.0, 0.0, rho_ref, E_ref};
         for (int l = 0; l < 5; l++) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] - s * (Q[l * n3 + p] - Qref[l]);
         Yrhs[p] = Yrhs[p] - s * (Q[3 * n3 + p] * Y[p] - Q[3 * n3 + p] * Y_ref);
@@ -863,6 +867,26 @@ int dev_fix_pressure(st_ctx *c, double *Q) {
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
         if (P < 0.0) P = base;
         Q5[p] = (1.0 / fac1) * P + 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]);
+    });
+    return ST_OK;
+}
+
+// Fix_Pressure of the FP32 mode's stages: as above, and the float copy of
+// the state for the next stage
+static int fix_pressure_copy(st_ctx *c, double *Q, float *qs) {
+    const size_t n3 = c->dm.n3;
+    double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
+    const double *g = c->gamma_eff;
+    const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
+    PFOR(c, n3, {
+        double fac1 = g[p] - 1.0;
+        double Vs = 1.0 / Q4[p];
+        double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
+        if (P < 0.0) P = base;
+        double q5 = (1.0 / fac1) * P + 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]);
+        Q5[p] = q5;
+        qs[p] = (float)Q1[p]; qs[n3 + p] = (float)Q2[p]; qs[2 * n3 + p] = (float)Q3[p];
+        qs[3 * n3 + p] = (float)Q4[p]; qs[4 * n3 + p] = (float)q5;
     });
     return ST_OK;
 }
@@ -1075,6 +1099,8 @@ template <> struct StateCopy<float> {
     const float *q(const double *) const { return qs; }
     const float *y(const double *) const { return ys; }
 };
+// (the Compute_Y/Fix_Pressure kernel at the end of a stage writes the copy
+// for the next stage; a call's first stage makes it here)
 template <class R>
 static int refresh(st_ctx *c, StateCopy<R> &sc, const double *Q, const double *Y, bool with_y) {
     if constexpr (!is_fp64<R>()) {
@@ -1104,6 +1130,7 @@ static int lddrk4_sf(st_ctx *c) {
     Scratch Qfs(c, 5);
     double *Qf = Qfs;
     StateCopy<R> sc(c);
+    bool fresh = false;   // the float state copy holds the current state
     const double *dtp = c->dscal + 6;
     double *timep = c->dscal + 7;
     for (int loop = 0; loop < 2; loop++) {
@@ -1116,7 +1143,7 @@ static int lddrk4_sf(st_ctx *c) {
             const bool first = K == 0;
             double *Q = c->Q, *QW = c->QW;
             R *dQ = Store<R>::dQ(c);
-            ST_TRY(refresh<R>(c, sc, Q, c->Y, false));
+            if (!fresh) ST_TRY(refresh<R>(c, sc, Q, c->Y, false));
             ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, c->Y));
             ST_TRY(hyper_rhs_t<R>(c, Q, dQ, c->Y, sc.y(c->Y)));
             PFOR(c, n3, {
@@ -1133,7 +1160,12 @@ static int lddrk4_sf(st_ctx *c) {
                 ST_TRY(dev_filter(c, 1, 0, Qf + l * n3, Qf + l * n3));
                 ST_TRY(dev_filter(c, 2, 0, Qf + l * n3, Q + l * n3));
             }
-            ST_TRY(dev_fix_pressure(c, Q));
+            if constexpr (is_fp64<R>()) {
+                ST_TRY(dev_fix_pressure(c, Q));
+            } else {
+                ST_TRY(fix_pressure_copy(c, Q, sc.qs));
+                fresh = true;
+            }
         }
         PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
     }
@@ -1150,6 +1182,7 @@ static int lddrk4_mf(st_ctx *c) {
     Scratch rYs(c), Qfs(c, 5);
     double *rY = rYs, *Qf = Qfs;
     StateCopy<R> sc(c);
+    bool fresh = false;   // the float state copy holds the current state
     const double *dtp = c->dscal + 6;
     double *timep = c->dscal + 7;
     for (int loop = 0; loop < 2; loop++) {
@@ -1159,7 +1192,7 @@ static int lddrk4_mf(st_ctx *c) {
             const bool first = K == 0;
             double *Q = c->Q, *QW = c->QW, *Y = c->Y, *rYW = c->rYW;
             R *dQ = Store<R>::dQ(c), *drYi = Store<R>::drYi(c);
-            ST_TRY(refresh<R>(c, sc, Q, Y, true));
+            if (!fresh) ST_TRY(refresh<R>(c, sc, Q, Y, true));
             ST_TRY(dev_compute_gamma(c, Y));
             ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, Y));
             ST_TRY(hyper_rhs_t<R>(c, Q, dQ, Y, sc.y(Y)));
@@ -1188,16 +1221,26 @@ static int lddrk4_mf(st_ctx *c) {
             ST_TRY(dev_filter(c, 0, 0, rY, rY));
             ST_TRY(dev_filter(c, 1, 0, rY, rY));
             ST_TRY(dev_filter(c, 2, 0, rY, rY));
-            // Compute_Y + Fix_Pressure (pproc/pproc_mf.f:190-233)
+            // Compute_Y + Fix_Pressure (pproc/pproc_mf.f:190-233); the FP32
+            // mode also writes the next stage's float copy of the state
             const double *g = c->gamma_eff;
+            float *qs = nullptr, *ys = nullptr;
+            if constexpr (!is_fp64<R>()) { qs = sc.qs; ys = sc.ys; fresh = true; }
             PFOR(c, n3, {
                 double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p];
-                Y[p] = rY[p] / q4;
+                double y = rY[p] / q4;
+                Y[p] = y;
                 double fac1 = g[p] - 1.0;
                 double Vs = 1.0 / q4;
                 double P = fac1 * (Q[4 * n3 + p] - 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3));
                 if (P < 0.0) P = 0.71429;
-                Q[4 * n3 + p] = (1.0 / fac1) * P + 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3);
+                double q5 = (1.0 / fac1) * P + 5.0e-1 * Vs * (q1 * q1 + q2 * q2 + q3 * q3);
+                Q[4 * n3 + p] = q5;
+                if (qs) {
+                    qs[p] = (float)q1; qs[n3 + p] = (float)q2; qs[2 * n3 + p] = (float)q3;
+                    qs[3 * n3 + p] = (float)q4; qs[4 * n3 + p] = (float)q5;
+                    ys[p] = (float)y;
+                }
             });
         }
         PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
