@@ -179,19 +179,28 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     R *Gxz = G[G_DUX_DZ], *Gyz = G[G_DUY_DZ], *Gzz = G[G_DUZ_DZ];
     R *GTx = G[G_DTDX], *GTy = G[G_DTDY], *GTz = G[G_DTDZ];
     ScratchT<R> sQcx(c, 5), sQcy(c, 5), sQcz(c, 5), sQv(c, 5);
-    R *Qcx = sQcx, *Qcy = sQcy, *Qcz = sQcz, *Qv = sQv;
-    ScratchNT<R> s(c, 17);
-    R *Vs = s[0], *P = s[1], *T = s[2], *u = s[3], *v = s[4], *w = s[5], *mu = s[6], *dmu = s[7];
-    R *Flux = s[8], *FF = s[9], *dF = s[10], *dFz = s[11], *U4 = s[12], *U5 = s[13], *Tdy = s[14];
-    R *Tdz = s[15], *T2 = s[16];
+    R *Qcx = sQcx, *Qcy = sQcy, *Qcz = sQcz, *Qv = sQv;   // Qv(:,:,:,4) is never formed
+    ScratchNT<R> s(c, 8);
+    R *P = s[0], *T = s[1], *u = s[2], *v = s[3], *w = s[4], *mu = s[5], *dmu = s[6], *FF = s[7];
+    // second derivatives and derivatives of /GRAD/ consumed by the two
+    // pointwise passes below (one field each, so that all of them can be
+    // formed before the pass that uses them)
+    ScratchNT<R> dd(c, 14);
     const double *g = c->gamma_eff;
 
     // ---- RHS_x (src/rhsv_sym_mf.f:37-481)
+    // P, T, u, and (the same expressions the reference evaluates later from
+    // the same inputs) v, w, mu, dmu/dT
     PFOR(c, n3, {
-        double vs, pp, tt;
+        double vs, pp, tt, m, dm;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], vs, pp, tt);
-        Vs[p] = vs; P[p] = pp; T[p] = tt;
+        P[p] = pp; T[p] = tt;
         u[p] = Q1[p] * vs;
+        v[p] = Q2[p] * vs;
+        w[p] = Q3[p] * vs;
+        viscosity(f, (R)tt, Y[p], m, dm);
+        mu[p] = m;
+        dmu[p] = dm;
     });
     ST_TRY(dfd(c, 0, 1, pr_mul(q4r, u), Qcx + 3 * n3, 0, -1.0));
     ST_TRY(dfd(c, 0, 1, pr_addmul(q5r, P, u), Qcx + 4 * n3, 0, -1.0));
@@ -200,52 +209,46 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     ST_TRY(dfd(c, 0, 1, pr_mul(q2r, u), Qcx + n3, 0, -5.0e-1));
     ST_TRY(dfd(c, 0, 1, pr_mul(q3r, u), Qcx + 2 * n3, 0, -5.0e-1));
     ST_TRY(dfd(c, 0, 1, q1r, FF, 0, 1.0));
-    PFOR(c, n3, {
-        double m, dm;
-        v[p] = Q2[p] * Vs[p];
-        w[p] = Q3[p] * Vs[p];
-        viscosity(f, T[p], Y[p], m, dm);
-        mu[p] = m;
-        dmu[p] = dm;
-        double fac2 = -5.0e-1 * FF[p];
-        Qcx[p] = Qcx[p] + fac2 * u[p];
-        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * v[p];
-        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * w[p];
-    });
+    R *dTx = dd[0], *duxx = dd[1], *dvxx = dd[2], *dwxx = dd[3];
     if (visc) {
-        const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
-        ST_TRY(d2fd2(c, 0, 0, T, GTx, dF, 1));
-        PFOR(c, n3, { Qv[4 * n3 + p] = Pri * (mu[p] * dF[p] + dmu[p] * GTx[p] * GTx[p]); });
-        ST_TRY(d2fd2(c, 0, 1, u, Gxx, dF, 1));
-        PFOR(c, n3, {
-            double fac2 = fac1 * mu[p] * dF[p];
-            Qv[p] = fac2;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac2;
-        });
-        ST_TRY(d2fd2(c, 0, 0, v, Gyx, dF, 1));
-        PFOR(c, n3, {
-            double fac2 = mu[p] * dF[p];
-            Qv[n3 + p] = fac2;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + v[p] * fac2;
-        });
-        ST_TRY(d2fd2(c, 0, 0, w, Gzx, dF, 1));
-        PFOR(c, n3, {
-            double fac2 = mu[p] * dF[p];
-            Qv[2 * n3 + p] = fac2;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + w[p] * fac2;
-        });
+        ST_TRY(d2fd2(c, 0, 0, (const R *)T, GTx, dTx, 1));
+        ST_TRY(d2fd2(c, 0, 1, (const R *)u, Gxx, duxx, 1));
+        ST_TRY(d2fd2(c, 0, 0, (const R *)v, Gyx, dvxx, 1));
+        ST_TRY(d2fd2(c, 0, 0, (const R *)w, Gzx, dwxx, 1));
     } else {
-        ST_TRY(dfd(c, 0, 0, T, GTx, 0, 1.0));
-        ST_TRY(dfd(c, 0, 1, u, Gxx, 0, 1.0));
-        ST_TRY(dfd(c, 0, 0, v, Gyx, 0, 1.0));
-        ST_TRY(dfd(c, 0, 0, w, Gzx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, (const R *)T, GTx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 1, (const R *)u, Gxx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, (const R *)v, Gyx, 0, 1.0));
+        ST_TRY(dfd(c, 0, 0, (const R *)w, Gzx, 0, 1.0));
     }
-    PFOR(c, n3, {
-        double fac2 = -5.0e-1 * Q4[p] * u[p];
-        Qcx[p] = Qcx[p] + fac2 * Gxx[p];
-        Qcx[n3 + p] = Qcx[n3 + p] + fac2 * Gyx[p];
-        Qcx[2 * n3 + p] = Qcx[2 * n3 + p] + fac2 * Gzx[p];
-    });
+    // convective terms -0.5*d(rho u)/dx*(u,v,w) and -0.5*rho*u*d(u,v,w)/dx,
+    // and the x part of Qvisc, in the reference's order of accumulation
+    {
+        const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
+        PFOR(c, n3, {
+            double fac2 = -5.0e-1 * FF[p];
+            double c1 = Qcx[p] + fac2 * u[p];
+            double c2 = Qcx[n3 + p] + fac2 * v[p];
+            double c3 = Qcx[2 * n3 + p] + fac2 * w[p];
+            if (visc) {
+                double q5 = Pri * (mu[p] * dTx[p] + dmu[p] * GTx[p] * GTx[p]);
+                double fx = fac1 * mu[p] * duxx[p];
+                q5 = q5 + u[p] * fx;
+                double fy = mu[p] * dvxx[p];
+                q5 = q5 + v[p] * fy;
+                double fz = mu[p] * dwxx[p];
+                q5 = q5 + w[p] * fz;
+                Qv[p] = fx;
+                Qv[n3 + p] = fy;
+                Qv[2 * n3 + p] = fz;
+                Qv[4 * n3 + p] = q5;
+            }
+            fac2 = -5.0e-1 * Q4[p] * u[p];
+            Qcx[p] = c1 + fac2 * Gxx[p];
+            Qcx[n3 + p] = c2 + fac2 * Gyx[p];
+            Qcx[2 * n3 + p] = c3 + fac2 * Gzx[p];
+        });
+    }
 
     // ---- RHS_yz (src/rhsv_sym_mf.f:492-1428)
     // d(rho v)/dy and d(rho w)/dz with iadd=0, cadd=-1: Qconv(4) = 0 - d(.) exactly
@@ -261,126 +264,123 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     ST_TRY(dfd(c, 2, 0, pr_mul(q3r, w), Qcz + 2 * n3, 0, -5.0e-1));
     ST_TRY(dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
     ST_TRY(dfd(c, 2, 1, pr_addmul(q5r, P, w), Qcz + 4 * n3, 0, -1.0));
-    // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
-    const R *dFy = Qcy + 3 * n3, *dFzz = Qcz + 3 * n3;
-    PFOR(c, n3, {
-        double fac2 = -5.0e-1 * (-dFy[p]);
-        Qcy[p] = Qcy[p] + fac2 * u[p];
-        Qcy[n3 + p] = Qcy[n3 + p] + fac2 * v[p];
-        Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * w[p];
-        fac2 = -5.0e-1 * (-dFzz[p]);
-        Qcz[p] = Qcz[p] + fac2 * u[p];
-        Qcz[n3 + p] = Qcz[n3 + p] + fac2 * v[p];
-        Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * w[p];
-    });
+    R *d2Ty = dd[0], *d2Tz = dd[1], *d2uy = dd[2], *d2vy = dd[3], *d2wy = dd[4], *d2wz = dd[5];
+    R *dGzz_y = dd[6], *d2uz = dd[7], *d2vz = dd[8], *dGxx_y = dd[9], *dGxx_z = dd[10], *dGyx_y = dd[11];
+    R *dGzx_z = dd[12], *dGyz_y = dd[13];
     if (visc) {
-        const double Pri = f.Pr_inv;
-        ST_TRY(d2fd2(c, 1, 0, T, GTy, U5, 1));
-        ST_TRY(d2fd2(c, 2, 0, T, GTz, Flux, 1));
-        PFOR(c, n3, {
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + Pri * (mu[p] * (U5[p] + Flux[p]) +
-                                                    dmu[p] * (GTy[p] * GTy[p] + GTz[p] * GTz[p]));
-            U4[p] = dmu[p] * GTx[p];
-            Tdy[p] = dmu[p] * GTy[p];
-            Tdz[p] = dmu[p] * GTz[p];
-        });
-        ST_TRY(d2fd2(c, 1, 0, u, Gxy, U5, 1));
-        ST_TRY(d2fd2(c, 1, 1, v, Gyy, dF, 1));
-        ST_TRY(d2fd2(c, 1, 0, w, Gzy, T2, 1));
+        ST_TRY(d2fd2(c, 1, 0, (const R *)T, GTy, d2Ty, 1));
+        ST_TRY(d2fd2(c, 2, 0, (const R *)T, GTz, d2Tz, 1));
+        ST_TRY(d2fd2(c, 1, 0, (const R *)u, Gxy, d2uy, 1));
+        ST_TRY(d2fd2(c, 1, 1, (const R *)v, Gyy, d2vy, 1));
+        ST_TRY(d2fd2(c, 1, 0, (const R *)w, Gzy, d2wy, 1));
     } else {
-        ST_TRY(dfd(c, 1, 0, T, GTy, 0, 1.0));
-        ST_TRY(dfd(c, 2, 0, T, GTz, 0, 1.0));
-        ST_TRY(dfd(c, 1, 0, u, Gxy, 0, 1.0));
-        ST_TRY(dfd(c, 1, 1, v, Gyy, 0, 1.0));
-        ST_TRY(dfd(c, 1, 0, w, Gzy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, (const R *)T, GTy, 0, 1.0));
+        ST_TRY(dfd(c, 2, 0, (const R *)T, GTz, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, (const R *)u, Gxy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, (const R *)v, Gyy, 0, 1.0));
+        ST_TRY(dfd(c, 1, 0, (const R *)w, Gzy, 0, 1.0));
     }
-    ST_TRY(dfd(c, 2, 0, u, Gxz, 0, 1.0));
-    ST_TRY(dfd(c, 2, 0, v, Gyz, 0, 1.0));
-    ST_TRY(dfd(c, 2, 1, w, Gzz, 0, 1.0));
-    {
-        const double fac1 = f.bulk + 4.0 / 3.0;
-        PFOR(c, n3, {
-            double fac2 = -5.0e-1 * Q4[p] * v[p];
-            Qcy[p] = Qcy[p] + fac2 * Gxy[p];
-            Qcy[n3 + p] = Qcy[n3 + p] + fac2 * Gyy[p];
-            Qcy[2 * n3 + p] = Qcy[2 * n3 + p] + fac2 * Gzy[p];
-            fac2 = -5.0e-1 * Q4[p] * w[p];
-            Qcz[p] = Qcz[p] + fac2 * Gxz[p];
-            Qcz[n3 + p] = Qcz[n3 + p] + fac2 * Gyz[p];
-            Qcz[2 * n3 + p] = Qcz[2 * n3 + p] + fac2 * Gzz[p];
-            if (visc) {
-                double fac_X = mu[p] * U5[p];
-                double fac_Y = fac1 * mu[p] * dF[p];
-                double fac_Z = mu[p] * T2[p];
-                Qv[p] = Qv[p] + fac_X;
-                Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-                Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-                Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z;
-            }
-        });
-    }
+    ST_TRY(dfd(c, 2, 0, (const R *)u, Gxz, 0, 1.0));
+    ST_TRY(dfd(c, 2, 0, (const R *)v, Gyz, 0, 1.0));
+    ST_TRY(dfd(c, 2, 1, (const R *)w, Gzz, 0, 1.0));
     if (visc) {
-        const double fac1 = f.bulk - 2.0 / 3.0, fac2 = f.bulk + 4.0 / 3.0, fac3 = f.bulk + 1.0 / 3.0;
-        ST_TRY(d2fd2(c, 2, 1, w, nullptr, T2, 0));
-        ST_TRY(dfd(c, 1, 0, Gzz, U5, 0, 1.0));
-        PFOR(c, n3, {
-            double tmp1 = Gxx[p];
-            double dil = tmp1 + Gyy[p] + Gzz[p];
-            double fac_X = U4[p] * (2.0 * tmp1 + fac1 * dil);
-            double fac_Y = Tdy[p] * (2.0 * Gyy[p] + fac1 * dil) + fac3 * mu[p] * U5[p];
-            double fac_Z = Tdz[p] * (2.0 * Gzz[p] + fac1 * dil) + fac2 * mu[p] * T2[p];
-            Qv[p] = Qv[p] + fac_X;
-            Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-            Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
-                             mu[p] * (2.0 * (tmp1 * tmp1 + Gyy[p] * Gyy[p] + Gzz[p] * Gzz[p]) + fac1 * dil * dil);
-        });
-        ST_TRY(d2fd2(c, 2, 0, u, nullptr, dF, 0));
-        ST_TRY(d2fd2(c, 2, 0, v, nullptr, U5, 0));
-        PFOR(c, n3, {
-            double tmp1 = Gyx[p] + Gxy[p];
-            double tmp2 = Gzx[p] + Gxz[p];
-            double tmp3 = Gzy[p] + Gyz[p];
-            double fac_X = Tdy[p] * tmp1 + Tdz[p] * tmp2 + mu[p] * dF[p];
-            double fac_Y = U4[p] * tmp1 + Tdz[p] * tmp3 + mu[p] * U5[p];
-            double fac_Z = U4[p] * tmp2 + Tdy[p] * tmp3;
-            Qv[p] = Qv[p] + fac_X;
-            Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-            Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-            Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z +
-                             mu[p] * (tmp1 * tmp1 + tmp2 * tmp2 + tmp3 * tmp3);
-        });
-        ST_TRY(dfd(c, 1, 0, Gxx, U4, 0, 1.0));
-        ST_TRY(dfd(c, 2, 0, Gxx, U5, 0, 1.0));
-        ST_TRY(dfd(c, 1, 1, Gyx, Tdy, 0, 1.0));
-        ST_TRY(dfd(c, 2, 1, Gzx, Tdz, 0, 1.0));
-        ST_TRY(dfd(c, 1, 1, Gyz, T2, 0, 1.0));
+        ST_TRY(d2fd2(c, 2, 1, (const R *)w, (R *)nullptr, d2wz, 0));
+        ST_TRY(dfd(c, 1, 0, (const R *)Gzz, dGzz_y, 0, 1.0));
+        ST_TRY(d2fd2(c, 2, 0, (const R *)u, (R *)nullptr, d2uz, 0));
+        ST_TRY(d2fd2(c, 2, 0, (const R *)v, (R *)nullptr, d2vz, 0));
+        ST_TRY(dfd(c, 1, 0, (const R *)Gxx, dGxx_y, 0, 1.0));
+        ST_TRY(dfd(c, 2, 0, (const R *)Gxx, dGxx_z, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, (const R *)Gyx, dGyx_y, 0, 1.0));
+        ST_TRY(dfd(c, 2, 1, (const R *)Gzx, dGzx_z, 0, 1.0));
+        ST_TRY(dfd(c, 1, 1, (const R *)Gyz, dGyz_y, 0, 1.0));
     }
+    // One pass for the rest of RHS_yz and the sum Qrhs = Qconvx + Qconvy +
+    // Qconvz + Qvisc: each accumulator receives its terms in the order the
+    // reference adds them (src/rhsv_sym_mf.f:992-1424), in registers.
     {
-        const double fac3 = f.bulk + 1.0 / 3.0;
+        const double Pri = f.Pr_inv;
+        const double fb43 = f.bulk + 4.0 / 3.0, fb23 = f.bulk - 2.0 / 3.0, fb13 = f.bulk + 1.0 / 3.0;
         const bool fp64 = is_fp64<R>();
         PFOR(c, n3, {
+            const double uu = u[p], vv = v[p], ww = w[p], q4 = Q4[p];
+            // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
+            double fac2 = -5.0e-1 * (-(double)Qcy[3 * n3 + p]);
+            double cy1 = Qcy[p] + fac2 * uu, cy2 = Qcy[n3 + p] + fac2 * vv, cy3 = Qcy[2 * n3 + p] + fac2 * ww;
+            fac2 = -5.0e-1 * (-(double)Qcz[3 * n3 + p]);
+            double cz1 = Qcz[p] + fac2 * uu, cz2 = Qcz[n3 + p] + fac2 * vv, cz3 = Qcz[2 * n3 + p] + fac2 * ww;
+            double v1 = 0.0, v2 = 0.0, v3 = 0.0, v5 = 0.0, U4 = 0.0, Tdy = 0.0, Tdz = 0.0, m = 0.0;
             if (visc) {
-                double fac_X = fac3 * mu[p] * (Tdy[p] + Tdz[p]);
-                double fac_Y = fac3 * mu[p] * U4[p];
-                double fac_Z = fac3 * mu[p] * (U5[p] + T2[p]);
-                Qv[p] = Qv[p] + fac_X;
-                Qv[n3 + p] = Qv[n3 + p] + fac_Y;
-                Qv[2 * n3 + p] = Qv[2 * n3 + p] + fac_Z;
-                Qv[4 * n3 + p] = Qv[4 * n3 + p] + u[p] * fac_X + v[p] * fac_Y + w[p] * fac_Z;
+                m = mu[p];
+                const double dm = dmu[p];
+                v5 = Qv[4 * n3 + p] + Pri * (m * (d2Ty[p] + d2Tz[p]) +
+                                             dm * (GTy[p] * GTy[p] + GTz[p] * GTz[p]));
+                U4 = dm * GTx[p];
+                Tdy = dm * GTy[p];
+                Tdz = dm * GTz[p];
+            }
+            const double gxx = Gxx[p], gyx = Gyx[p], gzx = Gzx[p], gxy = Gxy[p], gyy = Gyy[p], gzy = Gzy[p];
+            const double gxz = Gxz[p], gyz = Gyz[p], gzz = Gzz[p];
+            fac2 = -5.0e-1 * q4 * vv;
+            cy1 = cy1 + fac2 * gxy;
+            cy2 = cy2 + fac2 * gyy;
+            cy3 = cy3 + fac2 * gzy;
+            fac2 = -5.0e-1 * q4 * ww;
+            cz1 = cz1 + fac2 * gxz;
+            cz2 = cz2 + fac2 * gyz;
+            cz3 = cz3 + fac2 * gzz;
+            if (visc) {
+                // mu * d2(u,v,w)/dy2 terms
+                double fX = m * d2uy[p];
+                double fY = fb43 * m * d2vy[p];
+                double fZ = m * d2wy[p];
+                v1 = Qv[p] + fX;
+                v2 = Qv[n3 + p] + fY;
+                v3 = Qv[2 * n3 + p] + fZ;
+                v5 = v5 + uu * fX + vv * fY + ww * fZ;
+                // dilatation terms
+                double tmp1 = gxx;
+                double dil = tmp1 + gyy + gzz;
+                fX = U4 * (2.0 * tmp1 + fb23 * dil);
+                fY = Tdy * (2.0 * gyy + fb23 * dil) + fb13 * m * dGzz_y[p];
+                fZ = Tdz * (2.0 * gzz + fb23 * dil) + fb43 * m * d2wz[p];
+                v1 = v1 + fX;
+                v2 = v2 + fY;
+                v3 = v3 + fZ;
+                v5 = v5 + uu * fX + vv * fY + ww * fZ +
+                     m * (2.0 * (tmp1 * tmp1 + gyy * gyy + gzz * gzz) + fb23 * dil * dil);
+                // shear terms
+                double t1 = gyx + gxy, t2 = gzx + gxz, t3 = gzy + gyz;
+                fX = Tdy * t1 + Tdz * t2 + m * d2uz[p];
+                fY = U4 * t1 + Tdz * t3 + m * d2vz[p];
+                fZ = U4 * t2 + Tdy * t3;
+                v1 = v1 + fX;
+                v2 = v2 + fY;
+                v3 = v3 + fZ;
+                v5 = v5 + uu * fX + vv * fY + ww * fZ + m * (t1 * t1 + t2 * t2 + t3 * t3);
+                // cross derivatives of the velocity gradient
+                fX = fb13 * m * (dGyx_y[p] + dGzx_z[p]);
+                fY = fb13 * m * dGxx_y[p];
+                fZ = fb13 * m * (dGxx_z[p] + dGyz_y[p]);
+                v1 = v1 + fX;
+                v2 = v2 + fY;
+                v3 = v3 + fZ;
+                v5 = v5 + uu * fX + vv * fY + ww * fZ;
             }
             // velocities back to momenta, (m/rho)*rho as the reference does;
             // the FP32 mode keeps the double momenta instead of rounding them
             // through the float velocities
             if (fp64) {
-                Q1[p] = u[p] * Q4[p];
-                Q2[p] = v[p] * Q4[p];
-                Q3[p] = w[p] * Q4[p];
+                Q1[p] = uu * q4;
+                Q2[p] = vv * q4;
+                Q3[p] = ww * q4;
             }
+            const double cy[5] = {cy1, cy2, cy3, Qcy[3 * n3 + p], Qcy[4 * n3 + p]};
+            const double cz[5] = {cz1, cz2, cz3, Qcz[3 * n3 + p], Qcz[4 * n3 + p]};
+            const double vq[5] = {v1, v2, v3, 0.0, v5};
             for (int l = 0; l < 5; l++) {
                 size_t q = l * n3 + p;
-                double r = Qcx[q] + Qcy[q] + Qcz[q];
-                if (visc && l != 3) r = r + Qv[q];   // Qvisc(:,:,:,4) stays zero
+                double r = Qcx[q] + cy[l] + cz[l];
+                if (visc && l != 3) r = r + vq[l];   // Qvisc(:,:,:,4) stays zero
                 Qrhs[q] = r;
             }
         });

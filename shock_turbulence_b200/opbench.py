@@ -27,11 +27,13 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--dirs", default="xyz")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="step: FP64, or the FP32 mode (its line kernels run only inside the step)")
     args = ap.parse_args()
 
     import torch
     from shock_turbulence_b200 import Solver, default_params
-    p = default_params(args.n, re=100.0)
+    p = default_params(args.n, re=100.0, precision=1 if args.precision == "fp32" else 0)
     s = Solver(p)
     stream = torch.cuda.current_stream()
     s._check(s.lib.st_set_stream(s._h, stream.cuda_stream), "st_set_stream")
