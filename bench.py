@@ -567,7 +567,16 @@ def main():
     s.lib.st_launch_count(s._h, ctypes.byref(c1))
     buf = ctypes.create_string_buffer(1 << 16)
     s._check(s.lib.st_profile_report(s._h, buf, len(buf)), "st_profile_report")
-    prof = json.loads(buf.value.decode())
+    prof_sites = json.loads(buf.value.decode())
+    # pointwise launches are reported per source site; fold them into one entry
+    prof, sites = {}, {}
+    for k, v in prof_sites.items():
+        key = "k_pointwise" if k.startswith("k_pointwise@") else k
+        if key != k:
+            sites[k.split("@")[1]] = v
+        a = prof.setdefault(key, {"launches": 0, "ms": 0.0, "bytes": 0.0})
+        for f in ("launches", "ms", "bytes"):
+            a[f] += v[f]
     ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     cells = args.n ** 3
     value = aggregate_rate(cells, args.steps, ms, world)
@@ -613,7 +622,9 @@ def main():
                 "share_of_kernel_time": d["ms"] / step_ms_all if step_ms_all else None,
                 "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                                 "GB/s": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["bytes"] and v["ms"] else None}
-                            for k, v in prof.items()}}
+                            for k, v in prof.items()},
+                "pointwise_sites_ms": {"st_physics.cu:" + k: round(v["ms"], 2)
+                                       for k, v in sorted(sites.items(), key=lambda kv: -kv[1]["ms"])[:12]}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -206,6 +206,13 @@ int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd,
 int dev_dfd_prod_f(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd);
 int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd);
 int dev_gauss_f(st_ctx *c, int dir, const float *F, float *Fg);
+// last pass of a Laplacian: out = (derivative + E1) + E2 (x and z lines)
+int dev_dfd_sum(st_ctx *c, int dir, int asym, const double *F, double *dF, const double *E1, const double *E2);
+int dev_d2fd2_sum(st_ctx *c, int dir, int asym, const double *F, double *d2F, const double *E1,
+                  const double *E2);
+int dev_dfd_sum_f(st_ctx *c, int dir, int asym, const float *F, float *dF, const float *E1, const float *E2);
+int dev_d2fd2_sum_f(st_ctx *c, int dir, int asym, const float *F, float *d2F, const float *E1,
+                    const float *E2);
 int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd);
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0);
 int dev_gauss(st_ctx *c, int dir, const double *F, double *Fg);

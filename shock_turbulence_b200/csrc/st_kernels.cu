@@ -55,6 +55,28 @@ int dev_d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, double 
     return launch_line(c, OP_D2, a);
 }
 
+// The last pass of a Laplacian with the sum of the three directions fused into
+// its store: out = (d(F)/ds + E1) + E2 (first derivative, cadd = 1) or
+// (d2(F)/ds2 + E1) + E2; x and z lines only.
+int dev_dfd_sum(st_ctx *c, int dir, int asym, const double *F, double *dF, const double *E1, const double *E2) {
+    if (dir == 1) return fail(c, ST_E_ARG, "fused sum: x or z lines only");
+    LineArgs a = make_args(c, dir);
+    a.F = plain(F); a.O1 = dF; a.asym = asym; a.iadd = 0; a.E1 = E1; a.E2 = E2;
+    a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
+    a.t1 = c->tri[dir][asym ? K_D1A : K_D1S];
+    return launch_line(c, OP_D1, a);
+}
+
+int dev_d2fd2_sum(st_ctx *c, int dir, int asym, const double *F, double *d2F, const double *E1,
+                  const double *E2) {
+    if (dir == 1) return fail(c, ST_E_ARG, "fused sum: x or z lines only");
+    LineArgs a = make_args(c, dir);
+    a.F = plain(F); a.O2 = d2F; a.asym = asym; a.iadd = 0; a.E1 = E1; a.E2 = E2;
+    a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];
+    a.t2 = c->tri[dir][asym ? K_D2A : K_D2S];
+    return launch_line(c, OP_D2, a);
+}
+
 int dev_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
     LineArgs a = make_args(c, dir);
     a.F = plain(F); a.O1 = F0; a.asym = asym;
@@ -105,6 +127,27 @@ int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *
     a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
     a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];
     a.t1 = c->trif[dir][asym ? K_D1A : K_D1S];
+    a.t2 = c->trif[dir][asym ? K_D2A : K_D2S];
+    return launch_line(c, OP_D2, a);
+}
+
+int dev_dfd_sum_f(st_ctx *c, int dir, int asym, const float *F, float *dF, const float *E1, const float *E2) {
+    if (dir == 1) return fail(c, ST_E_ARG, "fused sum: x or z lines only");
+    ST_TRY(check_f2(c, plain_f(F), dF, E1) == ST_OK ? check_f2(c, plain_f(E2), nullptr, nullptr) : ST_E_ARG);
+    LineArgsF a = make_args<float>(c, dir);
+    a.F = plain_f(F); a.O1 = dF; a.asym = asym; a.iadd = 0; a.E1 = E1; a.E2 = E2;
+    a.fac1 = 1.0 * c->s1[dir] * (double)(a.geo.n - 1);
+    a.t1 = c->trif[dir][asym ? K_D1A : K_D1S];
+    return launch_line(c, OP_D1, a);
+}
+
+int dev_d2fd2_sum_f(st_ctx *c, int dir, int asym, const float *F, float *d2F, const float *E1,
+                    const float *E2) {
+    if (dir == 1) return fail(c, ST_E_ARG, "fused sum: x or z lines only");
+    ST_TRY(check_f2(c, plain_f(F), d2F, E1) == ST_OK ? check_f2(c, plain_f(E2), nullptr, nullptr) : ST_E_ARG);
+    LineArgsF a = make_args<float>(c, dir);
+    a.F = plain_f(F); a.O2 = d2F; a.asym = asym; a.iadd = 0; a.E1 = E1; a.E2 = E2;
+    a.fac2 = ((double)((a.geo.n - 1) * (a.geo.n - 1))) * c->s2[dir];
     a.t2 = c->trif[dir][asym ? K_D2A : K_D2S];
     return launch_line(c, OP_D2, a);
 }

@@ -140,10 +140,25 @@ __device__ __forceinline__ void stv(double *p, double v) { *p = v; }
 __device__ __forceinline__ void stv(float *p, double v) { *p = (float)v; }
 __device__ __forceinline__ void stv(float *p, F2 v) { *reinterpret_cast<float2 *>(p) = make_float2(v.x, v.y); }
 
+// add: O += r; otherwise O = r, or O = (r + E1) + E2 when E1 is given (the
+// sum that follows the last derivative of a Laplacian, fused into its store)
 template <int S, int N, class T, class V>
 __device__ __forceinline__ void store_rows(const V (&r)[N], T *__restrict__ O, const ColMap &m,
-                                           int lane, int a, int add) {
-    T *p = O + m.base + (size_t)lane * Val<T>::W * m.lstride + (size_t)a * m.rstride;
+                                           int lane, int a, int add, const T *E1 = nullptr,
+                                           const T *E2 = nullptr) {
+    const size_t off = m.base + (size_t)lane * Val<T>::W * m.lstride + (size_t)a * m.rstride;
+    T *p = O + off;
+    if (E1) {
+        V e1[S], e2[S];
+#pragma unroll
+        for (int t = 0; t < S; t++) {
+            e1[t] = Ld<V, T>::get(E1 + off + (size_t)t * m.rstride);
+            e2[t] = Ld<V, T>::get(E2 + off + (size_t)t * m.rstride);
+        }
+#pragma unroll
+        for (int t = 0; t < S; t++) stv(p + (size_t)t * m.rstride, (r[t] + e1[t]) + e2[t]);
+        return;
+    }
     if (add) {
         V prev[S];
 #pragma unroll

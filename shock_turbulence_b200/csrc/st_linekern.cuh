@@ -22,6 +22,7 @@ struct LineArgsT {
     int S, P;
     double fac1, fac2;
     int asym, iadd;
+    const T *E1, *E2;   // x and z lines: O1 (k_dfd) / O2 (k_d2fd2) = (result + E1) + E2 when E1 is set
     int cyc;            // periodic family: wrapped halos, corner correction (selects the CYC kernels)
     TriTabT<T> t1, t2;
     PenTab p;
@@ -54,14 +55,15 @@ __device__ __forceinline__ void get_rows(V (&v)[S + 2 * H], const A *tile, const
 }
 template <int S, bool YT, int N, class T, class V, class A>
 __device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const ColMap &m,
-                                         int lane, int a, int n, int add) {
+                                         int lane, int a, int n, int add, const T *E1 = nullptr,
+                                         const T *E2 = nullptr) {
     if (YT) {
         __syncthreads();                 // every thread has finished reading the tile
         ytile_put<S>(tile, v, lane, a, n);
         __syncthreads();
         ytile_store<T>(tile, O, m.base, n, add);
     } else {
-        store_rows<S>(v, O, m, lane, a, add);
+        store_rows<S>(v, O, m, lane, a, add, E1, E2);
     }
 }
 
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
     rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
-    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd);
+    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd, a.E1, a.E2);
 }
 
 // D2F*2_sym/_asym and the periodic D2F*2: O2 = d2F/ds2; if iadd, O1 = dF/ds
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
         rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
         if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t2.cyc, s, a.P, lane, cb);
-        put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0);
+        put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0, a.E1, a.E2);
     }
     if (a.iadd) {
         __syncthreads();   // carry buffers and tile are reused
@@ -164,6 +166,7 @@ static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t 
     double b = es * nin[a.F.op] + es;              // + one output
     if (op == OP_D1 && a.iadd) b += es;            // read-modify-write
     if (op == OP_D2 && a.iadd) b += es;            // second output
+    if (a.E1) b += 2 * es;                         // epilogue addends
     static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
     int pi = prof_start(c, names[op], b * n3);
     switch (op) {

@@ -16,17 +16,21 @@ __global__ void k_pfor(size_t n, Fn fn) {
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
         fn(p);
 }
+// site: "k_pointwise@<source line>" for the per-launch timing report
 template <class Fn>
-static int pfor(st_ctx *c, size_t n, Fn fn) {
+static int pfor(st_ctx *c, size_t n, const char *site, Fn fn) {
     size_t blocks = (n + 255) / 256;    // one element per thread
     if (blocks == 0) return ST_OK;
-    int pi = prof_start(c, "k_pointwise", 0.0);
+    int pi = prof_start(c, site, 0.0);
     k_pfor<<<(unsigned)blocks, 256, 0, c->stream>>>(n, fn);
     prof_stop(c, pi);
     ST_CUDA(c, cudaGetLastError());
     return ST_OK;
 }
-#define PFOR(c, n, ...) ST_TRY(pfor((c), (n), [=] __device__(size_t p) __VA_ARGS__))
+#define ST_STR2(x) #x
+#define ST_STR(x) ST_STR2(x)
+#define PFOR(c, n, ...) \
+    ST_TRY(pfor((c), (n), "k_pointwise@" ST_STR(__LINE__), [=] __device__(size_t p) __VA_ARGS__))
 
 // producer expressions evaluated by the derivative kernels while loading
 template <class R>
@@ -59,6 +63,21 @@ static int d2fd2(st_ctx *c, int dir, int asym, const double *F, double *dF, doub
 }
 static int d2fd2(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd) {
     return dev_d2fd2_f(c, dir, asym, F, dF, d2F, iadd);
+}
+static int dfd_sum(st_ctx *c, int dir, int asym, const double *F, double *dF, const double *E1,
+                   const double *E2) {
+    return dev_dfd_sum(c, dir, asym, F, dF, E1, E2);
+}
+static int dfd_sum(st_ctx *c, int dir, int asym, const float *F, float *dF, const float *E1, const float *E2) {
+    return dev_dfd_sum_f(c, dir, asym, F, dF, E1, E2);
+}
+static int d2fd2_sum(st_ctx *c, int dir, int asym, const double *F, double *d2F, const double *E1,
+                     const double *E2) {
+    return dev_d2fd2_sum(c, dir, asym, F, d2F, E1, E2);
+}
+static int d2fd2_sum(st_ctx *c, int dir, int asym, const float *F, float *d2F, const float *E1,
+                     const float *E2) {
+    return dev_d2fd2_sum_f(c, dir, asym, F, d2F, E1, E2);
 }
 static int gauss(st_ctx *c, int dir, const double *F, double *Fg) { return dev_gauss(c, dir, F, Fg); }
 static int gauss(st_ctx *c, int dir, const float *F, float *Fg) { return dev_gauss_f(c, dir, F, Fg); }
@@ -412,18 +431,16 @@ static int laplacian(st_ctx *c, const R *S, R *d2S) {
         // Compute_Laplacian src/hyper_dynamic.f:41-58 (second derivatives)
         ST_TRY(d2fd2(c, 0, 0, S, (R *)nullptr, (R *)t1, 0));
         ST_TRY(d2fd2(c, 1, 0, S, (R *)nullptr, (R *)t2, 0));
-        ST_TRY(d2fd2(c, 2, 0, S, (R *)nullptr, d2S, 0));
-        PFOR(c, c->dm.n3, { d2S[p] = d2S[p] + pt1[p] + pt2[p]; });
-        return ST_OK;
+        // d2S = d2S + t1 + t2 in the z pass's store
+        return d2fd2_sum(c, 2, 0, S, d2S, (const R *)pt1, (const R *)pt2);
     }
     ST_TRY(dfd(c, 0, 0, S, (R *)dS, 0, 1.0));
     ST_TRY(dfd(c, 0, 1, (const R *)dS, (R *)t1, 0, 1.0));
     ST_TRY(dfd(c, 1, 0, S, (R *)dS, 0, 1.0));
     ST_TRY(dfd(c, 1, 1, (const R *)dS, (R *)t2, 0, 1.0));
     ST_TRY(dfd(c, 2, 0, S, (R *)dS, 0, 1.0));
-    ST_TRY(dfd(c, 2, 1, (const R *)dS, d2S, 0, 1.0));
-    PFOR(c, c->dm.n3, { d2S[p] = d2S[p] + pt1[p] + pt2[p]; });
-    return ST_OK;
+    // d2S = d2S + temp1 + temp2 (src/hyper_dynamic_sym_mf.f:61) in the z pass's store
+    return dfd_sum(c, 2, 1, (const R *)dS, d2S, (const R *)pt1, (const R *)pt2);
 }
 
 // Compute_hyper src/hyper_dynamic_sym_mf.f:166-334 (+ Compute_coeff1 :79-158,
@@ -697,13 +714,14 @@ static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     Phys f = phys(c);
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
-    // symmetry planes: x=0 (rho u), z=0 (rho w), y=0 (rho v)
-    PFOR(c, n3, {
-        size_t j = p % My, k = (p / My) % Mz, i = p / ((size_t)My * Mz);
-        if (i == 0) Q1[p] = 0.0;
-        if (k == 0) Q3[p] = 0.0;
-        if (j == 0) Q2[p] = 0.0;
-    });
+    // symmetry planes: x=0 (rho u), z=0 (rho w), y=0 (rho v); one launch per
+    // plane over its cells only
+    {
+        const size_t MyMz = (size_t)My * Mz;
+        PFOR(c, MyMz, { Q1[p] = 0.0; });                                          // i = 0: p = j + My*k
+        PFOR(c, (size_t)My * Mx, { Q3[(p % My) + MyMz * (p / My)] = 0.0; });      // k = 0: p = j + My*i
+        PFOR(c, (size_t)Mz * Mx, { Q2[(size_t)My * p] = 0.0; });                  // j = 0: p = k + Mz*i
+    }
     ScratchNT<R> s(c, 4);
     R *P = s[0], *dPx = s[1], *dPy = s[2], *dPz = s[3];
     PFOR(c, n3, {
@@ -770,8 +788,16 @@ static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrh
         len[d] = Ns[d] - start[d];
     }
     const int sx = start[0], sy = start[1], sz = start[2], lx = len[0], ly = len[1], lz = len[2];
+    const bool idx32 = n3 <= 0xffffffffull;   // 32-bit index arithmetic when it suffices
     PFOR(c, n3, {
-        int j = (int)(p % My), k = (int)((p / My) % Mz), i = (int)(p / ((size_t)My * Mz));
+        int j, k, i;
+        if (idx32) {
+            unsigned q = (unsigned)p, r = q / (unsigned)My;
+            j = (int)(q - r * (unsigned)My); k = (int)(r % (unsigned)Mz); i = (int)(r / (unsigned)Mz);
+        } else {
+            size_t r = p / My;
+            j = (int)(p - r * My); k = (int)(r % Mz); i = (int)(r / Mz);
+        }
         auto sig = [](int gI, int st, int ln) -> double {
             if (gI >= st) {
                 float r = (float)(gI - st) / (float)ln;   // REAL/REAL, src/sponge_mf.f:87-89
