@@ -317,76 +317,136 @@ struct RowReader {
 // They are copied with 16-byte coalesced accesses into an [NL][n+1] tile of
 // the arithmetic type (odd stride: the lines of a half-warp start in distinct
 // banks), so that each thread reads its segment conflict-free.
+// Each thread keeps kTB loads in flight: a batch of loads is issued before
+// any of them is stored into the tile (a load-then-store loop would wait for
+// every load in turn).
+constexpr int kTB = 4;
+
 template <int OP, class T>
 __device__ __forceinline__ void ytile_load(typename Val<T>::A *tile, const ProdT<T> &F, size_t base, int n) {
     constexpr int NL = kLanes * Val<T>::W;
+    const int nt = blockDim.x;
     if constexpr (sizeof(T) == 8) {
         const int half = NL * n / 2;
         if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
             const double2 *src = reinterpret_cast<const double2 *>(F.a + base);
-            for (int q = threadIdx.x; q < half; q += blockDim.x) {
-                double2 d = __ldg(src + q);
-                int e = 2 * q, line = e / n, row = e - line * n;
-                tile[line * (n + 1) + row] = d.x;
-                tile[line * (n + 1) + row + 1] = d.y;
+            for (int q0 = threadIdx.x; q0 < half; q0 += kTB * nt) {
+                double2 d[kTB];
+#pragma unroll
+                for (int u = 0; u < kTB; u++)
+                    if (q0 + u * nt < half) d[u] = __ldg(src + q0 + u * nt);
+#pragma unroll
+                for (int u = 0; u < kTB; u++) {
+                    const int q = q0 + u * nt;
+                    if (q < half) {
+                        int e = 2 * q, line = e / n, row = e - line * n;
+                        tile[line * (n + 1) + row] = d[u].x;
+                        tile[line * (n + 1) + row + 1] = d[u].y;
+                    }
+                }
             }
             return;
         }
     } else {
+        const int quarter = NL * n / 4;
         if (OP == PR_A && ((reinterpret_cast<uintptr_t>(F.a + base) & 15) == 0)) {
             const float4 *src = reinterpret_cast<const float4 *>(F.a + base);
-            for (int q = threadIdx.x; q < NL * n / 4; q += blockDim.x) {
-                float4 d = __ldg(src + q);
-                int e = 4 * q, line = e / n, row = e - line * n;   // n % 4 == 0: one line
-                float *t = tile + line * (n + 1) + row;
-                t[0] = d.x; t[1] = d.y; t[2] = d.z; t[3] = d.w;
+            for (int q0 = threadIdx.x; q0 < quarter; q0 += kTB * nt) {
+                float4 d[kTB];
+#pragma unroll
+                for (int u = 0; u < kTB; u++)
+                    if (q0 + u * nt < quarter) d[u] = __ldg(src + q0 + u * nt);
+#pragma unroll
+                for (int u = 0; u < kTB; u++) {
+                    const int q = q0 + u * nt;
+                    if (q < quarter) {
+                        int e = 4 * q, line = e / n, row = e - line * n;   // n % 4 == 0: one line
+                        float *t = tile + line * (n + 1) + row;
+                        t[0] = d[u].x; t[1] = d[u].y; t[2] = d[u].z; t[3] = d[u].w;
+                    }
+                }
             }
             return;
         }
     }
     using A = typename Val<T>::A;
-    for (int q = threadIdx.x; q < NL * n; q += blockDim.x) {
-        int line = q / n, row = q - line * n;
-        tile[line * (n + 1) + row] = prod_eval<OP, A>(F, base + q);
+    const int tot = NL * n;
+    for (int q0 = threadIdx.x; q0 < tot; q0 += kTB * nt) {
+        A d[kTB];
+#pragma unroll
+        for (int u = 0; u < kTB; u++)
+            if (q0 + u * nt < tot) d[u] = prod_eval<OP, A>(F, base + q0 + u * nt);
+#pragma unroll
+        for (int u = 0; u < kTB; u++) {
+            const int q = q0 + u * nt;
+            if (q < tot) {
+                int line = q / n, row = q - line * n;
+                tile[line * (n + 1) + row] = d[u];
+            }
+        }
     }
 }
 template <class T>
 __device__ __forceinline__ void ytile_store(const typename Val<T>::A *tile, T *__restrict__ O, size_t base, int n,
                                             int add) {
     constexpr int NL = kLanes * Val<T>::W;
+    const int nt = blockDim.x;
     if constexpr (sizeof(T) == 8) {
         if (!(reinterpret_cast<uintptr_t>(O + base) & 15)) {
             double2 *dst = reinterpret_cast<double2 *>(O + base);
             const int half = NL * n / 2;
-            for (int q = threadIdx.x; q < half; q += blockDim.x) {
-                int e = 2 * q, line = e / n, row = e - line * n;
-                double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
+            for (int q0 = threadIdx.x; q0 < half; q0 += kTB * nt) {
+                double2 o[kTB];
                 if (add) {
-                    double2 o = dst[q];
-                    d.x = o.x + d.x;
-                    d.y = o.y + d.y;
+#pragma unroll
+                    for (int u = 0; u < kTB; u++)
+                        if (q0 + u * nt < half) o[u] = dst[q0 + u * nt];
                 }
-                dst[q] = d;
+#pragma unroll
+                for (int u = 0; u < kTB; u++) {
+                    const int q = q0 + u * nt;
+                    if (q < half) {
+                        int e = 2 * q, line = e / n, row = e - line * n;
+                        double2 d = make_double2(tile[line * (n + 1) + row], tile[line * (n + 1) + row + 1]);
+                        if (add) {
+                            d.x = o[u].x + d.x;
+                            d.y = o[u].y + d.y;
+                        }
+                        dst[q] = d;
+                    }
+                }
             }
             return;
         }
     } else {
         if (!(reinterpret_cast<uintptr_t>(O + base) & 15)) {
             float4 *dst = reinterpret_cast<float4 *>(O + base);
-            for (int q = threadIdx.x; q < NL * n / 4; q += blockDim.x) {
-                int e = 4 * q, line = e / n, row = e - line * n;
-                const float *t = tile + line * (n + 1) + row;
-                float4 d = make_float4(t[0], t[1], t[2], t[3]);
+            const int quarter = NL * n / 4;
+            for (int q0 = threadIdx.x; q0 < quarter; q0 += kTB * nt) {
+                float4 o[kTB];
                 if (add) {
-                    float4 o = dst[q];
-                    d.x = o.x + d.x; d.y = o.y + d.y; d.z = o.z + d.z; d.w = o.w + d.w;
+#pragma unroll
+                    for (int u = 0; u < kTB; u++)
+                        if (q0 + u * nt < quarter) o[u] = dst[q0 + u * nt];
                 }
-                dst[q] = d;
+#pragma unroll
+                for (int u = 0; u < kTB; u++) {
+                    const int q = q0 + u * nt;
+                    if (q < quarter) {
+                        int e = 4 * q, line = e / n, row = e - line * n;
+                        const float *t = tile + line * (n + 1) + row;
+                        float4 d = make_float4(t[0], t[1], t[2], t[3]);
+                        if (add) {
+                            d.x = o[u].x + d.x; d.y = o[u].y + d.y; d.z = o[u].z + d.z; d.w = o[u].w + d.w;
+                        }
+                        dst[q] = d;
+                    }
+                }
             }
             return;
         }
     }
-    for (int q = threadIdx.x; q < NL * n; q += blockDim.x) {
+    for (int q = threadIdx.x; q < NL * n; q += nt) {
         int line = q / n, row = q - line * n;
         auto v = tile[line * (n + 1) + row];
         O[base + q] = (T)(add ? (T)O[base + q] + v : v);
