@@ -37,6 +37,11 @@ struct TriTabT {
     const A *wb;   // [P][P]: carry into segment s = sum_{s'>s} wb[s'][s] * B_{s'}
     int kf, kb;    // segments back/ahead whose carry weight can change a result of type A
     const A *cyc;  // periodic family: [n][2] corner correction (see st_tables.cpp), else null
+    // Away from the line ends the factorisation reaches a fixed point: in
+    // segments slo <= s < shi every row's l, up, id equal (bitwise) cl, cup,
+    // cid, which the solve then keeps in registers instead of loading per row.
+    int slo, shi;
+    A cl, cup, cid;
 };
 using TriTab = TriTabT<double>;
 
@@ -53,6 +58,10 @@ struct PenTab {
     const double *mb;        // [P][P][4]
     int kf, kb;              // segments back/ahead whose carry weight is >= 1e-20
     const double *cyc;       // periodic family: [n][4] corner correction, else null
+    // segments slo <= s < shi: every row's p1, p2, q1, q2, id equal (bitwise)
+    // the constants below (the factorisation's interior fixed point)
+    int slo, shi;
+    double cp1, cp2, cq1, cq2, cid;
 };
 
 enum TriKind { K_D1S = 0, K_D1A = 1, K_D2S = 2, K_D2A = 3 };

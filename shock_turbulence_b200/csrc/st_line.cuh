@@ -222,20 +222,36 @@ template <int S, int N, class V, class A>
 __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s, int P, int lane,
                                           CarryBufT<V> &cb) {
     const int a = s * S;
+    const bool flat = s >= T.slo && s < T.shi;   // interior: constant factors in registers
+    if (flat) {
+        const A l = T.cl;
 #pragma unroll
-    for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * __ldg(T.l + a + t);
+        for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * l;
+    } else {
+#pragma unroll
+        for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * __ldg(T.l + a + t);
+    }
     cb.a[s][lane][0] = r[S - 1];
     __syncthreads();
     V cin = V(0.0);
+#pragma unroll 4
     for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
-    r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
+    if (flat) {
+        const A up = T.cup, id = T.cid;
+        r[S - 1] = r[S - 1] * id;
 #pragma unroll
-    for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
+        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - up * r[t + 1]) * id;
+    } else {
+        r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
+#pragma unroll
+        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
+    }
     cb.b[s][lane][0] = r[0];
     __syncthreads();
     V ein = V(0.0);
+#pragma unroll 4
     for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
         ein = vfma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
 #pragma unroll
@@ -250,17 +266,30 @@ template <int S, int N>
 __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s, int P, int lane,
                                           CarryBuf &cb) {
     const int a = s * S;
+    const bool flat = s >= T.slo && s < T.shi;   // interior: constant factors in registers
+    if (flat) {
+        const double p1 = T.cp1, p2 = T.cp2;
 #pragma unroll
-    for (int t = 1; t < S; t++) {
-        double v = r[t];
-        if (t >= 2) v = v - __ldg(T.p2 + a + t) * r[t >= 2 ? t - 2 : 0];
-        v = v - __ldg(T.p1 + a + t) * r[t - 1];
-        r[t] = v;
+        for (int t = 1; t < S; t++) {
+            double v = r[t];
+            if (t >= 2) v = v - p2 * r[t >= 2 ? t - 2 : 0];
+            v = v - p1 * r[t - 1];
+            r[t] = v;
+        }
+    } else {
+#pragma unroll
+        for (int t = 1; t < S; t++) {
+            double v = r[t];
+            if (t >= 2) v = v - __ldg(T.p2 + a + t) * r[t >= 2 ? t - 2 : 0];
+            v = v - __ldg(T.p1 + a + t) * r[t - 1];
+            r[t] = v;
+        }
     }
     cb.a[s][lane][0] = r[S - 1];
     cb.a[s][lane][1] = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
     __syncthreads();
     double c1 = 0.0, c2 = 0.0;
+#pragma unroll 4
     for (int sp = max(0, s - T.kf); sp < s; sp++) {
         const double *m = T.mf + ((size_t)sp * P + s) * 4;
         double a1 = cb.a[sp][lane][0], a2 = cb.a[sp][lane][1];
@@ -269,17 +298,29 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
     }
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g1 + a + t), c1, fma(__ldg(T.g2 + a + t), c2, r[t]));
+    if (flat) {
+        const double q1 = T.cq1, q2 = T.cq2, id = T.cid;
 #pragma unroll
-    for (int t = S - 1; t >= 0; t--) {
-        double v = r[t];
-        if (t + 1 < S) v = v - __ldg(T.q1 + a + t) * r[t + 1 < S ? t + 1 : t];
-        if (t + 2 < S) v = v - __ldg(T.q2 + a + t) * r[t + 2 < S ? t + 2 : t];
-        r[t] = v * __ldg(T.id + a + t);
+        for (int t = S - 1; t >= 0; t--) {
+            double v = r[t];
+            if (t + 1 < S) v = v - q1 * r[t + 1 < S ? t + 1 : t];
+            if (t + 2 < S) v = v - q2 * r[t + 2 < S ? t + 2 : t];
+            r[t] = v * id;
+        }
+    } else {
+#pragma unroll
+        for (int t = S - 1; t >= 0; t--) {
+            double v = r[t];
+            if (t + 1 < S) v = v - __ldg(T.q1 + a + t) * r[t + 1 < S ? t + 1 : t];
+            if (t + 2 < S) v = v - __ldg(T.q2 + a + t) * r[t + 2 < S ? t + 2 : t];
+            r[t] = v * __ldg(T.id + a + t);
+        }
     }
     cb.b[s][lane][0] = r[0];
     cb.b[s][lane][1] = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
     __syncthreads();
     double e1 = 0.0, e2 = 0.0;
+#pragma unroll 4
     for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++) {
         const double *m = T.mb + ((size_t)sp * P + s) * 4;
         double b1 = cb.b[sp][lane][0], b2 = cb.b[sp][lane][1];

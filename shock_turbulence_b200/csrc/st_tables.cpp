@@ -204,11 +204,35 @@ static std::vector<double> cyclic_correction(int n, double bt, double al, int k)
 struct TriHost {
     std::vector<double> l, g, up, id, h, wf, wb;
     int kf = 0, kb = 0;
+    int slo = 0, shi = 0;
 };
 struct PenHost {
     std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mf, mb;
     int kf = 0, kb = 0;
+    int slo = 0, shi = 0;
 };
+
+// The contiguous range [slo, shi) of segments around the middle one in which
+// every listed coefficient array holds, on every row, exactly (bitwise) its
+// value at the middle row; empty when the middle segment itself varies (the
+// antisymmetric filter's factorisation ends in a cycle, not a fixed point).
+static void flat_segments(const std::vector<const std::vector<double> *> &arrs, int n, int S, int *slo,
+                          int *shi) {
+    const int P = n / S, mid = n / 2;
+    auto flat = [&](int s) {
+        for (const auto *v : arrs)
+            for (int i = s * S; i < s * S + S; i++)
+                if ((*v)[i] != (*v)[mid]) return false;
+        return true;
+    };
+    int sm = mid / S;
+    *slo = *shi = 0;
+    if (!flat(sm)) return;
+    int lo = sm, hi = sm + 1;
+    while (lo > 0 && flat(lo - 1)) lo--;
+    while (hi < P && flat(hi)) hi++;
+    *slo = lo; *shi = hi;
+}
 
 // Carry weights decay geometrically with the distance between segments.
 // Contributions with weight below 1e-20 cannot change an FP64 result of the
@@ -264,6 +288,7 @@ static TriHost tri_tables(const std::vector<double> &a, const std::vector<double
     }
     t.kf = carry_span(t.wf, P, 1, true);
     t.kb = carry_span(t.wb, P, 1, false);
+    flat_segments({&t.l, &t.up, &t.id}, n, S, &t.slo, &t.shi);
     return t;
 }
 
@@ -342,6 +367,7 @@ static PenHost pen_tables(std::vector<double> M[5], int n, int S) {
             mat2mul(v, &Nseg[sp * 4], v);
         }
     }
+    flat_segments({&t.p1, &t.p2, &t.q1, &t.q2, &t.id}, n, S, &t.slo, &t.shi);
     t.kf = carry_span(t.mf, P, 4, true);
     t.kb = carry_span(t.mb, P, 4, false);
     return t;
@@ -376,7 +402,12 @@ static void upload_tri(st_ctx *c, st::TriTab &t, st::TriTabT<float> &tf, const T
     t.wf = upload(c, h.wf, err); t.wb = upload(c, h.wb, err);
     t.kf = h.kf; t.kb = h.kb;
     t.cyc = K ? upload(c, *K, err) : nullptr;
+    const int mid = (int)h.l.size() / 2;
+    t.slo = h.slo; t.shi = h.shi;
+    t.cl = h.l[mid]; t.cup = h.up[mid]; t.cid = h.id[mid];
     tf = st::TriTabT<float>{};
+    tf.slo = h.slo; tf.shi = h.shi;
+    tf.cl = (float)t.cl; tf.cup = (float)t.cup; tf.cid = (float)t.cid;
     if (c->p.precision != ST_PRECISION_FP32) return;
     tf.l = upload_f(c, h.l, err); tf.g = upload_f(c, h.g, err); tf.up = upload_f(c, h.up, err);
     tf.id = upload_f(c, h.id, err); tf.h = upload_f(c, h.h, err);
@@ -418,6 +449,11 @@ static int build_tables_periodic(st_ctx *c) {
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
             t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
             t.kf = h.kf; t.kb = h.kb;
+            {
+                const int mid = n / 2;
+                t.slo = h.slo; t.shi = h.shi;
+                t.cp1 = h.p1[mid]; t.cp2 = h.p2[mid]; t.cq1 = h.q1[mid]; t.cq2 = h.q2[mid]; t.cid = h.id[mid];
+            }
             t.cyc = upload(c, K, &err);
         }
     }
@@ -447,6 +483,11 @@ int build_tables(st_ctx *c) {
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
             t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
             t.kf = h.kf; t.kb = h.kb;
+            {
+                const int mid = n / 2;
+                t.slo = h.slo; t.shi = h.shi;
+                t.cp1 = h.p1[mid]; t.cp2 = h.p2[mid]; t.cq1 = h.q1[mid]; t.cq2 = h.q2[mid]; t.cid = h.id[mid];
+            }
             t.cyc = nullptr;
         }
     }
