@@ -47,6 +47,36 @@ using LineArgsF = LineArgsT<float>;
                                       : RowReader<OP, T, V>{nullptr, &a.F, m.base + (size_t)lane * W * m.lstride, \
                                                             m.rstride, 0};
 
+// L2 prefetch of the rows the block kAhead blocks later will load (about one
+// wave of resident CTAs ahead: 2 per SM on 148 SMs), so that the next wave's
+// loads find their lines in L2 while this wave solves.
+constexpr unsigned kAhead = 2 * 148;
+__device__ __forceinline__ void pf_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+template <int S, bool YT, int OP, class T>
+__device__ __forceinline__ void prefetch_next(const LineArgsT<T> &a, int lane, int row0) {
+    const unsigned nb = blockIdx.x + kAhead;
+    if (nb >= gridDim.x) return;
+    constexpr int W = Val<T>::W;
+    constexpr int NI = OP == PR_A ? 1 : OP == PR_MUL ? 2 : OP == PR_SPECT ? 4 : 3;   // fields the producer reads
+    const ColMap m = a.geo.template map<W>(nb);
+    const T *f[4] = {a.F.a, a.F.b, a.F.c, a.F.d};
+    if (YT) {
+        // the block's lines are one contiguous range: one 128-byte line per thread and pass
+        const size_t bytes = (size_t)kLanes * W * a.geo.n * sizeof(T);
+        for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)
+#pragma unroll
+            for (int k = 0; k < NI; k++) pf_l2(reinterpret_cast<const char *>(f[k] + m.base) + off);
+    } else {
+        // a row of the block's lines is 128 contiguous bytes: lane 0 of each segment
+        if (lane != 0) return;
+#pragma unroll
+        for (int t = 0; t < S; t++)
+#pragma unroll
+            for (int k = 0; k < NI; k++) pf_l2(f[k] + m.base + (size_t)(row0 + t) * m.rstride);
+    }
+}
+
 template <int S, int H, bool YT, int OP, class T, class V, class A>
 __device__ __forceinline__ void get_rows(V (&v)[S + 2 * H], const A *tile, const ProdT<T> &F,
                                          const ColMap &m, int lane, int a, int n, int cyc) {
@@ -71,9 +101,10 @@ __device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const C
 template <int S, bool YT, int OP, bool CYC, class T>
 __global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
     LINE_PROLOGUE
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
     V v[S + 4];
     get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
     rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
@@ -88,9 +119,10 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
-        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
         V v[S + 4];
         get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+        if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
         rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
         if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t2.cyc, s, a.P, lane, cb);
@@ -132,9 +164,10 @@ __global__ void __launch_bounds__(512, 2) k_gauss(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
     V v[S + 8];
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
     rhs_gauss<S, 4>(v, row0, n, CYC, a.K, rd);
     put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
 }
