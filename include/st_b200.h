@@ -274,6 +274,26 @@ int  st_query(st_ctx *c);
  * scratch pool, tables); the pool grows during the first steps. */
 int  st_memory(st_ctx *c, long long *bytes);
 
+/* ---- Output-side diagnostics (_mf family) ----------------------------------
+ * The per-step calls of Output (src/out_mf.f:671-705) on the context's state.
+ * Compute_Grad src/grad_sym.f:13-120: Grad (4 fields w_x, w_y, w_z,
+ * dilatation, or NULL), MaxDil = max|dilatation| and Enstrophy =
+ * 0.5*sum(|w|^2)/(Nx*Ny*Nz) of /TRACK/; the nine velocity derivatives are
+ * left in /GRAD/ as the reference leaves them (FP64 mode). */
+int  st_compute_grad(st_ctx *c, double *Grad, double *maxdil, double *enstrophy);
+/* Compute_SRM_Stats pproc/pproc_mf.f:4-186 (with Compute_shell_avg
+ * src/auxiliary_mf.f:266-332): the mix_stats record (mixing width hmix,
+ * mean turbulent kinetic energy tke_total) and, when not NULL, the N_avg
+ * shell averages of the radial velocity and of Y (N_avg from
+ * st_shell_count, src/header:14).  Cells beyond the last tke bin, which the
+ * reference leaves unassigned, contribute 0. */
+int  st_shell_count(st_ctx *c, int *n_avg);
+int  st_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg);
+/* Generate_Shock_Surface src/shock.f:163-260: the shock_stats record
+ * (mean distance of the cells with beta_hyper > 0.1*max from their centroid,
+ * and sqrt(sum of squared deviations)/(n*mean)). */
+int  st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms);
+
 /* ---- 1-D spherical-radial family, batched ---------------------------------
  * Many independent problems, each one run of the reference's radial program
  * (src/makefile_radial) on a line of n[k] points, 16 <= n[k] <= 4096, of

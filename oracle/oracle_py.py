@@ -62,6 +62,10 @@ def _load():
     lib.orc_pentadiagonal.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
     lib.orc_set_threads.argtypes = [ctypes.c_int]
+    lib.orc_compute_grad.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+    lib.orc_shell_count.argtypes = [ctypes.c_void_p]
+    lib.orc_compute_srm_stats.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+    lib.orc_shock_surface.argtypes = [ctypes.c_void_p, _dp, _dp]
     rp = ctypes.POINTER(StRadialParams)
     ci, cd = ctypes.c_int, ctypes.c_double
     lib.orc_rad_radius.argtypes = [ci, cd, _dp]
@@ -223,6 +227,24 @@ class Oracle:
         out = np.zeros(10)
         lib().orc_get_monitors(ctypes.c_void_p(self._c), _p(out))
         return out
+
+    # Output-side diagnostics (src/grad_sym.f, pproc/pproc_mf.f, src/shock.f)
+    def compute_grad(self):
+        G = np.zeros((4,) + self.shape)
+        a, b = np.zeros(1), np.zeros(1)
+        lib().orc_compute_grad(ctypes.c_void_p(self._c), _p(G), _p(a), _p(b))
+        return G, float(a[0]), float(b[0])
+
+    def compute_srm_stats(self):
+        na = lib().orc_shell_count(ctypes.c_void_p(self._c))
+        h, t, ur, ya = np.zeros(1), np.zeros(1), np.zeros(na), np.zeros(na)
+        lib().orc_compute_srm_stats(ctypes.c_void_p(self._c), _p(h), _p(t), _p(ur), _p(ya))
+        return float(h[0]), float(t[0]), ur, ya
+
+    def shock_surface(self):
+        a, b = np.zeros(1), np.zeros(1)
+        lib().orc_shock_surface(ctypes.c_void_p(self._c), _p(a), _p(b))
+        return float(a[0]), float(b[0])
 
 
 # ---- 1-D spherical-radial family (st_oracle_radial.c) ---------------------

@@ -1920,3 +1920,180 @@ int orc_set_common(orc *c, const char *name, const double *in) {
     memcpy(p, in, nf * c->n3 * 8);
     return 0;
 }
+
+/* ---- Output-side diagnostics ------------------------------------------------ */
+/* grid coordinate xcor(I) of Uniform_X, src/grid.f:116-128 (i 0-based) */
+static double gcor(const orc *c, int d, int i) {
+    const double leng[3] = {c->p.x_leng, c->p.y_leng, c->p.z_leng};
+    const double start[3] = {c->p.x_start, c->p.y_start, c->p.z_start};
+    return start[d] + leng[d] * (double)(i) / (double)(c->M[d] - 1);
+}
+
+/* Compute_Grad src/grad_sym.f:13-120: Grad = (w_x, w_y, w_z, dilatation) of
+ * the state in /RKWORK/, the nine velocity derivatives left in /GRAD/ as the
+ * reference leaves them, MaxDil = max|Dil| (Compute_Max), Enstrophy =
+ * 0.5*sum(w.w)/(Nx*Ny*Nz) with Compute_Sum's loop order (src/auxiliary_mf.f:
+ * 187-213: I outer, K inner). */
+void orc_compute_grad(orc *c, double *Grad, double *maxdil, double *enstrophy) {
+    const size_t n3 = c->n3;
+    double *U = dalloc(3 * n3);
+    const double *Q = c->Q;
+    for (size_t p = 0; p < n3; p++) {
+        double tmp = 1.0 / Q[3 * n3 + p];
+        U[p] = Q[p] * tmp;
+        U[n3 + p] = Q[n3 + p] * tmp;
+        U[2 * n3 + p] = Q[2 * n3 + p] * tmp;
+    }
+    double **G = c->grad;
+    orc_dfd(c, 1, 0, U + 2 * n3, G[G_DUZ_DY], 0, 1.0);
+    orc_dfd(c, 2, 0, U + n3, G[G_DUY_DZ], 0, 1.0);
+    for (size_t p = 0; p < n3; p++) Grad[p] = G[G_DUZ_DY][p] - G[G_DUY_DZ][p];
+    orc_dfd(c, 0, 0, U + 2 * n3, G[G_DUZ_DX], 0, 1.0);
+    orc_dfd(c, 2, 0, U, G[G_DUX_DZ], 0, 1.0);
+    for (size_t p = 0; p < n3; p++) Grad[n3 + p] = G[G_DUX_DZ][p] - G[G_DUZ_DX][p];
+    orc_dfd(c, 0, 0, U + n3, G[G_DUY_DX], 0, 1.0);
+    orc_dfd(c, 1, 0, U, G[G_DUX_DY], 0, 1.0);
+    for (size_t p = 0; p < n3; p++) Grad[2 * n3 + p] = G[G_DUY_DX][p] - G[G_DUX_DY][p];
+    orc_dfd(c, 0, 1, U, G[G_DUX_DX], 0, 1.0);
+    orc_dfd(c, 1, 1, U + n3, G[G_DUY_DY], 0, 1.0);
+    orc_dfd(c, 2, 1, U + 2 * n3, G[G_DUZ_DZ], 0, 1.0);
+    for (size_t p = 0; p < n3; p++) Grad[3 * n3 + p] = G[G_DUX_DX][p] + G[G_DUY_DY][p] + G[G_DUZ_DZ][p];
+    double mx = 0.0, sum = 0.0;
+    for (size_t p = 0; p < n3; p++) if (fabs(Grad[3 * n3 + p]) > mx) mx = fabs(Grad[3 * n3 + p]);
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++) {
+                size_t p = IX(c, j, k, i);
+                double w1 = Grad[p], w2 = Grad[n3 + p], w3 = Grad[2 * n3 + p];
+                sum = sum + (w1 * w1 + w2 * w2 + w3 * w3);
+            }
+    *maxdil = mx;
+    *enstrophy = 0.5 * sum / (double)(c->M[0] * c->M[1] * c->M[2]);
+    free(U);
+}
+
+/* N_avg src/header:14 (symmetry boundaries) */
+int orc_shell_count(const orc *c) { return c->M[0] / 2 + 10 * (c->M[0] / 128); }
+
+/* radius of cell (i,j,k) from the origin, IX = DBLE(II-1)
+ * (src/auxiliary_mf.f:289-300, pproc/pproc_mf.f:102-110) */
+static double cell_rad(const orc *c, int i, int j, int k) {
+    double IXd = (double)(i + 1) - 1.0, IYd = (double)(j + 1) - 1.0, IZd = (double)(k + 1) - 1.0;
+    return sqrt((IXd * c->DX) * (IXd * c->DX) + (IYd * c->DY) * (IYd * c->DY) + (IZd * c->DZ) * (IZd * c->DZ));
+}
+
+/* Compute_shell_avg src/auxiliary_mf.f:266-332: N_avg bins, the first three
+ * 2*DX*sqrt(3) wide and the rest DX*sqrt(3); empty bins divide 0 by 0 */
+static void shell_avg(const orc *c, const double *F, double *avg) {
+    const int na = orc_shell_count(c);
+    double *r = dalloc(na + 1), *s = dalloc(na);
+    long *cnt = (long *)calloc(na, sizeof(long));
+    r[0] = 0.0;
+    for (int M = 2; M <= na + 1; M++)
+        r[M - 1] = r[M - 2] + (M <= 4 ? c->DX * 2.0 * sqrt(3.0) : c->DX * sqrt(3.0));
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++) {
+                double rad = cell_rad(c, i, j, k);
+                for (int M = 0; M < na; M++)
+                    if (rad >= r[M] && rad < r[M + 1]) { s[M] = s[M] + F[IX(c, j, k, i)]; cnt[M]++; }
+            }
+    for (int M = 0; M < na; M++) avg[M] = s[M] / (double)cnt[M];
+    free(r); free(s); free(cnt);
+}
+
+/* Compute_SRM_Stats pproc/pproc_mf.f:4-186: radial velocity Ur, its shell
+ * average and that of Y, tke = |u_t|^2 + (Ur - <Ur>)^2 summed over the cells
+ * that fall in one of its (uniform, DX*sqrt(3)) bins, and the mixing width
+ * hmix = sum 8<Y>(1-<Y>)DX*sqrt(3) over bins with 0 < <Y> < 1.  Cells beyond
+ * the last bin leave tke unassigned in the reference (a local array); here
+ * they contribute 0. */
+void orc_compute_srm_stats(orc *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg) {
+    const size_t n3 = c->n3;
+    const int na = orc_shell_count(c);
+    const double *Q = c->Q;
+    double *U = dalloc(3 * n3), *Ur = dalloc(n3), *rad = dalloc(n3);
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++) {
+                size_t p = IX(c, j, k, i);
+                double tmp = 1.0 / Q[3 * n3 + p];
+                U[p] = Q[p] * tmp; U[n3 + p] = Q[n3 + p] * tmp; U[2 * n3 + p] = Q[2 * n3 + p] * tmp;
+                rad[p] = cell_rad(c, i, j, k);
+                if (i == 0 && j == 0 && k == 0) Ur[p] = 0.0;
+                else Ur[p] = (gcor(c, 0, i) / rad[p]) * U[p] + (gcor(c, 1, j) / rad[p]) * U[n3 + p] +
+                             (gcor(c, 2, k) / rad[p]) * U[2 * n3 + p];
+            }
+    double *ura = dalloc(na), *ya = dalloc(na), *r = dalloc(na + 1);
+    shell_avg(c, Ur, ura);
+    shell_avg(c, c->Y, ya);
+    r[0] = 0.0;
+    for (int M = 2; M <= na + 1; M++) r[M - 1] = r[M - 2] + c->DX * sqrt(3.0);
+    double tke = 0.0;
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++) {
+                size_t p = IX(c, j, k, i);
+                double t = 0.0;
+                for (int M = 0; M < na; M++)
+                    if (rad[p] >= r[M] && rad[p] < r[M + 1]) {
+                        double d = Ur[p] - ura[M];
+                        double urp2 = d * d, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+                        if (i > 0 && j > 0 && k > 0) {
+                            double IXd = (double)(i + 1) - 1.0, IYd = (double)(j + 1) - 1.0, IZd = (double)(k + 1) - 1.0;
+                            t1 = U[p] - Ur[p] * (IXd * c->DX / rad[p]);
+                            t2 = U[n3 + p] - Ur[p] * (IYd * c->DY / rad[p]);
+                            t3 = U[2 * n3 + p] - Ur[p] * (IZd * c->DZ / rad[p]);
+                        }
+                        double utp2 = t1 * t1 + t2 * t2 + t3 * t3;
+                        t = utp2 + urp2;
+                    }
+                tke = tke + t;
+            }
+    *tke_total = tke / (double)(c->M[0] * c->M[1] * c->M[2]);
+    double h = 0.0;
+    for (int M = 0; M < na; M++)
+        if (ya[M] > 0.0 && ya[M] < 1.0) h = h + 8.0 * ya[M] * (1.0 - ya[M]) * c->DX * sqrt(3.0);
+    *hmix = h;
+    if (ur_avg) memcpy(ur_avg, ura, na * sizeof(double));
+    if (y_avg) memcpy(y_avg, ya, na * sizeof(double));
+    free(U); free(Ur); free(rad); free(ura); free(ya); free(r);
+}
+
+/* Generate_Shock_Surface src/shock.f:163-260: cells with beta_hyper above
+ * 0.1*max(beta_hyper) form the shock; their centroid, mean distance from it
+ * and sqrt(sum (rad - rad_avg)^2)/(n*rad_avg) */
+void orc_shock_surface(orc *c, double *rad_avg, double *rad_skew_rms) {
+    const double *b = c->hyp[H_BETA];
+    double bmax = -INFINITY;
+    for (size_t p = 0; p < c->n3; p++) if (b[p] > bmax) bmax = b[p];
+    const double thr = 0.1 * bmax;
+    double xc = 0.0, yc = 0.0, zc = 0.0, n = 0.0;
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++)
+                if (b[IX(c, j, k, i)] > thr) {
+                    xc = xc + gcor(c, 0, i); yc = yc + gcor(c, 1, j); zc = zc + gcor(c, 2, k); n = n + 1.0;
+                }
+    xc = xc / n; yc = yc / n; zc = zc / n;
+    double rs = 0.0;
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++)
+                if (b[IX(c, j, k, i)] > thr) {
+                    double dx = gcor(c, 0, i) - xc, dy = gcor(c, 1, j) - yc, dz = gcor(c, 2, k) - zc;
+                    rs = rs + sqrt(dx * dx + dy * dy + dz * dz);
+                }
+    const double ra = rs / n;
+    double sk = 0.0;
+    for (int i = 0; i < c->M[0]; i++)
+        for (int j = 0; j < c->M[1]; j++)
+            for (int k = 0; k < c->M[2]; k++)
+                if (b[IX(c, j, k, i)] > thr) {
+                    double dx = gcor(c, 0, i) - xc, dy = gcor(c, 1, j) - yc, dz = gcor(c, 2, k) - zc;
+                    double d = sqrt(dx * dx + dy * dy + dz * dz) - ra;
+                    sk = sk + d * d;
+                }
+    *rad_avg = ra;
+    *rad_skew_rms = sqrt(sk) / (n * ra);
+}

@@ -67,6 +67,11 @@ double orc_compute_tstep(orc *c, const double *Q, const double *Y, double cfl_re
 void orc_lddrk4(orc *c, double *time, int *step);
 void orc_step(orc *c, double *time, int *step);
 void orc_get_monitors(orc *c, double out[10]);
+/* Output-side diagnostics: Compute_Grad, Compute_SRM_Stats, Generate_Shock_Surface */
+void orc_compute_grad(orc *c, double *Grad, double *maxdil, double *enstrophy);
+int  orc_shell_count(const orc *c);
+void orc_compute_srm_stats(orc *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg);
+void orc_shock_surface(orc *c, double *rad_avg, double *rad_skew_rms);
 
 /* 1-D spherical-radial family (st_oracle_radial.c).  Q = (u_r, rho, s)
  * with s = P/rho^gamma, n points each; hyp = (beta_hyper, visc_hyper). */

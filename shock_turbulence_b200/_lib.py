@@ -44,6 +44,10 @@ SIGNATURES = {
     "st_lddrk4": [_ctx, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
     "st_step": [_ctx, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
     "st_get_monitors": [_ctx, _dp],
+    "st_compute_grad": [_ctx, _dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+    "st_shell_count": [_ctx, ctypes.POINTER(ctypes.c_int)],
+    "st_compute_srm_stats": [_ctx] + [ctypes.POINTER(ctypes.c_double)] * 4,
+    "st_generate_shock_surface": [_ctx] + [ctypes.POINTER(ctypes.c_double)] * 2,
     "st_sync": [_ctx],
     "st_step_async": [_ctx, ctypes.c_int],
     "st_get_time": [_ctx, ctypes.POINTER(ctypes.c_double)],

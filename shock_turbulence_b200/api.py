@@ -197,6 +197,36 @@ class Solver:
             self._check(st, "st_query")
         return st == 1
 
+    # -- Output-side diagnostics (src/out_mf.f:671-705) ---------------------
+    def Compute_Grad(self, Grad=None):
+        """Compute_Grad (src/grad_sym.f:13): returns (Grad, MaxDil, Enstrophy),
+        Grad = (w_x, w_y, w_z, dilatation) of the context's state."""
+        Grad = self.field(4) if Grad is None else Grad
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.st_compute_grad(self._h, self._a(Grad, 4), ctypes.byref(a), ctypes.byref(b)),
+                    "Compute_Grad")
+        return Grad, a.value, b.value
+
+    def Compute_SRM_Stats(self):
+        """Compute_SRM_Stats (pproc/pproc_mf.f:4): returns (hmix, tke_total,
+        shell-averaged radial velocity, shell-averaged Y)."""
+        na = ctypes.c_int()
+        self._check(self.lib.st_shell_count(self._h, ctypes.byref(na)), "st_shell_count")
+        ur, ya = np.zeros(na.value), np.zeros(na.value)
+        h, t = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.st_compute_srm_stats(self._h, ctypes.byref(h), ctypes.byref(t),
+                                                  ur.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  ya.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                    "Compute_SRM_Stats")
+        return h.value, t.value, ur, ya
+
+    def Generate_Shock_Surface(self):
+        """Generate_Shock_Surface (src/shock.f:163): returns (rad_avg, rad_skew_rms)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.st_generate_shock_surface(self._h, ctypes.byref(a), ctypes.byref(b)),
+                    "Generate_Shock_Surface")
+        return a.value, b.value
+
     def monitors(self):
         out = np.zeros(10)
         self._check(self.lib.st_get_monitors(self._h, out.ctypes.data), "st_get_monitors")

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libst_b200.so")
 SOURCES = ["st_kernels.cu", "st_kernels_cyc.cu", "st_kernels_f32.cu", "st_kernels_cyc_f32.cu", "st_physics.cu",
-           "st_radial.cu", "st_noalloc.cu", "st_tables.cpp", "st_api.cpp"]
+           "st_radial.cu", "st_noalloc.cu", "st_diag.cu", "st_tables.cpp", "st_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "--extended-lambda", "-std=c++17",
                      "-Xcompiler", "-fPIC"]

@@ -853,6 +853,42 @@ int st_profile_report(st_ctx *c, char *buf, int buflen) {
     API_END(c)
 }
 
+// ---- Output-side diagnostics -------------------------------------------------
+int st_compute_grad(st_ctx *c, double *Grad, double *maxdil, double *enstrophy) {
+    if (!maxdil || !enstrophy) return ST_E_ARG;
+    MF_ONLY(c, "Compute_Grad");
+    API_BEGIN(c)
+    Args a(c);
+    double *Gd = Grad ? a.map(Grad, 4, false, true) : nullptr;
+    ST_TRY(dev_compute_grad(c, Gd, maxdil, enstrophy));
+    return a.finish();
+    API_END(c)
+}
+
+int st_shell_count(st_ctx *c, int *n_avg) {
+    if (!c || !n_avg) return ST_E_ARG;
+    *n_avg = shell_count(c);
+    return ST_OK;
+}
+
+int st_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg) {
+    if (!hmix || !tke_total) return ST_E_ARG;
+    MF_ONLY(c, "Compute_SRM_Stats");
+    API_BEGIN(c)
+    ST_TRY(dev_compute_srm_stats(c, hmix, tke_total, ur_avg, y_avg));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms) {
+    if (!rad_avg || !rad_skew_rms) return ST_E_ARG;
+    MF_ONLY(c, "Generate_Shock_Surface");
+    API_BEGIN(c)
+    ST_TRY(dev_shock_surface(c, rad_avg, rad_skew_rms));
+    return ST_OK;
+    API_END(c)
+}
+
 int st_get_monitors(st_ctx *c, double out[10]) {
     if (!out) return ST_E_ARG;
     API_BEGIN(c)

@@ -250,4 +250,10 @@ int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, boo
 int dev_lddrk4(st_ctx *c, bool dt_on_device);
 int dev_monitors(st_ctx *c);
 
+// Output-side diagnostics (st_diag.cu)
+int shell_count(const st_ctx *c);
+int dev_compute_grad(st_ctx *c, double *Grad, double *maxdil, double *enstrophy);
+int dev_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg);
+int dev_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms);
+
 }  // namespace st
