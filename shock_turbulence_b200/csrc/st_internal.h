@@ -16,6 +16,7 @@ namespace st {
 
 constexpr int kMaxSeg = 32;       // max segments per line (warps per CTA)
 constexpr int kLanes = 16;        // lines per CTA (half a warp; a warp holds two segments)
+constexpr int kScanSteps = 5;     // log2(kMaxSeg): steps of a scan over the segments
 
 // A line of n rows is split into P = n/S segments of S rows; thread t of a CTA
 // works on line t%16 and segment t/16 of 16 neighbouring lines, so a warp
@@ -62,6 +63,11 @@ struct PenTab {
     // the constants below (the factorisation's interior fixed point)
     int slo, shi;
     double cp1, cp2, cq1, cq2, cid;
+    // Scan factors [kScanSteps][kMaxSeg][4]: products of 2^k consecutive
+    // segment transfer matrices, sf[k][s] = M_s M_{s-1} ... M_{s-2^k+1}
+    // (M_s: response of segment s's last two forward values to its carry-in)
+    // and sb[k][s] = N_s ... N_{s+2^k-1} (N_s: of its first two backward values)
+    const double *sf, *sb;
 };
 
 enum TriKind { K_D1S = 0, K_D1A = 1, K_D2S = 2, K_D2A = 3 };

@@ -285,17 +285,30 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
             r[t] = v;
         }
     }
-    cb.a[s][lane][0] = r[S - 1];
-    cb.a[s][lane][1] = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
+    // carry into segment s: c(s) = f(s-1) of the inclusive scan
+    // f(s) = a(s) + M_s f(s-1) over the segments' end values a(s), in
+    // log2(P) steps over a double buffer (the reach of the carries, up to the
+    // whole line for this nearly singular system, costs every segment the
+    // same)
+    double f1 = r[S - 1], f2 = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
+    double(*cur)[kLanes][2] = cb.a;
+    double(*nxt)[kLanes][2] = cb.b;
+    cur[s][lane][0] = f1;
+    cur[s][lane][1] = f2;
     __syncthreads();
-    double c1 = 0.0, c2 = 0.0;
-#pragma unroll 4
-    for (int sp = max(0, s - T.kf); sp < s; sp++) {
-        const double *m = T.mf + ((size_t)sp * P + s) * 4;
-        double a1 = cb.a[sp][lane][0], a2 = cb.a[sp][lane][1];
-        c1 = fma(__ldg(m + 0), a1, fma(__ldg(m + 1), a2, c1));
-        c2 = fma(__ldg(m + 2), a1, fma(__ldg(m + 3), a2, c2));
+    for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+        if (s >= d) {
+            const double *m = T.sf + ((size_t)k * kMaxSeg + s) * 4;
+            const double o1 = cur[s - d][lane][0], o2 = cur[s - d][lane][1];
+            f1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, f1));
+            f2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, f2));
+        }
+        nxt[s][lane][0] = f1;
+        nxt[s][lane][1] = f2;
+        __syncthreads();
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
     }
+    const double c1 = s > 0 ? cur[s - 1][lane][0] : 0.0, c2 = s > 0 ? cur[s - 1][lane][1] : 0.0;
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g1 + a + t), c1, fma(__ldg(T.g2 + a + t), c2, r[t]));
     if (flat) {
@@ -316,17 +329,28 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
             r[t] = v * __ldg(T.id + a + t);
         }
     }
-    cb.b[s][lane][0] = r[0];
-    cb.b[s][lane][1] = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
-    __syncthreads();
-    double e1 = 0.0, e2 = 0.0;
-#pragma unroll 4
-    for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++) {
-        const double *m = T.mb + ((size_t)sp * P + s) * 4;
-        double b1 = cb.b[sp][lane][0], b2 = cb.b[sp][lane][1];
-        e1 = fma(__ldg(m + 0), b1, fma(__ldg(m + 1), b2, e1));
-        e2 = fma(__ldg(m + 2), b1, fma(__ldg(m + 3), b2, e2));
+    // carry from the right: e(s) = g(s+1) of g(s) = b(s) + N_s g(s+1); the
+    // first write goes to the buffer nobody reads after the forward scan
+    double g1 = r[0], g2 = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
+    nxt[s][lane][0] = g1;
+    nxt[s][lane][1] = g2;
+    {
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
     }
+    __syncthreads();
+    for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+        if (s + d < P) {
+            const double *m = T.sb + ((size_t)k * kMaxSeg + s) * 4;
+            const double o1 = cur[s + d][lane][0], o2 = cur[s + d][lane][1];
+            g1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, g1));
+            g2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, g2));
+        }
+        nxt[s][lane][0] = g1;
+        nxt[s][lane][1] = g2;
+        __syncthreads();
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+    }
+    const double e1 = s + 1 < P ? cur[s + 1][lane][0] : 0.0, e2 = s + 1 < P ? cur[s + 1][lane][1] : 0.0;
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.h1 + a + t), e1, fma(__ldg(T.h2 + a + t), e2, r[t]));
 }

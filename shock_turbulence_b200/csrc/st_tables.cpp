@@ -207,7 +207,7 @@ struct TriHost {
     int slo = 0, shi = 0;
 };
 struct PenHost {
-    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mf, mb;
+    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mf, mb, sf, sb;
     int kf = 0, kb = 0;
     int slo = 0, shi = 0;
 };
@@ -353,6 +353,24 @@ static PenHost pen_tables(std::vector<double> M[5], int n, int S) {
             nn[0] = t.h1[a0]; nn[1] = t.h2[a0]; nn[2] = 1.0; nn[3] = 0.0;
         }
     }
+    // scan factors: T_0(s) = M_s, T_{k+1}(s) = T_k(s) T_k(s-2^k);
+    // U_0(s) = N_s, U_{k+1}(s) = U_k(s) U_k(s+2^k); entries whose span leaves
+    // [0, P) stay 0 (never read)
+    t.sf.assign((size_t)kScanSteps * kMaxSeg * 4, 0.0);
+    t.sb.assign((size_t)kScanSteps * kMaxSeg * 4, 0.0);
+    for (int s = 0; s < P; s++) {
+        std::memcpy(&t.sf[(size_t)s * 4], &Mseg[s * 4], 32);
+        std::memcpy(&t.sb[(size_t)s * 4], &Nseg[s * 4], 32);
+    }
+    for (int k = 1, d = 1; k < kScanSteps; k++, d <<= 1)
+        for (int s = 0; s < P; s++) {
+            if (s - d >= 0)
+                mat2mul(&t.sf[((size_t)(k - 1) * kMaxSeg + s) * 4], &t.sf[((size_t)(k - 1) * kMaxSeg + s - d) * 4],
+                        &t.sf[((size_t)k * kMaxSeg + s) * 4]);
+            if (s + d < P)
+                mat2mul(&t.sb[((size_t)(k - 1) * kMaxSeg + s) * 4], &t.sb[((size_t)(k - 1) * kMaxSeg + s + d) * 4],
+                        &t.sb[((size_t)k * kMaxSeg + s) * 4]);
+        }
     // carry weights: C_s = sum_{s'<s} (M_{s-1} ... M_{s'+1}) A_{s'} (2x2 products)
     t.mf.assign((size_t)P * P * 4, 0.0); t.mb.assign((size_t)P * P * 4, 0.0);
     for (int s = 0; s < P; s++) {
@@ -448,6 +466,7 @@ static int build_tables_periodic(st_ctx *c) {
             t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
             t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
+            t.sf = upload(c, h.sf, &err); t.sb = upload(c, h.sb, &err);
             t.kf = h.kf; t.kb = h.kb;
             {
                 const int mid = n / 2;
@@ -482,6 +501,7 @@ int build_tables(st_ctx *c) {
             t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
             t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
+            t.sf = upload(c, h.sf, &err); t.sb = upload(c, h.sb, &err);
             t.kf = h.kf; t.kb = h.kb;
             {
                 const int mid = n / 2;
