@@ -148,9 +148,10 @@ template <int S, bool YT, bool CYC, class T>
 __global__ void __launch_bounds__(512, 2) k_filter(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
     double v[S + 8];
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
+    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
     rhs_filter<S, 4>(v, row0, n, a.asym, CYC, a.K, rd);
     pen_solve<S>(v, a.p, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 8, 4>(v, a.p.cyc, s, a.P, lane, cb);
