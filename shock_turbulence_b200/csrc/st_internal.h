@@ -43,6 +43,10 @@ struct TriTabT {
     // cid, which the solve then keeps in registers instead of loading per row.
     int slo, shi;
     A cl, cup, cid;
+    // scan factors [kScanSteps][kMaxSeg]: sf[k][s] = B_s B_{s-1} ... B_{s-2^k+1}
+    // (B_s: response of segment s's last forward value to its carry-in) and
+    // sb[k][s] = G_s ... G_{s+2^k-1} (G_s: of its first backward value)
+    const A *sf, *sb;
 };
 using TriTab = TriTabT<double>;
 

@@ -231,11 +231,32 @@ __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s,
 #pragma unroll
         for (int t = 1; t < S; t++) r[t] = r[t] - r[t - 1] * __ldg(T.l + a + t);
     }
-    cb.a[s][lane][0] = r[S - 1];
-    __syncthreads();
+    // Carries reaching more than twice as many segments as a scan has steps
+    // (short segments: small grids, n <= 128) come from a log2(P)-step scan
+    // over a double buffer: f(s) = a(s) + B_s f(s-1), carry into s =
+    // f(s-1); otherwise from the sum over the kf segments before s (measured
+    // faster for n >= 256).  The choice is uniform over the CTA.
+    const bool scan = T.kf > 2 * kScanSteps || T.kb > 2 * kScanSteps;
     V cin = V(0.0);
+    V(*cur)[kLanes][2] = cb.a;
+    V(*nxt)[kLanes][2] = cb.b;
+    if (scan) {
+        V f = r[S - 1];
+        cur[s][lane][0] = f;
+        __syncthreads();
+        for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+            if (s >= d) f = vfma(__ldg(T.sf + k * kMaxSeg + s), cur[s - d][lane][0], f);
+            nxt[s][lane][0] = f;
+            __syncthreads();
+            V(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+        }
+        if (s > 0) cin = cur[s - 1][lane][0];
+    } else {
+        cb.a[s][lane][0] = r[S - 1];
+        __syncthreads();
 #pragma unroll 4
-    for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
+        for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
+    }
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
     if (flat) {
@@ -248,12 +269,30 @@ __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s,
 #pragma unroll
         for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
     }
-    cb.b[s][lane][0] = r[0];
-    __syncthreads();
     V ein = V(0.0);
+    if (scan) {
+        // g(s) = b(s) + G_s g(s+1), carry from the right = g(s+1); the first
+        // write goes to the buffer nobody reads after the forward scan
+        V g = r[0];
+        nxt[s][lane][0] = g;
+        {
+            V(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+        }
+        __syncthreads();
+        for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+            if (s + d < P) g = vfma(__ldg(T.sb + k * kMaxSeg + s), cur[s + d][lane][0], g);
+            nxt[s][lane][0] = g;
+            __syncthreads();
+            V(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+        }
+        if (s + 1 < P) ein = cur[s + 1][lane][0];
+    } else {
+        cb.b[s][lane][0] = r[0];
+        __syncthreads();
 #pragma unroll 4
-    for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
-        ein = vfma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
+        for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
+            ein = vfma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
+    }
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.h + a + t), ein, r[t]);
 }

@@ -202,7 +202,7 @@ static std::vector<double> cyclic_correction(int n, double bt, double al, int k)
 
 // ---- tables ---------------------------------------------------------------
 struct TriHost {
-    std::vector<double> l, g, up, id, h, wf, wb;
+    std::vector<double> l, g, up, id, h, wf, wb, sf, sb;
     int kf = 0, kb = 0;
     int slo = 0, shi = 0;
 };
@@ -289,6 +289,16 @@ static TriHost tri_tables(const std::vector<double> &a, const std::vector<double
     t.kf = carry_span(t.wf, P, 1, true);
     t.kb = carry_span(t.wb, P, 1, false);
     flat_segments({&t.l, &t.up, &t.id}, n, S, &t.slo, &t.shi);
+    // scan factors: products of 2^k consecutive B ending at s and G starting
+    // at s; entries whose span leaves [0, P) stay 0 (never read)
+    t.sf.assign((size_t)kScanSteps * kMaxSeg, 0.0);
+    t.sb.assign((size_t)kScanSteps * kMaxSeg, 0.0);
+    for (int s = 0; s < P; s++) { t.sf[s] = B[s]; t.sb[s] = G[s]; }
+    for (int k = 1, d = 1; k < kScanSteps; k++, d <<= 1)
+        for (int s = 0; s < P; s++) {
+            if (s - d >= 0) t.sf[k * kMaxSeg + s] = t.sf[(k - 1) * kMaxSeg + s] * t.sf[(k - 1) * kMaxSeg + s - d];
+            if (s + d < P) t.sb[k * kMaxSeg + s] = t.sb[(k - 1) * kMaxSeg + s] * t.sb[(k - 1) * kMaxSeg + s + d];
+        }
     return t;
 }
 
@@ -418,6 +428,7 @@ static void upload_tri(st_ctx *c, st::TriTab &t, st::TriTabT<float> &tf, const T
     t.l = upload(c, h.l, err); t.g = upload(c, h.g, err); t.up = upload(c, h.up, err);
     t.id = upload(c, h.id, err); t.h = upload(c, h.h, err);
     t.wf = upload(c, h.wf, err); t.wb = upload(c, h.wb, err);
+    t.sf = upload(c, h.sf, err); t.sb = upload(c, h.sb, err);
     t.kf = h.kf; t.kb = h.kb;
     t.cyc = K ? upload(c, *K, err) : nullptr;
     const int mid = (int)h.l.size() / 2;
@@ -430,6 +441,7 @@ static void upload_tri(st_ctx *c, st::TriTab &t, st::TriTabT<float> &tf, const T
     tf.l = upload_f(c, h.l, err); tf.g = upload_f(c, h.g, err); tf.up = upload_f(c, h.up, err);
     tf.id = upload_f(c, h.id, err); tf.h = upload_f(c, h.h, err);
     tf.wf = upload_f(c, h.wf, err); tf.wb = upload_f(c, h.wb, err);
+    tf.sf = upload_f(c, h.sf, err); tf.sb = upload_f(c, h.sb, err);
     tf.kf = carry_span(h.wf, P, 1, true, 1e-12);
     tf.kb = carry_span(h.wb, P, 1, false, 1e-12);
     tf.cyc = K ? upload_f(c, *K, err) : nullptr;
