@@ -52,16 +52,13 @@ using TriTab = TriTabT<double>;
 
 // Same for the pentadiagonal systems of the compact filter
 // (pentadiagonal_serial, src/pentadiagonal.f90:319-374); carries are
-// 2-vectors and the carry tables hold 2x2 matrices.
+// 2-vectors, propagated across the segments by a scan with 2x2 factors.
 struct PenTab {
     const double *p1, *p2;   // forward multipliers of r'_{i-1}, r'_{i-2}
     const double *g1, *g2;   // forward carry responses (carry = (r'_{a-1}, r'_{a-2}))
     const double *q1, *q2;   // back-substitution coefficients of x_{i+1}, x_{i+2}
     const double *id;        // 1 / (C'_i + tiny)
     const double *h1, *h2;   // backward carry responses (carry = (x_{b+1}, x_{b+2}))
-    const double *mf;        // [P][P][4]
-    const double *mb;        // [P][P][4]
-    int kf, kb;              // segments back/ahead whose carry weight is >= 1e-20
     const double *cyc;       // periodic family: [n][4] corner correction, else null
     // segments slo <= s < shi: every row's p1, p2, q1, q2, id equal (bitwise)
     // the constants below (the factorisation's interior fixed point)

@@ -207,8 +207,7 @@ struct TriHost {
     int slo = 0, shi = 0;
 };
 struct PenHost {
-    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, mf, mb, sf, sb;
-    int kf = 0, kb = 0;
+    std::vector<double> p1, p2, g1, g2, q1, q2, id, h1, h2, sf, sb;
     int slo = 0, shi = 0;
 };
 
@@ -363,6 +362,7 @@ static PenHost pen_tables(std::vector<double> M[5], int n, int S) {
             nn[0] = t.h1[a0]; nn[1] = t.h2[a0]; nn[2] = 1.0; nn[3] = 0.0;
         }
     }
+    flat_segments({&t.p1, &t.p2, &t.q1, &t.q2, &t.id}, n, S, &t.slo, &t.shi);
     // scan factors: T_0(s) = M_s, T_{k+1}(s) = T_k(s) T_k(s-2^k);
     // U_0(s) = N_s, U_{k+1}(s) = U_k(s) U_k(s+2^k); entries whose span leaves
     // [0, P) stay 0 (never read)
@@ -381,23 +381,6 @@ static PenHost pen_tables(std::vector<double> M[5], int n, int S) {
                 mat2mul(&t.sb[((size_t)(k - 1) * kMaxSeg + s) * 4], &t.sb[((size_t)(k - 1) * kMaxSeg + s + d) * 4],
                         &t.sb[((size_t)k * kMaxSeg + s) * 4]);
         }
-    // carry weights: C_s = sum_{s'<s} (M_{s-1} ... M_{s'+1}) A_{s'} (2x2 products)
-    t.mf.assign((size_t)P * P * 4, 0.0); t.mb.assign((size_t)P * P * 4, 0.0);
-    for (int s = 0; s < P; s++) {
-        double w[4] = {1.0, 0.0, 0.0, 1.0};
-        for (int sp = s - 1; sp >= 0; sp--) {
-            std::memcpy(&t.mf[((size_t)sp * P + s) * 4], w, 32);
-            mat2mul(w, &Mseg[sp * 4], w);
-        }
-        double v[4] = {1.0, 0.0, 0.0, 1.0};
-        for (int sp = s + 1; sp < P; sp++) {
-            std::memcpy(&t.mb[((size_t)sp * P + s) * 4], v, 32);
-            mat2mul(v, &Nseg[sp * 4], v);
-        }
-    }
-    flat_segments({&t.p1, &t.p2, &t.q1, &t.q2, &t.id}, n, S, &t.slo, &t.shi);
-    t.kf = carry_span(t.mf, P, 4, true);
-    t.kb = carry_span(t.mb, P, 4, false);
     return t;
 }
 
@@ -477,9 +460,7 @@ static int build_tables_periodic(st_ctx *c) {
             t.g1 = upload(c, h.g1, &err); t.g2 = upload(c, h.g2, &err);
             t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
-            t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
             t.sf = upload(c, h.sf, &err); t.sb = upload(c, h.sb, &err);
-            t.kf = h.kf; t.kb = h.kb;
             {
                 const int mid = n / 2;
                 t.slo = h.slo; t.shi = h.shi;
@@ -512,9 +493,7 @@ int build_tables(st_ctx *c) {
             t.g1 = upload(c, h.g1, &err); t.g2 = upload(c, h.g2, &err);
             t.q1 = upload(c, h.q1, &err); t.q2 = upload(c, h.q2, &err);
             t.id = upload(c, h.id, &err); t.h1 = upload(c, h.h1, &err); t.h2 = upload(c, h.h2, &err);
-            t.mf = upload(c, h.mf, &err); t.mb = upload(c, h.mb, &err);
             t.sf = upload(c, h.sf, &err); t.sb = upload(c, h.sb, &err);
-            t.kf = h.kf; t.kb = h.kb;
             {
                 const int mid = n / 2;
                 t.slo = h.slo; t.shi = h.shi;
