@@ -1,4 +1,4 @@
-"""ctypes loader for the CPU oracle (TEST INFRASTRUCTURE: the checker).
+"""ctypes loader for the CPU oracle (TEST INFRASTRUCTURE: GPU results are checked against it).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
 this module.  It mirrors the reference routine names (``DFDX_sym`` ...) on

@@ -1,5 +1,5 @@
 /*
- * st_oracle.c - CPU oracle (TEST INFRASTRUCTURE, the checker; see
+ * st_oracle.c - CPU oracle (TEST INFRASTRUCTURE, GPU results are checked against it; see
  * st_oracle.h).  Plain-C restatement of the reference's two-species "_mf"
  * right-hand side and LDDRK4 path, keeping the reference's expression
  * evaluation order (Fortran left-to-right) so that it reproduces the

@@ -1,7 +1,7 @@
 /*
  * st_oracle.h - CPU oracle for the per-stage RHS / LDDRK4 path.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker: a plain-C restatement of
+ * TEST INFRASTRUCTURE ONLY: the GPU results are checked against this plain-C restatement of
  * the reference Fortran (two-species "_mf" family) used by tests/, by
  * __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  Nothing in
  * the product path links or calls it.

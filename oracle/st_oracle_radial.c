@@ -1,5 +1,5 @@
 /*
- * st_oracle_radial.c - CPU oracle (TEST INFRASTRUCTURE, the checker) for the
+ * st_oracle_radial.c - CPU oracle (TEST INFRASTRUCTURE: GPU results are checked against it) for the
  * 1-D spherical-radial single-fluid family: src/rhsv_radial.f,
  * src/derivCDopt6_radial.f, src/filters_nonperiodic.f (x passes),
  * src/hyper_radial.f and src/lddrk4_nonperiodic_sf.f, one problem being one
