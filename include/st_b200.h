@@ -146,9 +146,10 @@ int  st_pentadiagonal(st_ctx *c, const double *A, const double *B, const double 
                       const double *D, const double *E, double *R,
                       int n, int lot, int nper);
 /* No counterpart in the reference.  st_tridiagonal for callers that must not
- * allocate device memory (code running during stream capture, or code that owns
- * the device's memory through its own pool): the working copies of A and B live
- * in a fixed static device array instead of cudaMalloc'd buffers.
+ * allocate device memory (a host program that owns the device's memory through
+ * its own pool, or a time-critical loop where a cudaMalloc may block on the
+ * driver): the working copies of A and B live in a fixed static device array
+ * instead of cudaMalloc'd buffers.
  * n*lot <= 262144 (ST_E_ARG beyond); A, B, C, R must be device arrays of the
  * context's device (ST_E_ARG for host arrays).  The first call on a device
  * looks the array up (cudaGetSymbolAddress) and should come before any stream

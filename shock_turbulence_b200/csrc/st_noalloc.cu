@@ -4,11 +4,10 @@
 // st_tridiagonal needs two working copies of A and B (the reference's
 // tridiagonal_serial overwrites its coefficients, src/tridiagonal.f90:274-284).
 // It gets them from cudaMalloc/cudaMallocAsync, and it stages host arrays
-// through more device buffers.  Some callers cannot allow that: code that runs
-// while a CUDA stream is being captured (allocation calls are not legal there),
-// code that owns all device memory through its own pool and must not see a
-// second allocator touch the device, and code on a latency budget where an
-// allocation can block on the driver.  This entry point takes the working copies
+// through more device buffers.  Some callers cannot allow that: a host program
+// that owns all device memory through its own pool and must not see a second
+// allocator touch the device, and code on a latency budget where an allocation
+// can block on the driver and stall the device's other work.  This entry point takes the working copies
 // from a fixed array in the library's static device memory instead.
 //
 // Limits and rules:

@@ -1,0 +1,282 @@
+"""The benchmark sizes themselves: the 384^3 blast-in-turbulence octant and the
+512^3 periodic turbulence box, checked on the GPU through the C ABI.
+
+- Every line operator (DFD*, D2FD*2, Compact_Filter_*, Gaussian_Filter_*) in
+  every direction against the oracle at 384^3 (periodic ones at 512^3):
+  1e-12 normwise relative per call, as at the small sizes.
+- Compute_hyper, RHS and Hyper_RHS of the 384^3 blast state against the
+  oracle: 1e-10 for the artificial-viscosity fields, 1e-11 per RHS field.
+- Compute_CFL + Compute_Tstep of that state against the oracle: 1e-12.
+- Properties of whole LDDRK4 steps at full size, where the oracle would take
+  minutes per step: a step is deterministic (two runs give the same bits), the
+  periodic box conserves mass (sum of rho) to 1e-12 relative, and the FP32
+  mode stays within 1e-5 relative L2 of FP64 per field after 3 steps.
+
+Each test skips with its reason when the host lacks the memory the oracle
+needs at these sizes (about 40 GB for the 384^3 physics calls)."""
+import gc
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from shock_turbulence_b200.params import default_params
+
+pytestmark = pytest.mark.gpu
+
+N3D = 384
+NPER = 512
+GB = 1 << 30
+
+
+def need_host(gbytes):
+    import psutil
+    avail = psutil.virtual_memory().available
+    if avail < gbytes * GB:
+        pytest.skip(f"needs {gbytes} GB of free host memory for the oracle, {avail / GB:.0f} GB free")
+
+
+def need_device(gbytes):
+    import torch
+    free, _ = torch.cuda.mem_get_info(0)
+    if free < gbytes * GB:
+        pytest.skip(f"needs {gbytes} GB of free device memory, {free / GB:.0f} GB free")
+
+
+def blast_params(**kw):
+    return default_params(N3D, re=100.0, c_beta_scale=1.75, **kw)
+
+
+def blast_state(p):
+    from shock_turbulence_b200.initial import blast_in_turbulence
+    return blast_in_turbulence(p, k0=8, mach_t=0.1, p_ratio=100.0, radius_cells=4, seed=1)
+
+
+def field(shape, seed):
+    """Smooth field plus 5 % noise, so the closures and the interior both matter."""
+    nx, nz, ny = shape
+    x = np.linspace(0, 1, nx, dtype=np.float64)[:, None, None]
+    z = np.linspace(0, 1, nz, dtype=np.float64)[None, :, None]
+    y = np.linspace(0, 1, ny, dtype=np.float64)[None, None, :]
+    f = np.sin(3 * x + 1) * np.cos(2 * y) * np.exp(z)
+    f = f + 0.05 * np.random.default_rng(seed).standard_normal(shape)
+    return np.ascontiguousarray(f)
+
+
+@pytest.fixture(scope="module")
+def oracle_384(oracle_mod):
+    need_host(8)
+    return oracle_mod.Oracle(blast_params())
+
+
+@pytest.fixture(scope="module")
+def solver_384():
+    from shock_turbulence_b200 import Solver
+    need_device(60)
+    s = Solver(blast_params())
+    yield s
+    s.close()
+    gc.collect()
+
+
+DIRS = "XYZ"
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_line_operators_384(solver_384, oracle_384, d):
+    s, o = solver_384, oracle_384
+    F = field(s.shape, 100 + d)
+    # DFD*_sym, iadd = 0
+    g, r = np.zeros(s.shape), np.zeros(s.shape)
+    getattr(s, f"DFD{DIRS[d]}_sym")(F, g, 0, 1.0)
+    o.dfd(d, 0, F, r, 0, 1.0)
+    assert rel_err(g, r) < 1e-12
+    # DFD*_asym, iadd = 1 onto a non-zero dF
+    base = field(s.shape, 200 + d)
+    g, r = base.copy(), base
+    getattr(s, f"DFD{DIRS[d]}_asym")(F, g, 1, -0.5)
+    o.dfd(d, 1, F, r, 1, -0.5)
+    assert rel_err(g, r) < 1e-12
+    del base
+    # D2FD*2_asym with iadd = 1 (first and second derivative)
+    g2, r2 = np.zeros(s.shape), np.zeros(s.shape)
+    getattr(s, f"D2FD{DIRS[d]}2_asym")(F, g, g2, 1)
+    o.d2fd2(d, 1, F, r, r2, 1)
+    assert rel_err(g, r) < 1e-12
+    assert rel_err(g2, r2) < 1e-12
+    del g2, r2
+    # Compact_Filter_*_sym out of place, _asym in place (F0 aliasing F)
+    getattr(s, f"Compact_Filter_{DIRS[d]}_sym")(F, g)
+    o.filter(d, 0, F, r)
+    assert rel_err(g, r) < 1e-12
+    g = F.copy()
+    getattr(s, f"Compact_Filter_{DIRS[d]}_asym")(g, g)
+    o.filter(d, 1, F, r)
+    assert rel_err(g, r) < 1e-12
+    # Gaussian_Filter_*
+    getattr(s, f"Gaussian_Filter_{DIRS[d]}")(F, g)
+    o.gauss(d, F, r)
+    assert rel_err(g, r) < 1e-12
+
+
+@pytest.fixture(scope="module")
+def blast_pair(solver_384, oracle_mod):
+    need_host(60)
+    s = solver_384
+    o = oracle_mod.Oracle(blast_params())
+    Q, Y = blast_state(s.params)
+    for h in (s, o):
+        h.set_state(Q, Y)
+    s.Compute_gamma(Y)
+    o.compute_gamma(Y)
+    yield s, o, Q, Y
+    del o
+    gc.collect()
+
+
+HYPER = ["beta_hyper", "visc_hyper", "k_hyper", "D_hyper"]
+
+
+def test_compute_hyper_384(blast_pair):
+    s, o, Q, Y = blast_pair
+    s.Compute_hyper(Q, Y)
+    o.compute_hyper(Q, Y)
+    for k in HYPER:
+        assert rel_err(s.get_common(k), o.get_common(k)) < 1e-10, k
+
+
+def test_rhs_and_hyper_rhs_384(blast_pair):
+    s, o, Q, Y = blast_pair
+    Qg, Qo = Q.copy(), Q.copy()
+    Rg, Ro = np.zeros_like(Q), np.zeros_like(Q)
+    s.RHS(Qg, Rg, Y)
+    o.rhs(Qo, Ro, Y)
+    for l in range(5):
+        assert rel_err(Rg[l], Ro[l]) < 1e-11, ("RHS", l)
+    s.Hyper_RHS(Qg, Rg, Y)
+    o.hyper_rhs(Qo, Ro, Y)
+    for l in range(5):
+        assert rel_err(Rg[l], Ro[l]) < 1e-11, ("Hyper_RHS", l)
+
+
+def test_cfl_and_tstep_384(blast_pair):
+    s, o, Q, Y = blast_pair
+    s.set_state(Q, Y)
+    o.set_state(Q, Y)
+    s.Compute_hyper(Q, Y)
+    o.compute_hyper(Q, Y)
+    cg = s.Compute_CFL(Q)                    # (cfl_stab, cfl_resv)
+    co = o.compute_cfl(Q)
+    for a, b in zip(cg, co):
+        assert abs(a - b) <= 1e-12 * abs(b)
+    for step in (0, 3):                      # without and with the hyperviscous limits
+        tg = s.Compute_Tstep(Q, Y, cg[1], step)
+        to = o.compute_tstep(Q, Y, co[1], step)
+        assert abs(tg - to) <= 1e-12 * abs(to), step
+
+
+def test_step_is_deterministic_384(blast_pair):
+    s, _, Q, Y = blast_pair
+    out = []
+    for _ in range(2):
+        s.set_state(Q, Y)
+        s.Compute_gamma(Y)
+        s.Compute_hyper(Q, Y)
+        t, k = s.step(0.0, 0)
+        Qs, Ys = s.get_state()
+        assert np.isfinite(Qs).all() and np.isfinite(Ys).all()
+        out.append((t, k, Qs, Ys))
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][3], out[1][3])
+
+
+def test_fp32_error_384(solver_384):
+    """FP32 intermediates against the FP64 path after 3 steps of the 384^3
+    blast: relative L2 <= 1e-5 and relative Linf <= 1e-4 per conserved field."""
+    from shock_turbulence_b200 import PRECISION_FP32, Solver
+    need_device(40)
+    p32 = blast_params(precision=PRECISION_FP32)
+    Q, Y = blast_state(p32)
+    res = []
+    for s in (solver_384, None):
+        own = s is None
+        if own:
+            s = Solver(p32)
+        s.set_state(Q, Y)
+        s.Compute_gamma(Y)
+        s.Compute_hyper(Q, Y)
+        t = 0.0
+        for k in range(3):
+            t, _ = s.step(t, k)
+        res.append(s.get_state())
+        if own:
+            s.close()
+            del s
+            gc.collect()
+    (Q64, Y64), (Q32, Y32) = res
+    fields = [Q64[l] for l in range(5)] + [Y64]
+    got = [Q32[l] for l in range(5)] + [Y32]
+    for i, (a, b) in enumerate(zip(got, fields)):
+        l2 = float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+        assert l2 <= 1e-5, (i, l2)
+        assert rel_err(a, b) <= 1e-4, i
+
+
+@pytest.fixture(scope="module")
+def periodic_solver(solver_384):
+    from shock_turbulence_b200 import Solver, periodic_params
+    solver_384.close()                       # the 512^3 FP64 box needs most of the device
+    gc.collect()
+    need_device(120)
+    s = Solver(periodic_params(NPER))
+    yield s
+    s.close()
+    gc.collect()
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_periodic_line_operators_512(periodic_solver, oracle_mod, d):
+    from shock_turbulence_b200 import periodic_params
+    need_host(12)
+    s = periodic_solver
+    o = oracle_mod.Oracle(periodic_params(NPER))
+    F = np.random.default_rng(300 + d).standard_normal(s.shape)
+    g, r = np.zeros(s.shape), np.zeros(s.shape)
+    getattr(s, "DFD" + DIRS[d])(F, g, 0, 1.0)
+    o.dfd(d, 0, F, r, 0, 1.0)
+    assert rel_err(g, r) < 1e-12
+    getattr(s, "Compact_Filter_" + DIRS[d])(F, g)
+    o.filter(d, 0, F, r)
+    assert rel_err(g, r) < 1e-12
+
+
+def test_periodic_mass_conservation_512(periodic_solver):
+    """Cyclic compact derivatives of a flux sum to zero over a periodic line and
+    the filter's transfer function is 1 at k = 0, so a step leaves the sum of
+    rho unchanged up to rounding."""
+    need_host(24)
+    s = periodic_solver
+    nx, nz, ny = s.shape
+    x = (np.arange(nx) * 2 * np.pi / nx)[:, None, None]
+    z = (np.arange(nz) * 2 * np.pi / nz)[None, :, None]
+    y = (np.arange(ny) * 2 * np.pi / ny)[None, None, :]
+    g = 1.4
+    rho = 1.0 + 0.05 * np.sin(x + 2 * y) * np.cos(3 * z)
+    u = 0.1 * np.sin(x) * np.cos(y) * np.cos(z)
+    v = -0.1 * np.cos(x) * np.sin(y) * np.cos(z)
+    w = 0.02 * np.sin(2 * z + 1.0) * np.ones_like(x)
+    Q = np.empty((5, nx, nz, ny))
+    Q[0], Q[1], Q[2], Q[3] = rho * u, rho * v, rho * w, rho
+    Q[4] = 1.0 / (g * (g - 1.0)) + 0.5 * rho * (u * u + v * v + w * w)
+    del rho, u, v, w
+    s.set_state(Q, None)
+    s.Compute_hyper(Q, None)
+    m0 = float(Q[3].sum())
+    t = 0.0
+    for k in range(2):
+        t, _ = s.step(t, k)
+    Qs, _ = s.get_state()
+    assert np.isfinite(Qs).all()
+    assert abs(float(Qs[3].sum()) - m0) <= 1e-12 * m0
+    assert not np.array_equal(Qs[3], Q[3])   # the step did change the density field
