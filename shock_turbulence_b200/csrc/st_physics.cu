@@ -17,11 +17,13 @@ __global__ void k_pfor(size_t n, Fn fn) {
         fn(p);
 }
 // site: "k_pointwise@<source line>" for the per-launch timing report
+// bpe: algorithmic bytes per element (every array element the launch reads
+// or writes, once; an element both read and written counts twice)
 template <class Fn>
-static int pfor(st_ctx *c, size_t n, const char *site, Fn fn) {
+static int pfor(st_ctx *c, size_t n, const char *site, double bpe, Fn fn) {
     size_t blocks = (n + 255) / 256;    // one element per thread
     if (blocks == 0) return ST_OK;
-    int pi = prof_start(c, site, 0.0);
+    int pi = prof_start(c, site, bpe * (double)n);
     k_pfor<<<(unsigned)blocks, 256, 0, c->stream>>>(n, fn);
     prof_stop(c, pi);
     ST_CUDA(c, cudaGetLastError());
@@ -29,8 +31,12 @@ static int pfor(st_ctx *c, size_t n, const char *site, Fn fn) {
 }
 #define ST_STR2(x) #x
 #define ST_STR(x) ST_STR2(x)
-#define PFOR(c, n, ...) \
-    ST_TRY(pfor((c), (n), "k_pointwise@" ST_STR(__LINE__), [=] __device__(size_t p) __VA_ARGS__))
+#define PFOR(c, n, bpe, ...) \
+    ST_TRY(pfor((c), (n), "k_pointwise@" ST_STR(__LINE__), (bpe), [=] __device__(size_t p) __VA_ARGS__))
+// bytes of one element of each listed array (its element type's size), for
+// the algorithmic byte count of a pointwise launch
+template <class... P>
+static constexpr double io(const P *...) { return (0.0 + ... + (double)sizeof(P)); }
 
 // producer expressions evaluated by the derivative kernels while loading
 template <class R>
@@ -142,22 +148,22 @@ struct ScratchNT {
 };
 
 int dev_fill(st_ctx *c, double *x, size_t n, double v) {
-    PFOR(c, n, { x[p] = v; });
+    PFOR(c, n, io(x), { x[p] = v; });
     return ST_OK;
 }
 int dev_to_float(st_ctx *c, const double *x, float *y, size_t n) {
-    PFOR(c, n, { y[p] = (float)x[p]; });
+    PFOR(c, n, io(x, y), { y[p] = (float)x[p]; });
     return ST_OK;
 }
 int dev_to_double(st_ctx *c, const float *x, double *y, size_t n) {
-    PFOR(c, n, { y[p] = (double)x[p]; });
+    PFOR(c, n, io(x, y), { y[p] = (double)x[p]; });
     return ST_OK;
 }
 
 int dev_compute_gamma(st_ctx *c, const double *Y) {
     Phys f = phys(c);
     double *ge = c->gamma_eff;
-    PFOR(c, c->dm.n3, {
+    PFOR(c, c->dm.n3, io(Y, ge), {
         double fac1 = f.g1 - 1.0, fac2 = f.g2 - 1.0;
         double num = (Y[p] * f.g1 / fac1) + (f.eps * (1.0 - Y[p]) * f.g2 / fac2);
         double den = (Y[p] / fac1) + (f.eps * (1.0 - Y[p]) / fac2);
@@ -210,7 +216,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     // ---- RHS_x (src/rhsv_sym_mf.f:37-481)
     // P, T, u, and (the same expressions the reference evaluates later from
     // the same inputs) v, w, mu, dmu/dT
-    PFOR(c, n3, {
+    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, P, T, u, v, w, mu, dmu), {
         double vs, pp, tt, m, dm;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], vs, pp, tt);
         P[p] = pp; T[p] = tt;
@@ -244,7 +250,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     // and the x part of Qvisc, in the reference's order of accumulation
     {
         const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
-        PFOR(c, n3, {
+        PFOR(c, n3, io(FF, u, v, w, Q4, Gxx, Gyx, Gzx) + 6 * io(Qcx) + (visc ? io(mu, dTx, dmu, GTx, duxx, dvxx, dwxx) + 4 * io(Qv) : 0.0), {
             double fac2 = -5.0e-1 * FF[p];
             double c1 = Qcx[p] + fac2 * u[p];
             double c2 = Qcx[n3 + p] + fac2 * v[p];
@@ -320,7 +326,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
         const double Pri = f.Pr_inv;
         const double fb43 = f.bulk + 4.0 / 3.0, fb23 = f.bulk - 2.0 / 3.0, fb13 = f.bulk + 1.0 / 3.0;
         const bool fp64 = is_fp64<R>();
-        PFOR(c, n3, {
+        PFOR(c, n3, io(u, v, w, Q4, Gxx, Gyx, Gzx, Gxy, Gyy, Gzy, Gxz, Gyz, Gzz) + 5 * io(Qcx, Qcy, Qcz, Qrhs) + (fp64 ? io(Q1, Q2, Q3) : 0.0) + (visc ? io(mu, dmu, d2Ty, d2Tz, GTy, GTz, GTx, d2uy, d2vy, d2wy, dGzz_y, d2wz, d2uz, d2vz, dGyx_y, dGzx_z, dGxx_y, dGxx_z, dGyz_y) + 4 * io(Qv) : 0.0), {
             const double uu = u[p], vv = v[p], ww = w[p], q4 = Q4[p];
             // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
             double fac2 = -5.0e-1 * (-(double)Qcy[3 * n3 + p]);
@@ -460,7 +466,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     ScratchNT<R> s(c, 14);
     R *U1 = s[0], *U2 = s[1], *U3 = s[2], *W1 = s[3], *W2 = s[4], *W3 = s[5], *Dl = s[6];
     R *Cbeta = s[7], *S = s[8], *e = s[9], *T = s[10], *d2 = s[11], *d4S = s[12], *d4e = s[13];
-    PFOR(c, n3, {
+    PFOR(c, n3, io(Q1, Q2, Q3, Q4, U1, U2, U3), {
         double t = 1.0 / Q4[p];
         U1[p] = Q1[p] * t; U2[p] = Q2[p] * t; U3[p] = Q3[p] * t;
     });
@@ -478,7 +484,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
             *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
     R *P = U1, *Vs = U2;   // the velocities are dead from here on
-    PFOR(c, n3, {
+    PFOR(c, n3, io(Dl, W1, W2, W3, G0, G1, G2, G3, G4, G5, G6, G7, G8, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
         double eps = 1.0e-7, fac2 = 10.0;
         double dil = Dl[p];
         double fac = 5.0e-1 * (1.0 - tanh(2.5 + fac2 * dil));
@@ -504,7 +510,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     ST_TRY(laplacian(c, d2, d4e));
     ScratchT<R> etas(c, 4);
     R *eta = etas, *etag = eta + 2 * n3;   // [rho|d4S|, fac3|d4e|] and their filtered values
-    PFOR(c, n3, {
+    PFOR(c, n3, io(Q4, T, P, Vs, d4S, d4e) + 2 * io(eta), {
         double fac3 = (Q4[p] / T[p]) * sqrt(gam * P[p] * Vs[p]);
         eta[p] = Q4[p] * fabs(d4S[p]);
         eta[n3 + p] = fac3 * fabs(d4e[p]);
@@ -514,7 +520,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     const double C_mu = 2.0e-3, C_k = 1.0e-2;
     R **H = Store<R>::hyp(c);
     R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K];
-    PFOR(c, n3, {
+    PFOR(c, n3, io(Cbeta, hb, hv, hk) + 2 * io(etag), {
         hb[p] = Cbeta[p] * etag[p] * DX6;
         hv[p] = C_mu * etag[p] * DX6;
         hk[p] = C_k * etag[n3 + p] * DX5;
@@ -540,7 +546,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
             *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
     {
-        PFOR(c, n3, {
+        PFOR(c, n3, io(G0, G1, G2, G3, G4, G5, G6, G7, G8, g, Y, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
             // G0..G8 = dux_dx, duy_dx, duz_dx, dux_dy, duy_dy, duz_dy, dux_dz, duy_dz, duz_dz
             double w1 = G5[p] - G7[p];
             double w2 = G6[p] - G2[p];
@@ -573,7 +579,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
         ST_TRY(laplacian(c, Yr, d2));
         ST_TRY(laplacian(c, d2, d4Y));
         const double C_mu = 2.0e-3, C_k = 1.0e-2;
-        PFOR(c, n3, {
+        PFOR(c, n3, io(d4S, d4e, d4Y, g, P, Vs, Q4, T, Cbeta, Y) + 5 * io(eta), {
             double a4S = fabs(d4S[p]), a4e = fabs(d4e[p]), a4Y = fabs(d4Y[p]);
             double cs = sqrt(g[p] * P[p] * Vs[p]);
             double fac3 = (Q4[p] / T[p]) * sqrt(g[p] * P[p] * Vs[p]);
@@ -590,7 +596,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
         const double C_D = 1.0e-4, C_Y = 100.0;
         R **H = Store<R>::hyp(c);
         R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K], *hd = H[H_D];
-        PFOR(c, n3, {
+        PFOR(c, n3, 5 * io(etag) + io(hb, hv, hk, hd), {
             hb[p] = etag[2 * n3 + p] * DX6;
             hv[p] = etag[p] * DX6;
             hk[p] = etag[n3 + p] * DX5;
@@ -622,7 +628,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     const R *GTx = Gr[G_DTDX], *GTy = Gr[G_DTDY], *GTz = Gr[G_DTDZ];
     R *const *H = Store<R>::hyp(c);
     const R *vh = H[H_VISC], *bh = H[H_BETA], *kh = H[H_K];
-    PFOR(c, n3, {
+    PFOR(c, n3, io(Q1, Q2, Q3, Q4, G0, G1, G2, G3, G4, G5, G6, G7, G8, vh, bh, U1, U2, U3, dila, S1, S2, S3, Flux, Flux2), {
         U1[p] = Q1[p] / Q4[p];
         U2[p] = Q2[p] / Q4[p];
         U3[p] = Q3[p] / Q4[p];
@@ -648,7 +654,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     ST_TRY(dfd(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
     ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
     // z momentum
-    PFOR(c, n3, { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
+    PFOR(c, n3, io(vh, G8, bh, dila, Flux), { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
     ST_TRY(dfd(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
     ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
     ST_TRY(dfd(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
@@ -659,7 +665,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     ST_TRY(dfd(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
     ST_TRY(dfd(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
     ST_TRY(dfd(c, 2, 0, pr_mul(kh, GTz), h5, 1, 1.0));
-    PFOR(c, n3, {
+    PFOR(c, n3, 4 * io(Qrhs, Qrhs, Qh), {
         for (int l = 0; l < 5; l++)
             if (l != 3) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] + Qh[l * n3 + p];
     });
@@ -682,7 +688,7 @@ static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const
     R *const *dYd = Store<R>::dYd(c);
     const R *Dh = Store<R>::hyp(c)[H_D];
     const double *g = c->gamma_eff;
-    PFOR(c, n3, {
+    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, T), {
         double Vs, P, Tt;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, P, Tt);
         T[p] = Tt;
@@ -702,7 +708,7 @@ static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const
         ST_TRY(dfd(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
         ST_TRY(dfd(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
     }
-    PFOR(c, n3, { Yrhs[p] = Yrhs[p] + Yd[p]; });
+    PFOR(c, n3, io(Yrhs, Yrhs, Yd), { Yrhs[p] = Yrhs[p] + Yd[p]; });
     return ST_OK;
 }
 
@@ -718,13 +724,13 @@ static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     // plane over its cells only
     {
         const size_t MyMz = (size_t)My * Mz;
-        PFOR(c, MyMz, { Q1[p] = 0.0; });                                          // i = 0: p = j + My*k
-        PFOR(c, (size_t)My * Mx, { Q3[(p % My) + MyMz * (p / My)] = 0.0; });      // k = 0: p = j + My*i
-        PFOR(c, (size_t)Mz * Mx, { Q2[(size_t)My * p] = 0.0; });                  // j = 0: p = k + Mz*i
+        PFOR(c, MyMz, io(Q1), { Q1[p] = 0.0; });                                          // i = 0: p = j + My*k
+        PFOR(c, (size_t)My * Mx, io(Q3), { Q3[(p % My) + MyMz * (p / My)] = 0.0; });      // k = 0: p = j + My*i
+        PFOR(c, (size_t)Mz * Mx, io(Q2), { Q2[(size_t)My * p] = 0.0; });                  // j = 0: p = k + Mz*i
     }
     ScratchNT<R> s(c, 4);
     R *P = s[0], *dPx = s[1], *dPy = s[2], *dPz = s[3];
-    PFOR(c, n3, {
+    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, P), {
         double Vs, Pp, T;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, Pp, T);
         P[p] = Pp;
@@ -737,7 +743,7 @@ static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     // faces in the reference order x, y, z (later faces overwrite edges)
     for (int face = 0; face < 3; face++) {
         size_t nf = face == 0 ? (size_t)My * Mz : face == 1 ? (size_t)Mx * Mz : (size_t)Mx * My;
-        PFOR(c, nf, {
+        PFOR(c, nf, io(Q1, Q2, Q3, Q4, P, g, dPx, Gxx, Yrhs) + 5 * io(Qrhs), {
             size_t q;
             if (face == 0) q = p + (size_t)My * Mz * (Mx - 1);                    // p = j + My*k
             else if (face == 1) q = (My - 1) + (size_t)My * p;                    // p = k + Mz*i
@@ -789,7 +795,9 @@ static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrh
     }
     const int sx = start[0], sy = start[1], sz = start[2], lx = len[0], ly = len[1], lz = len[2];
     const bool idx32 = n3 <= 0xffffffffull;   // 32-bit index arithmetic when it suffices
-    PFOR(c, n3, {
+    // fraction of the cells in the sponge shell (the only ones touched)
+    const double shell = (double)(n3 - (size_t)sx * sy * sz) / (double)n3;
+    PFOR(c, n3, shell * (10 * io(Qrhs) + 5 * io(Q) + io(Y) + 2 * io(Yrhs)), {
         int j, k, i;
         if (idx32) {
             unsigned q = (unsigned)p, r = q / (unsigned)My;
@@ -887,7 +895,7 @@ int dev_fix_pressure(st_ctx *c, double *Q) {
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
     const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
-    PFOR(c, n3, {
+    PFOR(c, n3, io(g, Q1, Q2, Q3, Q4, Q5, Q5), {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
@@ -904,7 +912,7 @@ static int fix_pressure_copy(st_ctx *c, double *Q, float *qs) {
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
     const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
-    PFOR(c, n3, {
+    PFOR(c, n3, io(g, Q1, Q2, Q3, Q4, Q5, Q5) + 5 * io(qs), {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
@@ -1132,7 +1140,7 @@ static int refresh(st_ctx *c, StateCopy<R> &sc, const double *Q, const double *Y
     if constexpr (!is_fp64<R>()) {
         const size_t n3 = c->dm.n3;
         float *qs = sc.qs, *ys = sc.ys;
-        PFOR(c, n3, {
+        PFOR(c, n3, 5 * io(Q, qs) + (with_y ? io(Y, ys) : 0.0), {
             for (int l = 0; l < 5; l++) qs[l * n3 + p] = (float)Q[l * n3 + p];
             if (with_y) ys[p] = (float)Y[p];
         });
@@ -1172,7 +1180,7 @@ static int lddrk4_sf(st_ctx *c) {
             if (!fresh) ST_TRY(refresh<R>(c, sc, Q, c->Y, false));
             ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, c->Y));
             ST_TRY(hyper_rhs_t<R>(c, Q, dQ, c->Y, sc.y(c->Y)));
-            PFOR(c, n3, {
+            PFOR(c, n3, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)), {
                 double dt = *dtp;
                 for (int l = 0; l < 5; l++) {
                     size_t q = l * n3 + p;
@@ -1193,7 +1201,7 @@ static int lddrk4_sf(st_ctx *c) {
                 fresh = true;
             }
         }
-        PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
+        PFOR(c, 1, io(timep, timep), { timep[0] = timep[0] + dtp[0]; });
     }
     return ST_OK;
 }
@@ -1225,7 +1233,7 @@ static int lddrk4_mf(st_ctx *c) {
             ST_TRY(species_rhs_t<R>(c, Q, sc.q(Q), dQ, Y, sc.y(Y), drYi));
             ST_TRY(bc_rhs_t<R>(c, Q, dQ, Y, drYi));
             ST_TRY(sponge_t<R>(c, Q, dQ, Y, drYi));
-            PFOR(c, n3, {
+            PFOR(c, n3, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)) + io(Y, drYi, rYW, rY) + (first ? 0.0 : io(rYW)), {
                 double dt = *dtp;
                 double ry = Q[3 * n3 + p] * Y[p];
                 for (int l = 0; l < 5; l++) {
@@ -1252,7 +1260,7 @@ static int lddrk4_mf(st_ctx *c) {
             const double *g = c->gamma_eff;
             float *qs = nullptr, *ys = nullptr;
             if constexpr (!is_fp64<R>()) { qs = sc.qs; ys = sc.ys; fresh = true; }
-            PFOR(c, n3, {
+            PFOR(c, n3, 5 * io(Q) + io(rY, g, Y, Q) + (qs ? 5 * io(qs) + io(ys) : 0.0), {
                 double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p];
                 double y = rY[p] / q4;
                 Y[p] = y;
@@ -1269,7 +1277,7 @@ static int lddrk4_mf(st_ctx *c) {
                 }
             });
         }
-        PFOR(c, 1, { timep[0] = timep[0] + dtp[0]; });
+        PFOR(c, 1, io(timep, timep), { timep[0] = timep[0] + dtp[0]; });
     }
     return ST_OK;
 }
