@@ -96,3 +96,50 @@ def test_rhs_cancels_manufactured_source(oracle_mod, case):
         # sixth-order convergence where the error is above rounding
         if e16[l] > 1e-11:
             assert e16[l] / max(e32[l], 1e-16) > 2 ** 5.3, (case, l, e16[l], e32[l])
+
+
+def test_mf_rhs_cancels_manufactured_source(oracle_mod):
+    """The same check on the two-species octant family (src/rhsv_sym_mf.f),
+    with Y = 1, Re = 0 (no molecular viscosity) and the state of block A
+    without phase shifts: rho u = sin x is odd about x = 0 and every other
+    field is even there, the parities the reference's sym/asym derivative
+    choices assume at the symmetry planes.  A wrong sym/asym choice would leave
+    an O(1) error at those planes.  The one-sided closures at the far faces
+    are third order, so the residual over the whole octant must fall at least
+    2^2.8-fold from 32^3 to 64^3 (measured: 8x in the momenta, 17x in mass and
+    energy)."""
+    from shock_turbulence_b200.params import default_params
+    L = 2 * math.pi
+
+    def res(n):
+        p = default_params(n, length=L, gamma1=GAMMA, gamma2=GAMMA)
+        o = oracle_mod.Oracle(p)
+        t = np.arange(n) * (L / (n - 1))
+        x, y, z = t[:, None, None], t[None, None, :], t[None, :, None]
+        shape = (n, n, n)
+        zero = np.zeros(shape)
+        sx, sy, sz = np.sin(x) + zero, np.sin(y) + zero, np.sin(z) + zero
+        cx, cy, cz = np.cos(x) + zero, np.cos(y) + zero, np.cos(z) + zero
+        P = 100.0
+        Q = np.empty((5,) + shape)
+        Q[0], Q[1], Q[2], Q[3] = sx, sy, sz, 1.0
+        Q[4] = P / (GAMMA - 1.0) + 0.5 * (sx * sx + sy * sy + sz * sz)
+        src = np.empty_like(Q)
+        src[3] = cx + cy + cz
+        src[0] = np.sin(2 * x) + sx * cy + sx * cz
+        src[1] = np.sin(2 * y) + sy * cx + sy * cz
+        src[2] = np.sin(2 * z) + sz * cx + sz * cy
+        src[4] = (FAC2 * P * (cx + cy + cz) + 1.5 * (sx * sx * cx + sy * sy * cy + sz * sz * cz)
+                  + 0.5 * (sy * sy * cx + sz * sz * cx + sx * sx * cy + sz * sz * cy + sx * sx * cz + sy * sy * cz))
+        Y = np.ones(shape)
+        o.set_state(Q, Y)
+        o.compute_gamma(Y)
+        R = np.zeros_like(Q)
+        o.rhs(Q.copy(), R, Y)
+        scale = np.abs(src).max()
+        return [float(np.abs(R[l] + src[l]).max() / scale) for l in range(5)]
+
+    e32, e64 = res(32), res(64)
+    for l in range(5):
+        assert e64[l] < 2e-5, (l, e64[l])
+        assert e32[l] / e64[l] > 2 ** 2.8, (l, e32[l], e64[l])
