@@ -16,7 +16,11 @@ with f = sin(x+pi/6) sin(y+pi/3) sin(z+pi/2).  On the periodic box
 RHS + source must vanish up to the sixth-order truncation error of the compact
 derivatives: small on 32^3, and shrinking by about 2^6 from 16^3 to 32^3.
 This pins the oracle's flux assembly to the equations themselves, not to a
-restatement of the reference."""
+restatement of the reference.
+
+The file's last block ("viscous part only", 5/28/08) is checked through the
+difference of two RHS evaluations, one with mu = 1 and one with a negligible
+viscosity, which leaves the viscous terms alone."""
 import math
 
 import numpy as np
@@ -143,3 +147,86 @@ def test_mf_rhs_cancels_manufactured_source(oracle_mod):
     for l in range(5):
         assert e64[l] < 2e-5, (l, e64[l])
         assert e32[l] / e64[l] > 2 ** 2.8, (l, e32[l], e64[l])
+
+
+def viscous_state(n, h):
+    """The block "MMS source terms for viscous part only" (5/28/08): rho = 1,
+    P = 100 and u = (sin x cos y cos z, cos x sin y cos z, cos x cos y sin z).
+    With mu = 1 the viscous terms of RHS equal -source: -4 u_i in the momenta
+    and -4|u|^2 + 4 (s_xy^2 + s_xz^2 + s_yz^2) in the energy (u_i d_j tau_ij
+    plus the dissipation tau_ij d_j u_i, the diagonal of tau being zero)."""
+    t = np.arange(n) * h
+    x, y, z = t[:, None, None], t[None, None, :], t[None, :, None]
+    zero = np.zeros((n, n, n))
+    a = np.sin(x) * np.cos(y) * np.cos(z) + zero
+    b = np.cos(x) * np.sin(y) * np.cos(z) + zero
+    c = np.cos(x) * np.cos(y) * np.sin(z) + zero
+    sxy = np.sin(x) * np.sin(y) * np.cos(z) + zero
+    sxz = np.sin(x) * np.cos(y) * np.sin(z) + zero
+    syz = np.cos(x) * np.sin(y) * np.sin(z) + zero
+    P = 100.0
+    Q = np.empty((5, n, n, n))
+    Q[0], Q[1], Q[2], Q[3] = a, b, c, 1.0
+    Q[4] = P / (GAMMA - 1.0) + 0.5 * (a * a + b * b + c * c)
+    src = np.zeros_like(Q)
+    src[0], src[1], src[2] = 4 * a, 4 * b, 4 * c
+    src[4] = 4 * (a * a + b * b + c * c) - 4 * (sxy ** 2 + sxz ** 2 + syz ** 2)
+    return Q, src
+
+
+def viscous_residual(oracle_mod, make_params, n, h, with_y):
+    """RHS with mu = 1 (Re = 1, vis_exp = 0) minus RHS with a negligible
+    viscosity (Re = 1e30) is the viscous part alone; its residual against the
+    source, relative to max|source|, per conserved field."""
+    Q, src = viscous_state(n, h)
+    Y = np.ones(Q.shape[1:]) if with_y else None
+    out = []
+    for re in (1.0, 1.0e30):
+        o = oracle_mod.Oracle(make_params(re))
+        if with_y:
+            o.set_state(Q, Y)
+            o.compute_gamma(Y)
+        R = np.zeros_like(Q)
+        o.rhs(Q.copy(), R, Y)
+        out.append(R)
+    V = out[0] - out[1]
+    scale = np.abs(src).max()
+    return [float(np.abs(V[l] + src[l]).max() / scale) for l in range(5)]
+
+
+def test_periodic_viscous_part_cancels_manufactured_source(oracle_mod):
+    """Periodic box (src/rhsv_periodic_sf.f, mu = ((gamma-1)T)^vis_exp / Re):
+    sixth-order convergence, measured 1.5e-6 on 16^3 and 2.4e-8 on 32^3."""
+    from shock_turbulence_b200 import periodic_params
+
+    def res(n):
+        return viscous_residual(oracle_mod, lambda re: periodic_params(n, re=re, gamma=GAMMA, vis_exp=0.0),
+                                n, 2 * math.pi / n, False)
+
+    e16, e32 = res(16), res(32)
+    assert e16[3] == 0.0 and e32[3] == 0.0        # no viscous term in the mass equation
+    for l in (0, 1, 2, 4):
+        assert e32[l] < 1e-7, (l, e32[l])
+        assert e16[l] / e32[l] > 2 ** 5.3, (l, e16[l], e32[l])
+
+
+def test_mf_viscous_part_cancels_manufactured_source(oracle_mod):
+    """_mf octant (src/rhsv_sym_mf.f) with Y = 1 and Re = Re1 = 1 (the viscous
+    term is added because Re > 0): u is odd about its own symmetry plane and
+    even about the others, as the sym/asym closures assume.  The far faces'
+    one-sided second-derivative closures set the rate: measured 6.7e-3 on
+    32^3 and 8.6e-4 on 64^3 in the momenta, 4.5e-3 and 2.7e-4 in the energy."""
+    from shock_turbulence_b200.params import default_params
+    L = 2 * math.pi
+
+    def res(n):
+        return viscous_residual(
+            oracle_mod, lambda re: default_params(n, length=L, gamma1=GAMMA, gamma2=GAMMA, re=re, re1=re,
+                                                  vis_exp=0.0),
+            n, L / (n - 1), True)
+
+    e32, e64 = res(32), res(64)
+    assert e32[3] == 0.0 and e64[3] == 0.0
+    for l in (0, 1, 2, 4):
+        assert e64[l] < 2e-3, (l, e64[l])
+        assert e32[l] / e64[l] > 2 ** 2.5, (l, e32[l], e64[l])
