@@ -25,6 +25,7 @@
 //    contexts on one device) race on it.  Calls on one stream are ordered and
 //    safe; the call returns once R is written (it synchronises its stream).
 #include <mutex>
+#include <new>
 #include "st_internal.h"
 
 namespace st {
@@ -39,7 +40,8 @@ namespace {
 constexpr size_t kNoAllocMaxElems = size_t(1) << 18;
 constexpr int kMaxDevices = 64;
 
-// working copies of A (first half) and B (second half)
+// working copies of A and B: a call with N = n*lot elements puts A's copy in
+// the first N entries and B's copy right after it, in entries N .. 2N-1
 __device__ __align__(256) double g_tri_scratch[2 * kNoAllocMaxElems];
 
 std::mutex g_setup_mu;
@@ -78,9 +80,10 @@ bool on_device(const void *p, int dev) {
 
 using namespace st;
 
-extern "C" int st_tridiagonal_noalloc(st_ctx *c, const double *A, const double *B, const double *C,
-                                      double *R, int n, int lot, int nper) {
-    if (!c) return ST_E_ARG;
+// The body runs inside a try block: a std::bad_alloc from building an error
+// message must not cross the C boundary into a Fortran or C caller.
+static int tridiagonal_noalloc(st_ctx *c, const double *A, const double *B, const double *C, double *R,
+                               int n, int lot, int nper) {
     if (!A || !B || !C || !R || n < 1 || lot < 1) return fail(c, ST_E_ARG, "st_tridiagonal_noalloc: bad argument");
     const size_t N = (size_t)n * lot;
     if (N > kNoAllocMaxElems)
@@ -103,4 +106,14 @@ extern "C" int st_tridiagonal_noalloc(st_ctx *c, const double *A, const double *
     ST_CUDA(c, cudaGetLastError());
     ST_CUDA(c, cudaStreamSynchronize(c->stream));
     return ST_OK;
+}
+
+extern "C" int st_tridiagonal_noalloc(st_ctx *c, const double *A, const double *B, const double *C,
+                                      double *R, int n, int lot, int nper) {
+    if (!c) return ST_E_ARG;
+    try {
+        return tridiagonal_noalloc(c, A, B, C, R, n, lot, nper);
+    } catch (const std::bad_alloc &) {
+        return fail(c, ST_E_NOMEM, "host allocation failed");
+    }
 }

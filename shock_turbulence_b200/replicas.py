@@ -1,7 +1,7 @@
 """Replica bookkeeping for runs with one independent grid per GPU.
 
 The solver keeps a whole grid resident on one GPU (the reference's MPI pencil
-decomposition, src/mpi_stuff*.f, is not needed for grids that fit in one GPU's
+decomposition, set up in src/initialize_mpi_nonperiodic.f90, is not needed for grids that fit in one GPU's
 memory).  N GPUs therefore run N independent replicas: each rank steps its own
 seeded grid and nothing is exchanged on the data path.  The only cross-rank
 operations are the barrier around a timed region and the maximum of the ranks'

@@ -1,8 +1,8 @@
 """FP32 mode (float intermediates, double state, accumulators, state filter and
 pressure recovery) against the FP64 path and the CPU oracle.
 
-Tolerance: relative L2 error per conserved field <= 1e-5 after the steps
-below, the bound the FP32 mode is specified to; Linf is reported beside it
+Tolerance: relative L2 error per conserved field <= 1e-5 after 100 steps
+(the precision workload's horizon), the bound the FP32 mode is specified to; Linf is reported beside it
 and bounded at 1e-4.  Single operators (one RHS evaluation, whose derivatives
 of float-rounded fields carry an error of about eps_float * N) are bounded at
 1e-4 relative L2."""
@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 L2_TOL = 1e-5
 LINF_TOL = 1e-4
+NSTEPS = 100
 
 
 def blast(p, seed=5):
@@ -53,11 +54,11 @@ def test_blast_steps_vs_fp64():
     p64 = default_params(64, **kw)
     p32 = default_params(64, precision=PRECISION_FP32, **kw)
     Q, Y = blast(p64)
-    Q64, Y64, t64 = run(p64, Q, Y, 20)
-    Q32, Y32, t32 = run(p32, Q, Y, 20)
+    Q64, Y64, t64 = run(p64, Q, Y, NSTEPS)
+    Q32, Y32, t32 = run(p32, Q, Y, NSTEPS)
     errs = field_errors(Q32, Q64, Y32, Y64)
     l2, linf = worst(errs)
-    print("blast 64^3, 20 steps:", report(errs))
+    print(f"blast 64^3, {NSTEPS} steps:", report(errs))
     assert np.isfinite(Q32).all()
     assert abs(t32 - t64) <= 1e-5 * t64
     assert l2 <= L2_TOL, report(errs)
@@ -69,18 +70,18 @@ def test_periodic_steps_vs_fp64():
     p64 = periodic_params(64)
     p32 = periodic_params(64, precision=PRECISION_FP32)
     Q = periodic_turbulence(p64, k0=4.0, urms=0.1, seed=2)
-    Q64, _, t64 = run(p64, Q, None, 20)
-    Q32, _, t32 = run(p32, Q, None, 20)
+    Q64, _, t64 = run(p64, Q, None, NSTEPS)
+    Q32, _, t32 = run(p32, Q, None, NSTEPS)
     errs = field_errors(Q32, Q64)
     l2, linf = worst(errs)
-    print("periodic 64^3, 20 steps:", report(errs))
+    print(f"periodic 64^3, {NSTEPS} steps:", report(errs))
     assert abs(t32 - t64) <= 1e-5 * t64
     assert l2 <= L2_TOL, report(errs)
     assert linf <= LINF_TOL, report(errs)
 
 
 def test_steps_vs_oracle(oracle_mod):
-    """FP32 GPU steps against the FP64 CPU oracle directly (3 steps)."""
+    """FP32 GPU steps against the FP64 CPU oracle directly (100 steps)."""
     from shock_turbulence_b200 import Solver
     p = default_params(32, 32, 64, re=100.0, precision=PRECISION_FP32)
     po = default_params(32, 32, 64, re=100.0)
@@ -91,13 +92,13 @@ def test_steps_vs_oracle(oracle_mod):
     s.Compute_gamma(Y); o.compute_gamma(Y)
     s.Compute_hyper(Q, Y); o.compute_hyper(Q, Y)
     ts, ss, to, so = 0.0, 0, 0.0, 0
-    for _ in range(3):
+    for _ in range(NSTEPS):
         ts, ss = s.step(ts, ss)
         to, so = o.step(to, so)
     Qg, Yg = s.get_state()
     Qo, Yo = o.get_state()
     errs = field_errors(Qg, Qo, Yg, Yo)
-    print("oracle 32x32x64, 3 steps:", report(errs))
+    print(f"oracle 32x32x64, {NSTEPS} steps:", report(errs))
     assert worst(errs)[0] <= L2_TOL, report(errs)
 
 

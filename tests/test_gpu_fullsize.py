@@ -7,10 +7,14 @@
 - Compute_hyper, RHS and Hyper_RHS of the 384^3 blast state against the
   oracle: 1e-10 for the artificial-viscosity fields, 1e-11 per RHS field.
 - Compute_CFL + Compute_Tstep of that state against the oracle: 1e-12.
-- Properties of whole LDDRK4 steps at full size, where the oracle would take
-  minutes per step: a step is deterministic (two runs give the same bits), the
-  periodic box conserves mass (sum of rho) to 1e-12 relative, and the FP32
-  mode stays within 1e-5 relative L2 of FP64 per field after 3 steps.
+- One whole main-loop step (Compute_CFL, Compute_Tstep and the ten stages of
+  LDDRK4) of the 384^3 blast, and one (eleven stages) of the 512^3 periodic
+  box, against the oracle: 1e-10 per conserved field and Y, the step bound of
+  the small grids.  The oracle takes minutes per step at these sizes.
+- Properties of whole LDDRK4 steps at full size: a step is deterministic (two
+  runs give the same bits), the periodic box conserves mass (sum of rho) to
+  1e-12 relative, and the FP32 mode stays within 1e-5 relative L2 of FP64 per
+  field after 3 steps.
 
 Each test skips with its reason when the host lacks the memory the oracle
 needs at these sizes (about 40 GB for the 384^3 physics calls)."""
@@ -175,6 +179,27 @@ def test_cfl_and_tstep_384(blast_pair):
         assert abs(tg - to) <= 1e-12 * abs(to), step
 
 
+def test_step_matches_oracle_384(blast_pair):
+    s, o, Q, Y = blast_pair
+    for h in (s, o):
+        h.set_state(Q, Y)
+    s.Compute_gamma(Y)
+    o.compute_gamma(Y)
+    s.Compute_hyper(Q, Y)
+    o.compute_hyper(Q, Y)
+    tg, kg = s.step(0.0, 0)
+    to, ko = o.step(0.0, 0)
+    assert kg == ko == 1
+    assert abs(tg - to) <= 1e-12 * to
+    Qg, Yg = s.get_state()
+    Qo, Yo = o.get_state()
+    for l in range(5):
+        assert rel_err(Qg[l], Qo[l]) < 1e-10, l
+    assert rel_err(Yg, Yo) < 1e-10
+    del Qg, Yg, Qo, Yo
+    gc.collect()
+
+
 def test_step_is_deterministic_384(blast_pair):
     s, _, Q, Y = blast_pair
     out = []
@@ -249,6 +274,31 @@ def test_periodic_line_operators_512(periodic_solver, oracle_mod, d):
     getattr(s, "Compact_Filter_" + DIRS[d])(F, g)
     o.filter(d, 0, F, r)
     assert rel_err(g, r) < 1e-12
+
+
+def test_periodic_step_matches_oracle_512(periodic_solver, oracle_mod):
+    """The 512^3 box with the config-0 statistics at k0 = 8."""
+    from shock_turbulence_b200 import periodic_params
+    from shock_turbulence_b200.initial import periodic_turbulence
+    need_host(120)
+    s = periodic_solver
+    o = oracle_mod.Oracle(periodic_params(NPER))
+    Q = periodic_turbulence(s.params, k0=8.0, urms=0.1, seed=0)
+    s.set_state(Q, None)
+    o.set_state(Q, None)
+    s.Compute_hyper(Q, None)
+    o.compute_hyper(Q, None)
+    tg, kg = s.step(0.0, 0)
+    to, ko = o.step(0.0, 0)
+    assert kg == ko == 1
+    assert abs(tg - to) <= 1e-12 * to
+    del Q
+    Qg, _ = s.get_state()
+    Qo, _ = o.get_state()
+    del o
+    gc.collect()
+    for l in range(5):
+        assert rel_err(Qg[l], Qo[l]) < 1e-10, l
 
 
 def test_periodic_mass_conservation_512(periodic_solver):

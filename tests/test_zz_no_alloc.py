@@ -1,5 +1,6 @@
 """st_tridiagonal_noalloc: the allocation-free tridiagonal entry point agrees
-with st_tridiagonal, call after call, and rejects what it cannot serve.
+with st_tridiagonal and with the CPU oracle's tridiagonal, call after call,
+and rejects what it cannot serve.
 
 Kept in its own file, collected last, so that it also runs after every other
 GPU test in the same process; it passes alone in a fresh process as well."""
@@ -37,7 +38,7 @@ def _noalloc(s, A, B, C, R, n, lot, nper):
 
 
 @pytest.mark.parametrize("nper", [0, 1])
-def test_two_calls_match_st_tridiagonal(solver, nper):
+def test_two_calls_match_st_tridiagonal(solver, oracle_mod, nper):
     import torch
     rng = np.random.default_rng(11 + nper)
     for n, lot in ((40, 300), (512, 512)):          # the second size is exactly at the limit
@@ -49,9 +50,29 @@ def test_two_calls_match_st_tridiagonal(solver, nper):
             st = _noalloc(solver, dA, dB, dC, dR, n, lot, nper)
             assert st == 0, solver.lib.st_last_error(solver._h)
             assert rel_err(dR.cpu().numpy(), ref) < TOL
+            orc = R.copy()
+            oracle_mod.tridiagonal(A.copy(), B.copy(), C.copy(), orc, nper)
+            assert rel_err(dR.cpu().numpy(), orc) < TOL
             # the coefficients are inputs only
             assert torch.equal(dA.cpu(), torch.from_numpy(A))
             assert torch.equal(dB.cpu(), torch.from_numpy(B))
+
+
+@pytest.mark.parametrize("nper", [0, 1])
+@pytest.mark.parametrize("n", [1, 2, 3, 5])
+def test_short_lines_match_the_oracle(solver, oracle_mod, nper, n):
+    """The solver's special cases of very short (periodic) lines."""
+    import torch
+    rng = np.random.default_rng(100 * n + nper)
+    lot = 64
+    for _ in range(2):
+        A, B, C, R = _system(rng, n, lot)
+        orc = R.copy()
+        oracle_mod.tridiagonal(A.copy(), B.copy(), C.copy(), orc, nper)
+        dA, dB, dC, dR = (torch.from_numpy(x).cuda() for x in (A, B, C, R))
+        st = _noalloc(solver, dA, dB, dC, dR, n, lot, nper)
+        assert st == 0, solver.lib.st_last_error(solver._h)
+        assert rel_err(dR.cpu().numpy(), orc) < TOL
 
 
 def test_rejects_sizes_beyond_the_limit(solver):
