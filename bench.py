@@ -465,6 +465,72 @@ def run_precision(args, rank, world, local, dist):
         "clocks": clk}), flush=True)
 
 
+# ---------------------------------------------------------------- extensions
+def fp32_extension(args, local, Q0, Y0, ref_state, fp64_value):
+    """The FP32 mode on the same 384^3 blast: the same warm-up and timed steps
+    from the same initial state as the FP64 line, device-timed, and the
+    relative L2/Linf error per field of its final state against the FP64
+    run's."""
+    import torch
+    from shock_turbulence_b200 import Solver
+    from shock_turbulence_b200.precision import field_errors, worst
+    p = make_params(args.n, device=local, precision=1)
+    s = Solver(p)
+    stream = torch.cuda.current_stream()
+    s._check(s.lib.st_set_stream(s._h, stream.cuda_stream), "st_set_stream")
+    s.set_state(Q0, Y0)
+    s.Compute_gamma(Y0)
+    s.Compute_hyper(Q0, Y0)
+    t, st = 0.0, 0
+    for _ in range(args.warmup):
+        t, st = s.step(t, st)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(gpu_smi_id(local))
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        t, st = s.step(t, st)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    Q32, Y32 = s.get_state()
+    s.close()
+    errs = field_errors(Q32, ref_state[0], Y32, ref_state[1])
+    l2, linf = worst(errs)
+    value = args.n ** 3 * args.steps / (ms / 1e3) / 1e6
+    return {"metric": METRIC_FP32, "value": value, "unit": UNIT, "ms_per_step": ms / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "speedup_vs_fp64": value / fp64_value,
+            "dtype": "f32 intermediates / f64 state, accumulators, state filter, pressure recovery",
+            "errors_vs_fp64_after_steps": args.warmup + args.steps,
+            "errors": {k: {"l2_rel": v[0], "linf_rel": v[1]} for k, v in errs.items()},
+            "worst_l2_rel": l2, "worst_linf_rel": linf, "clocks": clk}
+
+
+def serving_extension(args, local, fp64_value):
+    """A short serving run (FP32 mode): Poisson arrivals at 20/s of blast
+    cases of mixed grid sizes, 100 LDDRK4 steps each, 150 GB HBM budget,
+    same-size cases stepped together; aggregate cell-steps/s over the
+    makespan and p50/p99 time to solution."""
+    import torch
+    from shock_turbulence_b200.serving import Server, _gpu_solver_factory, summarize
+    torch.cuda.set_device(local)
+    reqs = serving_requests(args.ext_requests, 100, 20.0, seed=4)
+    srv = Server(hbm_budget=150e9, make_solver=_gpu_solver_factory(precision=1))
+    clocks = ClockSampler(gpu_smi_id(local))
+    clocks.start()
+    res = srv.run(reqs)
+    clk = clocks.stop()
+    srv.close()
+    summ = summarize(res)
+    return {"metric": "Mcell-steps/s (serving: mixed-size blast cases, FP32 mode, 100 LDDRK4 steps each)",
+            "value": summ["mcell_steps_per_s"], "unit": UNIT, "ratio_vs_fp64_plain": summ["mcell_steps_per_s"] / fp64_value,
+            "requests": len(res), "p50_s": summ["p50_s"], "p99_s": summ["p99_s"], "makespan_s": summ["makespan_s"],
+            "sizes": sorted(r.n for r in res), "clocks": clk,
+            "timing": "wall clock over the run (arrival of the first request to completion of the last)"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -476,6 +542,11 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=96, help="grid of the CPU-oracle sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extensions", action="store_true",
+                    help="blast3d, FP64, one GPU: skip the FP32-mode and serving measurements that the "
+                         "default line carries under 'extensions'")
+    ap.add_argument("--ext-requests", type=int, default=16,
+                    help="requests of the serving measurement in the default line")
     ap.add_argument("--workload", default="blast3d", choices=["blast3d", "radial", "serving", "precision"],
                     help="blast3d: the 384^3 octant case; radial: the batch of 4096 1-D radial blasts; "
                          "serving: a Poisson stream of mixed-size blast cases through the serving loop; "
@@ -582,6 +653,8 @@ def main():
     value = aggregate_rate(cells, args.steps, ms, world)
     mon = s.monitors()
     finite = bool(math.isfinite(mon[0]) and math.isfinite(mon[5]))
+    want_ext = world == 1 and not args.no_extensions and not fp32
+    ref_state = s.get_state() if want_ext else None     # FP64 state after warm-up + timed steps
 
     # ---- end-to-end through the public API with host buffers ----
     import numpy as np
@@ -649,6 +722,13 @@ def main():
                "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 3 timed steps "
                          f"({el:.1f} s), {threads} OpenMP threads"}
 
+    ext = None
+    if want_ext:
+        s.close()
+        s = None
+        ext = {"fp32_mode": fp32_extension(args, local, Q, Y, ref_state, value),
+               "serving": serving_extension(args, local, value)}
+
     if rank == 0:
         line = {
             "metric": METRIC_FP32 if fp32 else METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -668,8 +748,11 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        if ext is not None:
+            line["extensions"] = ext
         print(json.dumps(line), flush=True)
-    s.close()
+    if s is not None:
+        s.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -10,7 +10,9 @@
 - One whole main-loop step (Compute_CFL, Compute_Tstep and the ten stages of
   LDDRK4) of the 384^3 blast, and one (eleven stages) of the 512^3 periodic
   box, against the oracle: 1e-10 per conserved field and Y, the step bound of
-  the small grids.  The oracle takes minutes per step at these sizes.
+  the small grids.  The oracle takes about 4 minutes for the 384^3 step and
+  about 14 minutes for the 512^3 step on a 16-core host, so the 512^3 step
+  runs only when ST_FULL_PERIODIC_STEP=1 is set.
 - Properties of whole LDDRK4 steps at full size: a step is deterministic (two
   runs give the same bits), the periodic box conserves mass (sum of rho) to
   1e-12 relative, and the FP32 mode stays within 1e-5 relative L2 of FP64 per
@@ -278,8 +280,11 @@ def test_periodic_line_operators_512(periodic_solver, oracle_mod, d):
 
 def test_periodic_step_matches_oracle_512(periodic_solver, oracle_mod):
     """The 512^3 box with the config-0 statistics at k0 = 8."""
+    import os
     from shock_turbulence_b200 import periodic_params
     from shock_turbulence_b200.initial import periodic_turbulence
+    if os.environ.get("ST_FULL_PERIODIC_STEP") != "1":
+        pytest.skip("the oracle's 512^3 step takes about 14 minutes; set ST_FULL_PERIODIC_STEP=1 to run it")
     need_host(120)
     s = periodic_solver
     o = oracle_mod.Oracle(periodic_params(NPER))
