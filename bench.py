@@ -353,8 +353,8 @@ def run_serving(args, rank, world, local, dist):
     torch.cuda.set_device(local)
     reqs = serving_requests(args.requests, steps, 20.0, seed=4 + rank)
     fp32 = args.precision == "fp32"
-    from shock_turbulence_b200.serving import _gpu_solver_factory
-    srv = Server(hbm_budget=150e9, make_solver=_gpu_solver_factory(precision=1 if fp32 else 0))
+    from shock_turbulence_b200.serving import _gpu_batch_factory
+    srv = Server(hbm_budget=150e9, make_batch=_gpu_batch_factory(precision=1 if fp32 else 0))
     # warm the slot kinds once (not timed): context creation, scratch pools, graphs
     clocks = ClockSampler(gpu_smi_id(local))
     clocks.start()
@@ -379,7 +379,7 @@ def run_serving(args, rank, world, local, dist):
             "config": {"workload": f"{args.requests} requests, Poisson arrivals at 20/s, grid sizes {SRV_SIZES} with "
                                    f"weights {SRV_WEIGHTS}, pressure ratio uniform in [10, 200], 150 GB HBM budget",
                        "p50_s": summ["p50_s"], "p99_s": summ["p99_s"], "mean_s": summ["mean_s"],
-                       "makespan_s": summ["makespan_s"], "slots_created": len(srv.slots),
+                       "makespan_s": summ["makespan_s"], "batches": {g.n: g.capacity for g in srv.slots},
                        "sizes": [r.n for r in sorted(res, key=lambda r: r.rid)]},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": h2d / max(1, steps * len(res)),
                     "d2h_bytes_per_step": h2d / max(1, steps * len(res)),
@@ -514,20 +514,21 @@ def serving_extension(args, local, fp64_value):
     same-size cases stepped together; aggregate cell-steps/s over the
     makespan and p50/p99 time to solution."""
     import torch
-    from shock_turbulence_b200.serving import Server, _gpu_solver_factory, summarize
+    from shock_turbulence_b200.serving import Server, _gpu_batch_factory, summarize
     torch.cuda.set_device(local)
     reqs = serving_requests(args.ext_requests, 100, 20.0, seed=4)
-    srv = Server(hbm_budget=150e9, make_solver=_gpu_solver_factory(precision=1))
+    srv = Server(hbm_budget=150e9, make_batch=_gpu_batch_factory(precision=1))
     clocks = ClockSampler(gpu_smi_id(local))
     clocks.start()
     res = srv.run(reqs)
     clk = clocks.stop()
+    batches = {g.n: g.capacity for g in srv.slots}
     srv.close()
     summ = summarize(res)
     return {"metric": "Mcell-steps/s (serving: mixed-size blast cases, FP32 mode, 100 LDDRK4 steps each)",
             "value": summ["mcell_steps_per_s"], "unit": UNIT, "ratio_vs_fp64_plain": summ["mcell_steps_per_s"] / fp64_value,
             "requests": len(res), "p50_s": summ["p50_s"], "p99_s": summ["p99_s"], "makespan_s": summ["makespan_s"],
-            "sizes": sorted(r.n for r in res), "clocks": clk,
+            "sizes": sorted(r.n for r in res), "batch_capacity": batches, "clocks": clk,
             "timing": "wall clock over the run (arrival of the first request to completion of the last)"}
 
 

@@ -342,6 +342,32 @@ int  st_radial_rhs(st_radial *h, const double *Q, double *Qrhs);
 int  st_radial_rhs_hyper(st_radial *h, const double *Q, double *Qrhs);
 int  st_radial_launch_count(const st_radial *h, long long *count);
 
+/* ---- batches of same-size cases (no reference counterpart) ----------------
+ * A batch context holds ncase independent cases of one grid and one set of
+ * parameters (serving: same-size requests stepped together).  On the device
+ * every field holds ncase consecutive blocks of Nx*Ny*Nz cells, so each line
+ * and pointwise kernel of a step is one launch over all active cases, not
+ * one per case.  Cases 0 .. nactive-1 are stepped; each keeps its own time
+ * step, time and step count, so cases that started at different times
+ * advance together and each gives the same results as alone.  The
+ * single-grid entry points above return ST_E_UNSUPPORTED on a batch
+ * context.
+ * st_case_start uploads case k's state (host or device arrays in the
+ * reference layout), sets its time and step count 0 and runs its set-up
+ * (Compute_gamma and Compute_hyper, src/main_mf.f:100-101).  st_case_get
+ * reads a case's state, time and step count.  st_case_move copies case src
+ * over case dst (to keep the active cases in front when one finishes).
+ * st_batch_step_async enqueues one main-loop step (Compute_CFL,
+ * Compute_Tstep, LDDRK4) of every active case: a CUDA graph per active
+ * count, captured on its first use. */
+int  st_create_batch(const st_params *p, int ncase, st_ctx **out);
+int  st_batch_info(st_ctx *c, int *ncase, int *nactive);
+int  st_set_active(st_ctx *c, int nactive);
+int  st_case_start(st_ctx *c, int k, const double *Q, const double *Y, double time);
+int  st_case_get(st_ctx *c, int k, double *Q, double *Y, double *time, int *step);
+int  st_case_move(st_ctx *c, int src, int dst);
+int  st_batch_step_async(st_ctx *c);
+
 /* ---- streams, instrumentation (no reference counterpart) ------------------ */
 /* Runs the context's work on a caller-owned cudaStream_t (NULL restores the
  * context's own stream), so callers can order and time it with their own

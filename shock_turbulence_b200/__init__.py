@@ -5,4 +5,4 @@ include/st_b200.h); this package is its host-side mirror of the reference's
 subroutine interface."""
 from .params import (FAMILY_MF, FAMILY_PERIODIC, PRECISION_FP32, PRECISION_FP64, StParams, default_params,  # noqa: F401
                      periodic_params)
-from .api import Solver, StError  # noqa: F401
+from .api import Batch, Solver, StError  # noqa: F401

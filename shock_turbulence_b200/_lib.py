@@ -59,6 +59,14 @@ SIGNATURES = {
     "st_profile": [_ctx, ctypes.c_int],
     "st_profile_report": [_ctx, ctypes.c_char_p, ctypes.c_int],
     "st_launch_count": [_ctx, ctypes.POINTER(ctypes.c_longlong)],
+    # batches of same-size cases
+    "st_create_batch": [ctypes.POINTER(StParams), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "st_batch_info": [_ctx, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    "st_set_active": [_ctx, ctypes.c_int],
+    "st_case_start": [_ctx, ctypes.c_int, _dp, _dp, ctypes.c_double],
+    "st_case_get": [_ctx, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)],
+    "st_case_move": [_ctx, ctypes.c_int, ctypes.c_int],
+    "st_batch_step_async": [_ctx],
     # 1-D spherical-radial batch (handle in place of the context)
     "st_radial_create": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_void_p)],

@@ -263,3 +263,87 @@ for _d in ("X", "Y", "Z"):
     setattr(Solver, f"Compact_Filter_{_d}", _make_line_op(f"st_compact_filter_{_d.lower()}", "f"))
 
 __all__ = ["Solver", "StError", "StParams", "default_params"]
+
+
+class Batch:
+    """A batch context: ``ncase`` independent cases of one grid size and one
+    parameter set, stepped together (one launch per operator for all active
+    cases; each case keeps its own time step, time and step count).  Cases
+    0 .. active-1 are stepped."""
+
+    def __init__(self, params, ncase):
+        self.lib = _lib.load()
+        self.params = params
+        p = params
+        self.shape = (p.nx, p.nz, p.ny)
+        self.n3 = p.nx * p.ny * p.nz
+        self.ncase = int(ncase)
+        h = ctypes.c_void_p()
+        st = self.lib.st_create_batch(ctypes.byref(p), self.ncase, ctypes.byref(h))
+        if st != 0:
+            raise StError(st, "st_create_batch failed: " + self.lib.st_status_string(st).decode())
+        self._h = h
+        self.active = self.ncase
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self.lib.st_last_error(self._h).decode(errors="replace")
+            raise StError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.st_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_active(self, n):
+        self._check(self.lib.st_set_active(self._h, int(n)), "st_set_active")
+        self.active = int(n)
+
+    def start(self, k, Q, Y=None, time=0.0):
+        """Case k's state, time and step count 0, and its set-up before the
+        main loop (Compute_gamma, Compute_hyper)."""
+        self._check(self.lib.st_case_start(self._h, int(k), _addr(Q, 5 * self.n3),
+                                           None if Y is None else _addr(Y, self.n3), float(time)),
+                    "st_case_start")
+
+    def get(self, k, Q=None, Y=None):
+        """(Q, Y, time, step) of case k."""
+        Q = np.zeros((5,) + self.shape) if Q is None else Q
+        Y = np.zeros(self.shape) if Y is None else Y
+        t = ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(self.lib.st_case_get(self._h, int(k), _addr(Q, 5 * self.n3), _addr(Y, self.n3),
+                                         ctypes.byref(t), ctypes.byref(n)), "st_case_get")
+        return Q, Y, t.value, n.value
+
+    def move(self, src, dst):
+        self._check(self.lib.st_case_move(self._h, int(src), int(dst)), "st_case_move")
+
+    def step_async(self):
+        self._check(self.lib.st_batch_step_async(self._h), "st_batch_step_async")
+
+    def done(self):
+        r = self.lib.st_query(self._h)
+        if r < 0:
+            self._check(r, "st_query")
+        return r == 1
+
+    def sync(self):
+        self._check(self.lib.st_sync(self._h), "st_sync")
+
+    def memory_bytes(self):
+        b = ctypes.c_longlong()
+        self._check(self.lib.st_memory(self._h, ctypes.byref(b)), "st_memory")
+        return b.value
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        self._check(self.lib.st_launch_count(self._h, ctypes.byref(c)), "st_launch_count")
+        return c.value
+

@@ -53,6 +53,34 @@ void release(st_ctx *c, const void *p) {
         if (e.p == p) { e.used = false; return; }
 }
 
+// per-case device arrays of a context, offset together by CaseWindow
+template <class F>
+static void each_case_array(st_ctx *c, F f) {
+    double **d[] = {&c->Q, &c->dQ, &c->QW, &c->Y, &c->drYi, &c->rYW, &c->gamma_eff};
+    for (double **a : d) f(*a);
+    for (double *&a : c->grad) f(a);
+    for (double *&a : c->hyp) f(a);
+    for (double *&a : c->dYd) f(a);
+    float **fl[] = {&c->dQf, &c->drYif};
+    for (float **a : fl) f(*a);
+    for (float *&a : c->gradf) f(a);
+    for (float *&a : c->hypf) f(a);
+    for (float *&a : c->dYdf) f(a);
+}
+
+CaseWindow::CaseWindow(st_ctx *cc, int kk) : c(cc), k(kk), na0(cc->na) {
+    const size_t off = (size_t)k * c->dm.n3;
+    each_case_array(c, [&](auto *&a) { if (a) a += off; });
+    c->dscal += (size_t)k * kScal;
+    c->na = 1;
+}
+CaseWindow::~CaseWindow() {
+    const size_t off = (size_t)k * c->dm.n3;
+    each_case_array(c, [&](auto *&a) { if (a) a -= off; });
+    c->dscal -= (size_t)k * kScal;
+    c->na = na0;
+}
+
 // ---- argument staging ------------------------------------------------------
 // Each array argument is either used in place (device memory of the context's
 // device) or staged through a pooled device buffer (host memory).
@@ -98,7 +126,7 @@ class Args {
 
   private:
     struct Arg { const double *host; double *dev; int nf; bool in, out, staged; };
-    size_t bytes(int nf) const { return (size_t)nf * c_->dm.n3 * sizeof(double); }
+    size_t bytes(int nf) const { return (size_t)nf * c_->fs * sizeof(double); }
     st_ctx *c_;
     std::vector<Arg> v_;
     bool err_ = false;
@@ -119,6 +147,13 @@ using namespace st;
     } catch (const std::bad_alloc &) {                                          \
         return fail(c, ST_E_NOMEM, "host allocation failed");                  \
     }
+// entry points on one grid: a batch context (st_create_batch) takes the
+// st_case_* and st_batch_* calls instead
+#define SINGLE_CASE(c)                                                          \
+    do {                                                                        \
+        if ((c) && (c)->nb > 1)                                                 \
+            return fail(c, ST_E_UNSUPPORTED, "batch context: use the st_case_ and st_batch_ calls"); \
+    } while (0)
 
 extern "C" {
 
@@ -150,8 +185,10 @@ void st_default_params(st_params *p, int nx, int ny, int nz) {
     p->precision = ST_PRECISION_FP64;
 }
 
-int st_create(const st_params *p, st_ctx **out) {
-    if (!p || !out) return ST_E_ARG;
+int st_create(const st_params *p, st_ctx **out) { return st_create_batch(p, 1, out); }
+
+int st_create_batch(const st_params *p, int ncase, st_ctx **out) {
+    if (!p || !out || ncase < 1 || ncase > 1024) return ST_E_ARG;
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return ST_E_NODEVICE; }
@@ -171,6 +208,8 @@ int st_create(const st_params *p, st_ctx **out) {
     c->dev = p->device;
     c->dm.n[0] = p->nx; c->dm.n[1] = p->ny; c->dm.n[2] = p->nz;
     c->dm.n3 = (size_t)p->nx * p->ny * p->nz;
+    c->nb = c->na = ncase;
+    c->fs = (size_t)ncase * c->dm.n3;
     for (int d = 0; d < 3; d++) c->seg[d] = choose_seg(n[d]);
     auto bail = [&](int code, const char *m) { c->err = m; st_destroy(c); return code; };
     if (cudaSetDevice(c->dev) != cudaSuccess) return bail(ST_E_CUDA, "cudaSetDevice");
@@ -202,7 +241,7 @@ int st_create(const st_params *p, st_ctx **out) {
     }
     fill_consts(c->k);
     if (build_tables(c) != ST_OK) return bail(ST_E_NOMEM, "tables");
-    const size_t b = c->dm.n3 * sizeof(double);
+    const size_t b = c->fs * sizeof(double);      // one field of every case
     auto al = [&](double **q, int nf) { return cudaMalloc((void **)q, nf * b) == cudaSuccess &&
                                               cudaMemset(*q, 0, nf * b) == cudaSuccess; };
     auto alf = [&](float **q, int nf) { return cudaMalloc((void **)q, nf * b / 2) == cudaSuccess &&
@@ -219,12 +258,12 @@ int st_create(const st_params *p, st_ctx **out) {
         for (int h = 0; h < 4 && ok; h++) ok = al(&c->hyp[h], 1);
         for (int h = 0; h < 3 && ok; h++) ok = al(&c->dYd[h], 1);
     }
-    ok = ok && cudaMalloc((void **)&c->dscal, 16 * sizeof(double)) == cudaSuccess &&
-         cudaMemset(c->dscal, 0, 16 * sizeof(double)) == cudaSuccess &&
-         cudaMallocHost((void **)&c->hpinned, 16 * sizeof(double)) == cudaSuccess;
+    const size_t sb = (size_t)ncase * kScal * sizeof(double);
+    ok = ok && cudaMalloc((void **)&c->dscal, sb) == cudaSuccess && cudaMemset(c->dscal, 0, sb) == cudaSuccess &&
+         cudaMallocHost((void **)&c->hpinned, sb) == cudaSuccess;
     if (!ok) { cudaGetLastError(); return bail(ST_E_NOMEM, "device allocation of the COMMON blocks failed"); }
     if (p->family == ST_FAMILY_PERIODIC) {
-        if (dev_fill(c, c->gamma_eff, c->dm.n3, p->gamma1) != ST_OK || dev_fill(c, c->Y, c->dm.n3, 1.0) != ST_OK ||
+        if (dev_fill(c, c->gamma_eff, c->fs, p->gamma1) != ST_OK || dev_fill(c, c->Y, c->fs, 1.0) != ST_OK ||
             cudaStreamSynchronize(c->stream) != cudaSuccess)
             return bail(ST_E_CUDA, "initialising the single-fluid fields");
     }
@@ -239,6 +278,7 @@ int st_destroy(st_ctx *c) {
     for (auto &r : c->prec) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : c->evpool) cudaEventDestroy(e);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    for (auto g : c->batch_graphs) if (g) cudaGraphExecDestroy(g);
     free_tables(c);
     double *arrs[] = {c->Q, c->dQ, c->QW, c->Y, c->drYi, c->rYW, c->gamma_eff, c->dscal};
     for (double *a : arrs) if (a) cudaFree(a);
@@ -266,6 +306,7 @@ int st_sync(st_ctx *c) {
 
 // ---- state -------------------------------------------------------------------
 int st_set_state(st_ctx *c, const double *Q, const double *Y) {
+    SINGLE_CASE(c);
     if (!Q) return ST_E_ARG;
     if (!Y && (!c || c->p.family != ST_FAMILY_PERIODIC)) return ST_E_ARG;
     API_BEGIN(c)
@@ -289,6 +330,7 @@ int st_set_state(st_ctx *c, const double *Q, const double *Y) {
 }
 
 int st_get_state(st_ctx *c, double *Q, double *Y) {
+    SINGLE_CASE(c);
     API_BEGIN(c)
     const size_t b = c->dm.n3 * 8;
     if (Q) ST_CUDA(c, cudaMemcpyAsync(Q, c->Q, 5 * b, cudaMemcpyDefault, c->stream));
@@ -299,6 +341,7 @@ int st_get_state(st_ctx *c, double *Q, double *Y) {
 }
 
 int st_set_tstep(st_ctx *c, double t) {
+    SINGLE_CASE(c);
     API_BEGIN(c)
     c->Tstep = t;
     c->hpinned[6] = t;
@@ -309,6 +352,7 @@ int st_set_tstep(st_ctx *c, double t) {
 }
 
 int st_get_tstep(st_ctx *c, double *t) {
+    SINGLE_CASE(c);
     if (!t) return ST_E_ARG;
     API_BEGIN(c)
     ST_CUDA(c, cudaMemcpyAsync(c->hpinned + 6, c->dscal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -338,6 +382,7 @@ static double *common_ptr(st_ctx *c, const char *name, int *nf, float **pf) {
 }
 
 int st_get_common(st_ctx *c, const char *name, double *out) {
+    SINGLE_CASE(c);
     if (!name || !out) return ST_E_ARG;
     API_BEGIN(c)
     int nf;
@@ -358,6 +403,7 @@ int st_get_common(st_ctx *c, const char *name, double *out) {
 }
 
 int st_set_common(st_ctx *c, const char *name, const double *in) {
+    SINGLE_CASE(c);
     if (!name || !in) return ST_E_ARG;
     API_BEGIN(c)
     int nf;
@@ -433,6 +479,7 @@ static int family_ok(st_ctx *c, int asym) {
     do { int rc_ = family_ok(c, asym); if (rc_ != ST_OK) return rc_; } while (0)
 
 static int do_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd) {
+    SINGLE_CASE(c);
     if (!F || !dF || (iadd != 0 && iadd != 1)) return ST_E_ARG;
     if (!c) return ST_E_ARG;
     FAMILY_CHECK(c, asym);
@@ -446,6 +493,7 @@ static int do_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int
     API_END(c)
 }
 static int do_d2(st_ctx *c, int dir, int asym, const double *F, double *dF, double *d2F, int iadd) {
+    SINGLE_CASE(c);
     if (!F || !d2F || (iadd && !dF)) return ST_E_ARG;
     if (!c) return ST_E_ARG;
     FAMILY_CHECK(c, asym);
@@ -460,6 +508,7 @@ static int do_d2(st_ctx *c, int dir, int asym, const double *F, double *dF, doub
     API_END(c)
 }
 static int do_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) {
+    SINGLE_CASE(c);
     if (!F || !F0) return ST_E_ARG;
     if (!c) return ST_E_ARG;
     FAMILY_CHECK(c, asym);
@@ -473,6 +522,7 @@ static int do_filter(st_ctx *c, int dir, int asym, const double *F, double *F0) 
     API_END(c)
 }
 static int do_gauss(st_ctx *c, int dir, const double *F, double *Fg) {
+    SINGLE_CASE(c);
     if (!F || !Fg) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -521,6 +571,7 @@ int st_gaussian_filter_y(st_ctx *c, const double *F, double *Fg) { return do_gau
 int st_gaussian_filter_z(st_ctx *c, const double *F, double *Fg) { return do_gauss(c, 2, F, Fg); }
 
 int st_compact_filter(st_ctx *c, const double *F, double *F0, int nvar) {
+    SINGLE_CASE(c);
     if (!F || !F0 || nvar < 1) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -532,6 +583,7 @@ int st_compact_filter(st_ctx *c, const double *F, double *F0, int nvar) {
 }
 
 int st_gaussian_filter(st_ctx *c, const double *F, double *Fg, int nvar) {
+    SINGLE_CASE(c);
     if (!F || !Fg || nvar < 1) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -558,6 +610,7 @@ static int mf_only(st_ctx *c, const char *what) {
     do { int rc_ = mf_only(c, what); if (rc_ != ST_OK) return rc_; } while (0)
 
 int st_compute_gamma(st_ctx *c, const double *Y) {
+    SINGLE_CASE(c);
     if (!Y) return ST_E_ARG;
     MF_ONLY(c, "Compute_gamma");
     API_BEGIN(c)
@@ -568,6 +621,7 @@ int st_compute_gamma(st_ctx *c, const double *Y) {
 }
 
 int st_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
+    SINGLE_CASE(c);
     if (!Q || !Qrhs || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -580,6 +634,7 @@ int st_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
 }
 
 int st_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
+    SINGLE_CASE(c);
     if (!Q || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -591,6 +646,7 @@ int st_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
 }
 
 int st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
+    SINGLE_CASE(c);
     if (!Q || !Qrhs || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -603,6 +659,7 @@ int st_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
 }
 
 int st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    SINGLE_CASE(c);
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
     MF_ONLY(c, "Species_RHS");
     API_BEGIN(c)
@@ -617,6 +674,7 @@ int st_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, do
 }
 
 int st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs, double time) {
+    SINGLE_CASE(c);
     (void)time;
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
     MF_ONLY(c, "bc_RHS");
@@ -632,6 +690,7 @@ int st_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs,
 }
 
 int st_sponge_forcing(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
+    SINGLE_CASE(c);
     if (!Q || !Qrhs || !Y || !Yrhs) return ST_E_ARG;
     MF_ONLY(c, "Sponge_Forcing");
     API_BEGIN(c)
@@ -646,6 +705,7 @@ int st_sponge_forcing(st_ctx *c, const double *Q, double *Qrhs, const double *Y,
 }
 
 int st_fix_pressure(st_ctx *c, double *Q, const double *Y) {
+    SINGLE_CASE(c);
     (void)Y;
     if (!Q) return ST_E_ARG;
     API_BEGIN(c)
@@ -656,6 +716,7 @@ int st_fix_pressure(st_ctx *c, double *Q, const double *Y) {
 }
 
 int st_compute_cfl(st_ctx *c, const double *Q, double *cfl_stab, double *cfl_resv) {
+    SINGLE_CASE(c);
     if (!Q) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -666,6 +727,7 @@ int st_compute_cfl(st_ctx *c, const double *Q, double *cfl_stab, double *cfl_res
 }
 
 int st_compute_tstep(st_ctx *c, const double *Q, const double *Y, double cfl_resv, int step, double *tstep) {
+    SINGLE_CASE(c);
     if (!Q || y_missing(c, Y)) return ST_E_ARG;
     API_BEGIN(c)
     Args a(c);
@@ -689,6 +751,7 @@ static int read_time(st_ctx *c, double *time) {
 }
 
 int st_lddrk4(st_ctx *c, double *time, int *step) {
+    SINGLE_CASE(c);
     if (!time || !step) return ST_E_ARG;
     API_BEGIN(c)
     c->hpinned[7] = *time;
@@ -702,6 +765,7 @@ int st_lddrk4(st_ctx *c, double *time, int *step) {
 }
 
 int st_step(st_ctx *c, double *time, int *step) {
+    SINGLE_CASE(c);
     if (!time || !step) return ST_E_ARG;
     API_BEGIN(c)
     c->hpinned[7] = *time;
@@ -723,43 +787,171 @@ static int enqueue_step(st_ctx *c, int step) {
     return ST_OK;
 }
 
+}  // extern "C"
+
+// captures fn's launches on the context stream into *out (kernels counted in *nk)
+template <class Fn>
+static int capture_graph(st_ctx *c, cudaGraphExec_t *out, long long *nk, Fn fn) {
+    cudaGraph_t g = nullptr;
+    const long long l0 = c->launches;
+    ST_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = fn();
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->launches = l0;
+    if (rc != ST_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(c, ST_E_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+    long long k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    *nk = k;
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { *out = nullptr; return fail(c, ST_E_CUDA, cudaGetErrorString(e)); }
+    return ST_OK;
+}
+
+extern "C" {
+
 int st_step_async(st_ctx *c, int step) {
     if (step < 0) return ST_E_ARG;
+    if (c && c->nb > 1) return st_batch_step_async(c);
     API_BEGIN(c)
     // Compute_Tstep's branch depends on the step number only up to step 2;
     // from then on every step is the same sequence of launches on the same
     // buffers, captured once as a CUDA graph and replayed.
     if (step < 2 || c->prof) return enqueue_step(c, step);
-    if (!c->step_graph) {
-        cudaGraph_t g = nullptr;
-        const long long l0 = c->launches;
-        ST_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(c, step);
-        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-        c->launches = l0;
-        if (rc != ST_OK) { if (g) cudaGraphDestroy(g); return rc; }
-        if (e != cudaSuccess) return fail(c, ST_E_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
-        size_t nn = 0;
-        cudaGraphGetNodes(g, nullptr, &nn);
-        std::vector<cudaGraphNode_t> nodes(nn);
-        if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
-        long long nk = 0;
-        for (auto nd : nodes) {
-            cudaGraphNodeType t;
-            if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) nk++;
-        }
-        c->graph_kernels = nk;
-        e = cudaGraphInstantiate(&c->step_graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) { c->step_graph = nullptr; return fail(c, ST_E_CUDA, cudaGetErrorString(e)); }
-    }
+    if (!c->step_graph) ST_TRY(capture_graph(c, &c->step_graph, &c->graph_kernels, [&] { return enqueue_step(c, step); }));
     ST_CUDA(c, cudaGraphLaunch(c->step_graph, c->stream));
     c->launches += c->graph_kernels;
     return ST_OK;
     API_END(c)
 }
 
+// ---- batches of same-size cases ----------------------------------------------
+static int case_ok(st_ctx *c, int k) {
+    if (k < 0 || k >= c->nb) return fail(c, ST_E_ARG, "case index out of range");
+    return ST_OK;
+}
+
+int st_batch_info(st_ctx *c, int *ncase, int *nactive) {
+    if (!c) return ST_E_ARG;
+    if (ncase) *ncase = c->nb;
+    if (nactive) *nactive = c->na;
+    return ST_OK;
+}
+
+int st_set_active(st_ctx *c, int nactive) {
+    if (!c || nactive < 1 || nactive > c->nb) return ST_E_ARG;
+    c->na = nactive;
+    return ST_OK;
+}
+
+int st_case_start(st_ctx *c, int k, const double *Q, const double *Y, double time) {
+    if (!c || !Q) return ST_E_ARG;
+    if (!Y && c->p.family != ST_FAMILY_PERIODIC) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_TRY(case_ok(c, k));
+    CaseWindow w(c, k);
+    const size_t b = c->dm.n3 * 8;
+    for (int l = 0; l < 5; l++)
+        ST_CUDA(c, cudaMemcpyAsync(c->Q + l * c->fs, Q + l * c->dm.n3, b, cudaMemcpyDefault, c->stream));
+    if (c->p.family != ST_FAMILY_PERIODIC) ST_CUDA(c, cudaMemcpyAsync(c->Y, Y, b, cudaMemcpyDefault, c->stream));
+    // scalars: time, step count 0 (time step and reductions are recomputed)
+    c->hpinned[0] = time;
+    ST_CUDA(c, cudaMemsetAsync(c->dscal, 0, kScal * sizeof(double), c->stream));
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + SC_TIME, c->hpinned, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // the set-up before the main loop, src/main_mf.f:100-101 (src/main.f:100)
+    if (c->p.family != ST_FAMILY_PERIODIC) ST_TRY(dev_compute_gamma(c, c->Y));
+    ST_TRY(dev_compute_hyper(c, c->Q, c->Y));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_case_get(st_ctx *c, int k, double *Q, double *Y, double *time, int *step) {
+    if (!c) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_TRY(case_ok(c, k));
+    const size_t b = c->dm.n3 * 8, off = (size_t)k * c->dm.n3;
+    if (Q)
+        for (int l = 0; l < 5; l++)
+            ST_CUDA(c, cudaMemcpyAsync(Q + l * c->dm.n3, c->Q + l * c->fs + off, b, cudaMemcpyDefault, c->stream));
+    if (Y) ST_CUDA(c, cudaMemcpyAsync(Y, c->Y + off, b, cudaMemcpyDefault, c->stream));
+    ST_CUDA(c, cudaMemcpyAsync(c->hpinned, c->dscal + (size_t)k * kScal, kScal * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (time) *time = c->hpinned[SC_TIME];
+    if (step) *step = (int)c->hpinned[SC_STEP];
+    return ST_OK;
+    API_END(c)
+}
+
+int st_case_move(st_ctx *c, int src, int dst) {
+    if (!c) return ST_E_ARG;
+    API_BEGIN(c)
+    ST_TRY(case_ok(c, src));
+    ST_TRY(case_ok(c, dst));
+    if (src == dst) return ST_OK;
+    const size_t n3 = c->dm.n3, so = (size_t)src * n3, d = (size_t)dst * n3;
+    auto mv = [&](auto *a, int nf) -> int {
+        if (!a) return ST_OK;
+        const size_t es = sizeof(*a);
+        for (int l = 0; l < nf; l++)
+            ST_CUDA(c, cudaMemcpyAsync(a + l * c->fs + d, a + l * c->fs + so, n3 * es, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+        return ST_OK;
+    };
+    // the state and what the next step reads before recomputing it: gamma_eff
+    // (Compute_CFL) and /HYPER/ (Compute_Tstep)
+    ST_TRY(mv(c->Q, 5));
+    ST_TRY(mv(c->Y, 1));
+    ST_TRY(mv(c->gamma_eff, 1));
+    for (int h = 0; h < 4; h++) { ST_TRY(mv(c->hyp[h], 1)); ST_TRY(mv(c->hypf[h], 1)); }
+    ST_CUDA(c, cudaMemcpyAsync(c->dscal + (size_t)dst * kScal, c->dscal + (size_t)src * kScal,
+                               kScal * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    ST_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ST_OK;
+    API_END(c)
+}
+
+// one main-loop step of every active case; each case's Compute_Tstep takes
+// its own step count from its scalars
+static int enqueue_batch_step(st_ctx *c) {
+    ST_TRY(dev_compute_cfl(c, c->Q, false, nullptr, nullptr));
+    ST_TRY(dev_compute_tstep(c, c->Q, c->Y, -1, true, 0.0));
+    ST_TRY(dev_lddrk4(c, true));
+    return ST_OK;
+}
+
+int st_batch_step_async(st_ctx *c) {
+    API_BEGIN(c)
+    // the first step runs eagerly: it sizes the scratch pool, which a
+    // captured graph then reuses (no allocation happens inside a capture)
+    if (c->prof || !c->batch_warm) {
+        ST_TRY(enqueue_batch_step(c));
+        c->batch_warm = true;
+        return ST_OK;
+    }
+    if ((int)c->batch_graphs.size() < c->nb) {
+        c->batch_graphs.assign(c->nb, nullptr);
+        c->batch_graph_kernels.assign(c->nb, 0);
+    }
+    cudaGraphExec_t &g = c->batch_graphs[c->na - 1];
+    if (!g) ST_TRY(capture_graph(c, &g, &c->batch_graph_kernels[c->na - 1], [&] { return enqueue_batch_step(c); }));
+    ST_CUDA(c, cudaGraphLaunch(g, c->stream));
+    c->launches += c->batch_graph_kernels[c->na - 1];
+    return ST_OK;
+    API_END(c)
+}
+
 int st_get_time(st_ctx *c, double *time) {
+    SINGLE_CASE(c);
     if (!time) return ST_E_ARG;
     API_BEGIN(c)
     return read_time(c, time);
@@ -767,6 +959,7 @@ int st_get_time(st_ctx *c, double *time) {
 }
 
 int st_set_time(st_ctx *c, double time) {
+    SINGLE_CASE(c);
     API_BEGIN(c)
     c->hpinned[7] = time;
     ST_CUDA(c, cudaMemcpyAsync(c->dscal + 7, c->hpinned + 7, sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -777,11 +970,11 @@ int st_set_time(st_ctx *c, double time) {
 
 int st_memory(st_ctx *c, long long *bytes) {
     if (!c || !bytes) return ST_E_ARG;
-    const size_t fb = c->dm.n3 * sizeof(double);
+    const size_t fb = c->fs * sizeof(double);
     // COMMON mirrors (13 double state fields; 25 intermediate fields, float in
     // the FP32 mode), tables, scalars and the scratch pool
     const size_t ib = fp32_mode(c) ? fb / 2 : fb;
-    size_t b = 13 * fb + 25 * ib + c->table_bytes + 16 * sizeof(double);
+    size_t b = 13 * fb + 25 * ib + c->table_bytes + (size_t)c->nb * kScal * sizeof(double);
     for (auto &e : c->pool) b += e.bytes;
     *bytes = (long long)b;
     return ST_OK;
@@ -855,6 +1048,7 @@ int st_profile_report(st_ctx *c, char *buf, int buflen) {
 
 // ---- Output-side diagnostics -------------------------------------------------
 int st_compute_grad(st_ctx *c, double *Grad, double *maxdil, double *enstrophy) {
+    SINGLE_CASE(c);
     if (!maxdil || !enstrophy) return ST_E_ARG;
     MF_ONLY(c, "Compute_Grad");
     API_BEGIN(c)
@@ -872,6 +1066,7 @@ int st_shell_count(st_ctx *c, int *n_avg) {
 }
 
 int st_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg) {
+    SINGLE_CASE(c);
     if (!hmix || !tke_total) return ST_E_ARG;
     MF_ONLY(c, "Compute_SRM_Stats");
     API_BEGIN(c)
@@ -881,6 +1076,7 @@ int st_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_
 }
 
 int st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms) {
+    SINGLE_CASE(c);
     if (!rad_avg || !rad_skew_rms) return ST_E_ARG;
     MF_ONLY(c, "Generate_Shock_Surface");
     API_BEGIN(c)
@@ -890,6 +1086,7 @@ int st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms) 
 }
 
 int st_get_monitors(st_ctx *c, double out[10]) {
+    SINGLE_CASE(c);
     if (!out) return ST_E_ARG;
     API_BEGIN(c)
     ST_TRY(dev_monitors(c));

@@ -108,14 +108,25 @@ enum { H_BETA, H_VISC, H_K, H_D };
 
 struct Dims {
     int n[3];          // Mx, My, Mz
-    size_t n3;
+    size_t n3;         // cells of one case
 };
+
+// Device scalars of one case: a block of kScal doubles (dscal + k*kScal)
+constexpr int kScal = 16;
+enum { SC_STAB = 0, SC_RESV = 1, SC_DT = 6, SC_TIME = 7, SC_STEP = 8 };
 
 }  // namespace st
 
 struct st_ctx {
     st_params p;
     st::Dims dm;
+    // Batches of same-size cases: every field holds nb consecutive blocks of
+    // dm.n3 cells (field f of case k at f*fs + k*dm.n3), so one launch of a
+    // line or pointwise kernel covers every case.  Cases 0 .. na-1 are
+    // processed.  A single-case context has nb = na = 1 and fs = dm.n3.
+    int nb = 1, na = 1;
+    size_t fs = 0;     // field stride: nb * dm.n3
+    size_t ncell() const { return (size_t)na * dm.n3; }   // cells the kernels process
     int seg[3];        // rows per segment along x, y, z
     int dev = 0;
     cudaStream_t stream = nullptr;
@@ -153,8 +164,8 @@ struct st_ctx {
     std::vector<PoolEntry> pool;
     bool pool_oom = false;
     // device scalars (reductions, dt)
-    double *dscal = nullptr;     // [16]
-    double *hpinned = nullptr;   // pinned host mirror [16]
+    double *dscal = nullptr;     // [nb][kScal]
+    double *hpinned = nullptr;   // pinned host mirror [nb][kScal]
     // host<->device staging for the per-operator entry points
     std::vector<double *> stage;
     cudaStream_t own_stream = nullptr;
@@ -162,6 +173,9 @@ struct st_ctx {
     long long launches = 0;
     cudaGraphExec_t step_graph = nullptr;   // captured main-loop step (st_step_async)
     long long graph_kernels = 0;            // kernels in one replay of step_graph
+    std::vector<cudaGraphExec_t> batch_graphs;   // batch step per active count (index na - 1)
+    std::vector<long long> batch_graph_kernels;
+    bool batch_warm = false;                     // a batch step has run eagerly (scratch pool sized)
     bool prof = false;
     struct ProfRec { const char *name; double bytes; cudaEvent_t a, b; };
     std::vector<ProfRec> prec;
@@ -196,11 +210,23 @@ void fill_consts(Consts &k);
 
 // scratch pool
 void *scratch_bytes(st_ctx *c, size_t bytes);
-inline double *scratch(st_ctx *c, int nfields = 1) {   // nfields contiguous N^3 double fields
-    return (double *)scratch_bytes(c, (size_t)nfields * c->dm.n3 * sizeof(double));
+inline double *scratch(st_ctx *c, int nfields = 1) {   // nfields contiguous fields (of every case)
+    return (double *)scratch_bytes(c, (size_t)nfields * c->fs * sizeof(double));
 }
 template <class R>
-inline R *scratch_t(st_ctx *c, int nfields) { return (R *)scratch_bytes(c, (size_t)nfields * c->dm.n3 * sizeof(R)); }
+inline R *scratch_t(st_ctx *c, int nfields) { return (R *)scratch_bytes(c, (size_t)nfields * c->fs * sizeof(R)); }
+
+// The context narrowed to case k of a batch while it lives: every per-case
+// device pointer (state, COMMON mirrors, scalars) points at case k's block
+// and one case is processed.  Scratch fields keep their stride.
+struct CaseWindow {
+    st_ctx *c;
+    int k, na0;
+    CaseWindow(st_ctx *cc, int kk);
+    ~CaseWindow();
+    CaseWindow(const CaseWindow &) = delete;
+    CaseWindow &operator=(const CaseWindow &) = delete;
+};
 void release(st_ctx *c, const void *p);
 template <class R>
 struct ScratchT {                                // RAII helper

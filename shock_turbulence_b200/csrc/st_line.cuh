@@ -55,11 +55,17 @@ struct ColMap {
 };
 struct LineGeo {
     int dir, n, My, Mz;
+    // batches: blocks of CTAs per case (set by the launcher for its lines per
+    // block) and the cells of a case; block blk works on case blk / cblk
+    unsigned cblk;
+    size_t cstride;
     // W lines per thread: a CTA owns kLanes*W lines
     template <int W>
     __device__ __forceinline__ ColMap map(unsigned blk) const {
         constexpr int NL = kLanes * W;
         ColMap m;
+        const unsigned cs = blk / cblk;
+        blk -= cs * cblk;
         const size_t sMy = My, sMz = Mz, jb = My / NL;
         if (dir == 0) {            // lines (j,k): NL consecutive j at one k
             m.base = (blk % jb) * NL + sMy * (blk / jb); m.lstride = 1; m.rstride = sMy * sMz;
@@ -68,6 +74,7 @@ struct LineGeo {
         } else {                   // lines (j,i): NL consecutive j at one i
             m.base = (blk % jb) * NL + sMy * sMz * (blk / jb); m.lstride = 1; m.rstride = sMy;
         }
+        m.base += (size_t)cs * cstride;
         return m;
     }
 };

@@ -91,15 +91,19 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// The tile of NL lines with index blk (LineGeo::map for NL lines per tile):
-// element (line l, row r) at base + l*lstride + r*rstride.
+// The tile of NL lines with index blk (LineGeo::map for NL lines per tile;
+// g.cblk tiles per case of a batch): element (line l, row r) at
+// base + l*lstride + r*rstride.
 template <int NL>
 __device__ __forceinline__ ColMap tile_map(const LineGeo &g, unsigned blk) {
     ColMap m;
+    const unsigned cs = blk / g.cblk;      // case of a batch
+    blk -= cs * g.cblk;
     const size_t sMy = g.My, sMz = g.Mz, jb = g.My / NL;
     if (g.dir == 0) { m.base = (blk % jb) * NL + sMy * (blk / jb); m.lstride = 1; m.rstride = sMy * sMz; }
     else if (g.dir == 1) { m.base = sMy * (size_t)blk * NL; m.lstride = sMy; m.rstride = 1; }
     else { m.base = (blk % jb) * NL + sMy * sMz * (blk / jb); m.lstride = 1; m.rstride = sMy; }
+    m.base += (size_t)cs * g.cstride;
     return m;
 }
 

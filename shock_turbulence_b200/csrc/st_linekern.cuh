@@ -209,10 +209,13 @@ inline bool whole_line_kernels_enabled() {
 }
 
 template <int S, int KIND, int OP, int KW, class T>
-static void launch_whole(st_ctx *c, const LineArgsT<T> &a, cudaStream_t st) {
+static void launch_whole(st_ctx *c, const LineArgsT<T> &a0, cudaStream_t st) {
     using RG = lk2::Ring<S, KIND, OP, KW, T>;
     constexpr int NL = KW * lk2::Elt<T>::LPW;
-    const unsigned ntiles = (unsigned)(c->dm.n3 / (size_t)a.geo.n / NL);
+    LineArgsT<T> a = a0;
+    a.geo.cblk = (unsigned)(c->dm.n3 / (size_t)a.geo.n / NL);       // tiles per case
+    a.geo.cstride = c->dm.n3;
+    const unsigned ntiles = a.geo.cblk * (unsigned)c->na;
     set_smem<lk2::k_line2<S, KIND, OP, KW, T>>(RG::kSmem);
     static int per_sm = 0;     // resident CTAs per SM of this instantiation
     if (!per_sm) {
@@ -264,13 +267,16 @@ static bool try_whole(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t 
 }
 
 template <int S, bool YT, bool CYC, class T>
-static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t st) {
-    const size_t nlines = c->dm.n3 / (size_t)a.geo.n;
+static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a0, cudaStream_t st) {
+    const size_t nlines = c->dm.n3 / (size_t)a0.geo.n;     // lines of one case
     constexpr int NL = kLanes * Val<T>::W;
-    dim3 grid((unsigned)(nlines / NL)), block(kLanes * a.P);
+    LineArgsT<T> a = a0;
+    a.geo.cblk = (unsigned)(nlines / NL);                  // CTAs per case
+    a.geo.cstride = c->dm.n3;
+    dim3 grid(a.geo.cblk * (unsigned)c->na), block(kLanes * a.P);
     const size_t smem = YT ? (size_t)NL * (a.geo.n + 1) * sizeof(T) : 0;
     // algorithmic bytes: every input and output field touched once
-    const double n3 = (double)c->dm.n3;
+    const double n3 = (double)c->ncell();
     // inputs: 1 field, or every field a producer expression reads
     static const int nin[6] = {1, 2, 3, 3, 3, 4};
     const double es = (double)sizeof(T);

@@ -163,7 +163,7 @@ int dev_to_double(st_ctx *c, const float *x, double *y, size_t n) {
 int dev_compute_gamma(st_ctx *c, const double *Y) {
     Phys f = phys(c);
     double *ge = c->gamma_eff;
-    PFOR(c, c->dm.n3, io(Y, ge), {
+    PFOR(c, c->ncell(), io(Y, ge), {
         double fac1 = f.g1 - 1.0, fac2 = f.g2 - 1.0;
         double num = (Y[p] * f.g1 / fac1) + (f.eps * (1.0 - Y[p]) * f.g2 / fac2);
         double den = (Y[p] / fac1) + (f.eps * (1.0 - Y[p]) / fac2);
@@ -192,7 +192,7 @@ int dev_compute_gamma(st_ctx *c, const double *Y) {
 // derivative operands come from Qr, the pointwise thermodynamics from Q.
 template <class R>
 static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     const Phys f = phys(c);
     // src/rhsv_periodic_sf.f:1381 adds Qvisc unconditionally
     const bool visc = c->p.re > 0.0 || c->p.family == ST_FAMILY_PERIODIC;
@@ -216,7 +216,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     // ---- RHS_x (src/rhsv_sym_mf.f:37-481)
     // P, T, u, and (the same expressions the reference evaluates later from
     // the same inputs) v, w, mu, dmu/dT
-    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, P, T, u, v, w, mu, dmu), {
+    PFOR(c, nc, io(g, Y, Q1, Q2, Q3, Q4, Q5, P, T, u, v, w, mu, dmu), {
         double vs, pp, tt, m, dm;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], vs, pp, tt);
         P[p] = pp; T[p] = tt;
@@ -250,7 +250,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     // and the x part of Qvisc, in the reference's order of accumulation
     {
         const double Pri = f.Pr_inv, fac1 = 4.0 / 3.0 + f.bulk;
-        PFOR(c, n3, io(FF, u, v, w, Q4, Gxx, Gyx, Gzx) + 6 * io(Qcx) + (visc ? io(mu, dTx, dmu, GTx, duxx, dvxx, dwxx) + 4 * io(Qv) : 0.0), {
+        PFOR(c, nc, io(FF, u, v, w, Q4, Gxx, Gyx, Gzx) + 6 * io(Qcx) + (visc ? io(mu, dTx, dmu, GTx, duxx, dvxx, dwxx) + 4 * io(Qv) : 0.0), {
             double fac2 = -5.0e-1 * FF[p];
             double c1 = Qcx[p] + fac2 * u[p];
             double c2 = Qcx[n3 + p] + fac2 * v[p];
@@ -326,7 +326,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
         const double Pri = f.Pr_inv;
         const double fb43 = f.bulk + 4.0 / 3.0, fb23 = f.bulk - 2.0 / 3.0, fb13 = f.bulk + 1.0 / 3.0;
         const bool fp64 = is_fp64<R>();
-        PFOR(c, n3, io(u, v, w, Q4, Gxx, Gyx, Gzx, Gxy, Gyy, Gzy, Gxz, Gyz, Gzz) + 5 * io(Qcx, Qcy, Qcz, Qrhs) + (fp64 ? io(Q1, Q2, Q3) : 0.0) + (visc ? io(mu, dmu, d2Ty, d2Tz, GTy, GTz, GTx, d2uy, d2vy, d2wy, dGzz_y, d2wz, d2uz, d2vz, dGyx_y, dGzx_z, dGxx_y, dGxx_z, dGyz_y) + 4 * io(Qv) : 0.0), {
+        PFOR(c, nc, io(u, v, w, Q4, Gxx, Gyx, Gzx, Gxy, Gyy, Gzy, Gxz, Gyz, Gzz) + 5 * io(Qcx, Qcy, Qcz, Qrhs) + (fp64 ? io(Q1, Q2, Q3) : 0.0) + (visc ? io(mu, dmu, d2Ty, d2Tz, GTy, GTz, GTx, d2uy, d2vy, d2wy, dGzz_y, d2wz, d2uz, d2vz, dGyx_y, dGzx_z, dGxx_y, dGxx_z, dGyz_y) + 4 * io(Qv) : 0.0), {
             const double uu = u[p], vv = v[p], ww = w[p], q4 = Q4[p];
             // -0.5*d(rho v)/dy = 0.5*Qconvy(4) exactly (cadd flips only the sign)
             double fac2 = -5.0e-1 * (-(double)Qcy[3 * n3 + p]);
@@ -416,7 +416,7 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
 // Gaussian_Filter src/filters_sym.f:1046-1071
 template <class R>
 static int gaussian_filter_t(st_ctx *c, const R *F, R *Fg, int nvar) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<R> tmp(c);
     R *t = tmp;
     for (int l = 0; l < nvar; l++) {
@@ -460,13 +460,13 @@ static int laplacian(st_ctx *c, const R *S, R *d2S) {
 // first one's (same input, same arithmetic) and is filtered once.
 template <class R>
 static int compute_hyper_sf(st_ctx *c, const double *Q) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     const double gam = c->p.gamma1;
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     ScratchNT<R> s(c, 14);
     R *U1 = s[0], *U2 = s[1], *U3 = s[2], *W1 = s[3], *W2 = s[4], *W3 = s[5], *Dl = s[6];
     R *Cbeta = s[7], *S = s[8], *e = s[9], *T = s[10], *d2 = s[11], *d4S = s[12], *d4e = s[13];
-    PFOR(c, n3, io(Q1, Q2, Q3, Q4, U1, U2, U3), {
+    PFOR(c, nc, io(Q1, Q2, Q3, Q4, U1, U2, U3), {
         double t = 1.0 / Q4[p];
         U1[p] = Q1[p] * t; U2[p] = Q2[p] * t; U3[p] = Q3[p] * t;
     });
@@ -484,7 +484,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
             *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
     R *P = U1, *Vs = U2;   // the velocities are dead from here on
-    PFOR(c, n3, io(Dl, W1, W2, W3, G0, G1, G2, G3, G4, G5, G6, G7, G8, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
+    PFOR(c, nc, io(Dl, W1, W2, W3, G0, G1, G2, G3, G4, G5, G6, G7, G8, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
         double eps = 1.0e-7, fac2 = 10.0;
         double dil = Dl[p];
         double fac = 5.0e-1 * (1.0 - tanh(2.5 + fac2 * dil));
@@ -510,7 +510,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     ST_TRY(laplacian(c, d2, d4e));
     ScratchT<R> etas(c, 4);
     R *eta = etas, *etag = eta + 2 * n3;   // [rho|d4S|, fac3|d4e|] and their filtered values
-    PFOR(c, n3, io(Q4, T, P, Vs, d4S, d4e) + 2 * io(eta), {
+    PFOR(c, nc, io(Q4, T, P, Vs, d4S, d4e) + 2 * io(eta), {
         double fac3 = (Q4[p] / T[p]) * sqrt(gam * P[p] * Vs[p]);
         eta[p] = Q4[p] * fabs(d4S[p]);
         eta[n3 + p] = fac3 * fabs(d4e[p]);
@@ -520,7 +520,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
     const double C_mu = 2.0e-3, C_k = 1.0e-2;
     R **H = Store<R>::hyp(c);
     R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K];
-    PFOR(c, n3, io(Cbeta, hb, hv, hk) + 2 * io(etag), {
+    PFOR(c, nc, io(Cbeta, hb, hv, hk) + 2 * io(etag), {
         hb[p] = Cbeta[p] * etag[p] * DX6;
         hv[p] = C_mu * etag[p] * DX6;
         hk[p] = C_k * etag[n3 + p] * DX5;
@@ -532,7 +532,7 @@ static int compute_hyper_sf(st_ctx *c, const double *Q) {
 template <class R>
 static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R *Yr) {
     if (c->p.family == ST_FAMILY_PERIODIC) return compute_hyper_sf<R>(c, Q);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     ScratchNT<R> s(c, 10);
@@ -546,7 +546,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
             *G7 = Gr[7], *G8 = Gr[8];
     const double scale = c->p.c_beta_scale;
     {
-        PFOR(c, n3, io(G0, G1, G2, G3, G4, G5, G6, G7, G8, g, Y, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
+        PFOR(c, nc, io(G0, G1, G2, G3, G4, G5, G6, G7, G8, g, Y, Q1, Q2, Q3, Q4, Q5, Cbeta, Vs, P, T, e, S), {
             // G0..G8 = dux_dx, duy_dx, duz_dx, dux_dy, duy_dy, duz_dy, dux_dz, duy_dz, duz_dz
             double w1 = G5[p] - G7[p];
             double w2 = G6[p] - G2[p];
@@ -579,7 +579,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
         ST_TRY(laplacian(c, Yr, d2));
         ST_TRY(laplacian(c, d2, d4Y));
         const double C_mu = 2.0e-3, C_k = 1.0e-2;
-        PFOR(c, n3, io(d4S, d4e, d4Y, g, P, Vs, Q4, T, Cbeta, Y) + 5 * io(eta), {
+        PFOR(c, nc, io(d4S, d4e, d4Y, g, P, Vs, Q4, T, Cbeta, Y) + 5 * io(eta), {
             double a4S = fabs(d4S[p]), a4e = fabs(d4e[p]), a4Y = fabs(d4Y[p]);
             double cs = sqrt(g[p] * P[p] * Vs[p]);
             double fac3 = (Q4[p] / T[p]) * sqrt(g[p] * P[p] * Vs[p]);
@@ -596,7 +596,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
         const double C_D = 1.0e-4, C_Y = 100.0;
         R **H = Store<R>::hyp(c);
         R *hb = H[H_BETA], *hv = H[H_VISC], *hk = H[H_K], *hd = H[H_D];
-        PFOR(c, n3, 5 * io(etag) + io(hb, hv, hk, hd), {
+        PFOR(c, nc, 5 * io(etag) + io(hb, hv, hk, hd), {
             hb[p] = etag[2 * n3 + p] * DX6;
             hv[p] = etag[p] * DX6;
             hk[p] = etag[n3 + p] * DX5;
@@ -613,7 +613,7 @@ static int compute_hyper_t(st_ctx *c, const double *Q, const double *Y, const R 
 template <class R>
 static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, const R *Yr) {
     if (c->p.hyper_param == 0) return ST_OK;
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ST_TRY(compute_hyper_t<R>(c, Q, Y, Yr));
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3;
     ScratchNT<R> s(c, 9);
@@ -628,7 +628,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     const R *GTx = Gr[G_DTDX], *GTy = Gr[G_DTDY], *GTz = Gr[G_DTDZ];
     R *const *H = Store<R>::hyp(c);
     const R *vh = H[H_VISC], *bh = H[H_BETA], *kh = H[H_K];
-    PFOR(c, n3, io(Q1, Q2, Q3, Q4, G0, G1, G2, G3, G4, G5, G6, G7, G8, vh, bh, U1, U2, U3, dila, S1, S2, S3, Flux, Flux2), {
+    PFOR(c, nc, io(Q1, Q2, Q3, Q4, G0, G1, G2, G3, G4, G5, G6, G7, G8, vh, bh, U1, U2, U3, dila, S1, S2, S3, Flux, Flux2), {
         U1[p] = Q1[p] / Q4[p];
         U2[p] = Q2[p] / Q4[p];
         U3[p] = Q3[p] / Q4[p];
@@ -654,7 +654,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     ST_TRY(dfd(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
     ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
     // z momentum
-    PFOR(c, n3, io(vh, G8, bh, dila, Flux), { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
+    PFOR(c, nc, io(vh, G8, bh, dila, Flux), { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
     ST_TRY(dfd(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
     ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
     ST_TRY(dfd(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
@@ -665,7 +665,7 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
     ST_TRY(dfd(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
     ST_TRY(dfd(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
     ST_TRY(dfd(c, 2, 0, pr_mul(kh, GTz), h5, 1, 1.0));
-    PFOR(c, n3, 4 * io(Qrhs, Qrhs, Qh), {
+    PFOR(c, nc, 4 * io(Qrhs, Qrhs, Qh), {
         for (int l = 0; l < 5; l++)
             if (l != 3) Qrhs[l * n3 + p] = Qrhs[l * n3 + p] + Qh[l * n3 + p];
     });
@@ -679,7 +679,7 @@ template <class R>
 static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const double *Y, const R *Yr,
                          R *Yrhs) {
     if (c->p.hyper_param == 0) return ST_OK;
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     Phys f = phys(c);
     const double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const R *q1r = Qr, *q2r = Qr + n3, *q3r = Qr + 2 * n3, *q4r = Qr + 3 * n3;
@@ -688,7 +688,7 @@ static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const
     R *const *dYd = Store<R>::dYd(c);
     const R *Dh = Store<R>::hyp(c)[H_D];
     const double *g = c->gamma_eff;
-    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, T), {
+    PFOR(c, nc, io(g, Y, Q1, Q2, Q3, Q4, Q5, T), {
         double Vs, P, Tt;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, P, Tt);
         T[p] = Tt;
@@ -708,29 +708,40 @@ static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const
         ST_TRY(dfd(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
         ST_TRY(dfd(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
     }
-    PFOR(c, n3, io(Yrhs, Yrhs, Yd), { Yrhs[p] = Yrhs[p] + Yd[p]; });
+    PFOR(c, nc, io(Yrhs, Yrhs, Yd), { Yrhs[p] = Yrhs[p] + Yd[p]; });
     return ST_OK;
 }
 
 // bc_RHS src/bc_mf.f:11-463 (active face blocks)
 template <class R>
 static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     const int Mx = c->dm.n[0], My = c->dm.n[1], Mz = c->dm.n[2];
     Phys f = phys(c);
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
     // symmetry planes: x=0 (rho u), z=0 (rho w), y=0 (rho v); one launch per
     // plane over its cells only
+    // (each plane of every processed case: case k's cells start at k*n3c)
+    const size_t n3c = c->dm.n3, na = (size_t)c->na;
     {
-        const size_t MyMz = (size_t)My * Mz;
-        PFOR(c, MyMz, io(Q1), { Q1[p] = 0.0; });                                          // i = 0: p = j + My*k
-        PFOR(c, (size_t)My * Mx, io(Q3), { Q3[(p % My) + MyMz * (p / My)] = 0.0; });      // k = 0: p = j + My*i
-        PFOR(c, (size_t)Mz * Mx, io(Q2), { Q2[(size_t)My * p] = 0.0; });                  // j = 0: p = k + Mz*i
+        const size_t MyMz = (size_t)My * Mz, MyMx = (size_t)My * Mx, MzMx = (size_t)Mz * Mx;
+        PFOR(c, na * MyMz, io(Q1), {                                          // i = 0: p = j + My*k
+            size_t k = p / MyMz;
+            Q1[k * n3c + (p - k * MyMz)] = 0.0;
+        });
+        PFOR(c, na * MyMx, io(Q3), {                                          // k = 0: p = j + My*i
+            size_t k = p / MyMx, q = p - k * MyMx;
+            Q3[k * n3c + (q % My) + MyMz * (q / My)] = 0.0;
+        });
+        PFOR(c, na * MzMx, io(Q2), {                                          // j = 0: p = k + Mz*i
+            size_t k = p / MzMx;
+            Q2[k * n3c + (size_t)My * (p - k * MzMx)] = 0.0;
+        });
     }
     ScratchNT<R> s(c, 4);
     R *P = s[0], *dPx = s[1], *dPy = s[2], *dPz = s[3];
-    PFOR(c, n3, io(g, Y, Q1, Q2, Q3, Q4, Q5, P), {
+    PFOR(c, nc, io(g, Y, Q1, Q2, Q3, Q4, Q5, P), {
         double Vs, Pp, T;
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, Pp, T);
         P[p] = Pp;
@@ -743,11 +754,13 @@ static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
     // faces in the reference order x, y, z (later faces overwrite edges)
     for (int face = 0; face < 3; face++) {
         size_t nf = face == 0 ? (size_t)My * Mz : face == 1 ? (size_t)Mx * Mz : (size_t)Mx * My;
-        PFOR(c, nf, io(Q1, Q2, Q3, Q4, P, g, dPx, Gxx, Yrhs) + 5 * io(Qrhs), {
+        PFOR(c, na * nf, io(Q1, Q2, Q3, Q4, P, g, dPx, Gxx, Yrhs) + 5 * io(Qrhs), {
+            const size_t k = p / nf, pl = p - k * nf;
             size_t q;
-            if (face == 0) q = p + (size_t)My * Mz * (Mx - 1);                    // p = j + My*k
-            else if (face == 1) q = (My - 1) + (size_t)My * p;                    // p = k + Mz*i
-            else q = (p % My) + (size_t)My * (Mz - 1) + (size_t)My * Mz * (p / My);  // p = j + My*i
+            if (face == 0) q = pl + (size_t)My * Mz * (Mx - 1);                    // pl = j + My*k
+            else if (face == 1) q = (My - 1) + (size_t)My * pl;                    // pl = k + Mz*i
+            else q = (pl % My) + (size_t)My * (Mz - 1) + (size_t)My * Mz * (pl / My);  // pl = j + My*i
+            q += k * n3c;
             double Vs = 1.0 / Q4[q];
             double Pq = P[q];
             double U[3] = {Q1[q] * Vs, Q2[q] * Vs, Q3[q] * Vs};
@@ -780,7 +793,7 @@ static int bc_rhs_t(st_ctx *c, double *Q, R *Qrhs, const double *Y, R *Yrhs) {
 // Sponge_Forcing src/sponge_mf.f:7-127
 template <class R>
 static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrhs) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     const int Mx = c->dm.n[0], My = c->dm.n[1], Mz = c->dm.n[2];
     const double g1 = c->p.gamma1;
     const double base_pressure = 0.71429, Ms = 1.8;
@@ -794,17 +807,22 @@ static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrh
         len[d] = Ns[d] - start[d];
     }
     const int sx = start[0], sy = start[1], sz = start[2], lx = len[0], ly = len[1], lz = len[2];
-    const bool idx32 = n3 <= 0xffffffffull;   // 32-bit index arithmetic when it suffices
+    const size_t n3c = c->dm.n3;
+    const bool idx32 = nc <= 0xffffffffull;   // 32-bit index arithmetic when it suffices
+    const bool one = c->na == 1;
     // fraction of the cells in the sponge shell (the only ones touched)
-    const double shell = (double)(n3 - (size_t)sx * sy * sz) / (double)n3;
-    PFOR(c, n3, shell * (10 * io(Qrhs) + 5 * io(Q) + io(Y) + 2 * io(Yrhs)), {
+    const double shell = (double)(n3c - (size_t)sx * sy * sz) / (double)n3c;
+    PFOR(c, nc, shell * (10 * io(Qrhs) + 5 * io(Q) + io(Y) + 2 * io(Yrhs)), {
         int j, k, i;
         if (idx32) {
-            unsigned q = (unsigned)p, r = q / (unsigned)My;
+            unsigned q = (unsigned)p;
+            if (!one) q -= (q / (unsigned)n3c) * (unsigned)n3c;   // position within the case
+            unsigned r = q / (unsigned)My;
             j = (int)(q - r * (unsigned)My); k = (int)(r % (unsigned)Mz); i = (int)(r / (unsigned)Mz);
         } else {
-            size_t r = p / My;
-            j = (int)(p - r * My); k = (int)(r % Mz); i = (int)(r / Mz);
+            size_t q = one ? p : p - (p / n3c) * n3c;
+            size_t r = q / My;
+            j = (int)(q - r * My); k = (int)(r % Mz); i = (int)(r / Mz);
         }
         auto sig = [](int gI, int st, int ln) -> double {
             if (gI >= st) {
@@ -830,7 +848,7 @@ static int sponge_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, R *Yrh
 // the float form runs, and accumulated outputs are widened back.
 int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
     if (!fp32_mode(c)) return rhs_t<double>(c, Q, Q, Qrhs, Y);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<float> Qs(c, 5), Rs(c, 5);
     ST_TRY(dev_to_float(c, Q, Qs, 5 * n3));
     ST_TRY(rhs_t<float>(c, Q, Qs, Rs, Y));
@@ -840,13 +858,13 @@ int dev_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y) {
 int dev_compute_hyper(st_ctx *c, const double *Q, const double *Y) {
     if (!fp32_mode(c)) return compute_hyper_t<double>(c, Q, Y, Y);
     ScratchT<float> Ys(c, 1);
-    ST_TRY(dev_to_float(c, Y, Ys, c->dm.n3));
+    ST_TRY(dev_to_float(c, Y, Ys, c->ncell()));
     return compute_hyper_t<float>(c, Q, Y, Ys);
 }
 
 int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
     if (!fp32_mode(c)) return hyper_rhs_t<double>(c, Q, Qrhs, Y, Y);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<float> Ys(c, 1), Rs(c, 5);
     ST_TRY(dev_to_float(c, Y, Ys, n3));
     ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
@@ -856,7 +874,7 @@ int dev_hyper_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y) {
 
 int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (!fp32_mode(c)) return species_rhs_t<double>(c, Q, Q, Qrhs, Y, Y, Yrhs);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<float> Qs(c, 5), Ys(c, 1), Rs(c, 5), YRs(c, 1);
     ST_TRY(dev_to_float(c, Q, Qs, 5 * n3));
     ST_TRY(dev_to_float(c, Y, Ys, n3));
@@ -868,7 +886,7 @@ int dev_species_rhs(st_ctx *c, const double *Q, double *Qrhs, const double *Y, d
 
 int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (!fp32_mode(c)) return bc_rhs_t<double>(c, Q, Qrhs, Y, Yrhs);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<float> Rs(c, 5), YRs(c, 1);
     ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
     ST_TRY(dev_to_float(c, Yrhs, YRs, n3));
@@ -879,7 +897,7 @@ int dev_bc_rhs(st_ctx *c, double *Q, double *Qrhs, const double *Y, double *Yrhs
 
 int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double *Yrhs) {
     if (!fp32_mode(c)) return sponge_t<double>(c, Q, Qrhs, Y, Yrhs);
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     ScratchT<float> Rs(c, 5), YRs(c, 1);
     ST_TRY(dev_to_float(c, Qrhs, Rs, 5 * n3));
     ST_TRY(dev_to_float(c, Yrhs, YRs, n3));
@@ -891,11 +909,11 @@ int dev_sponge(st_ctx *c, const double *Q, double *Qrhs, const double *Y, double
 // Fix_Pressure pproc/pproc_mf.f:190-233; periodic family
 // src/lddrk4_periodic_sf.f:436-473 (base pressure 0.71463, gamma_eff = gamma)
 int dev_fix_pressure(st_ctx *c, double *Q) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
     const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
-    PFOR(c, n3, io(g, Q1, Q2, Q3, Q4, Q5, Q5), {
+    PFOR(c, nc, io(g, Q1, Q2, Q3, Q4, Q5, Q5), {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
@@ -908,11 +926,11 @@ int dev_fix_pressure(st_ctx *c, double *Q) {
 // Fix_Pressure of the FP32 mode's stages: as above, and the float copy of
 // the state for the next stage
 static int fix_pressure_copy(st_ctx *c, double *Q, float *qs) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     double *Q1 = Q, *Q2 = Q + n3, *Q3 = Q + 2 * n3, *Q4 = Q + 3 * n3, *Q5 = Q + 4 * n3;
     const double *g = c->gamma_eff;
     const double base = c->p.family == ST_FAMILY_PERIODIC ? 0.71463 : 0.71429;
-    PFOR(c, n3, io(g, Q1, Q2, Q3, Q4, Q5, Q5) + 5 * io(qs), {
+    PFOR(c, nc, io(g, Q1, Q2, Q3, Q4, Q5, Q5) + 5 * io(qs), {
         double fac1 = g[p] - 1.0;
         double Vs = 1.0 / Q4[p];
         double P = fac1 * (Q5[p] - 5.0e-1 * Vs * (Q1[p] * Q1[p] + Q2[p] * Q2[p] + Q3[p] * Q3[p]));
@@ -927,7 +945,7 @@ static int fix_pressure_copy(st_ctx *c, double *Q, float *qs) {
 
 // Compact_Filter src/filters_sym.f:398-432
 int dev_compact_filter(st_ctx *c, const double *F, double *F0, int nvar) {
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     for (int l = 0; l < nvar; l++) {
         ST_TRY(dev_filter(c, 0, l == 0, F + l * n3, F0 + l * n3));
         ST_TRY(dev_filter(c, 1, l == 1, F0 + l * n3, F0 + l * n3));
@@ -950,11 +968,14 @@ __device__ __forceinline__ void atomic_min_pos(double *a, double v) {
 }
 
 // Compute_CFL src/lddrk4_nonperiodic_mf.f:7-66 -> dscal[0]=stab, dscal[1]=resv
-__global__ void k_cfl(const double *Q, const double *g, size_t n3, double DX, double DY, double DZ,
+// of each case (blockIdx.y: case; n3: cells of a case; fs: field stride)
+__global__ void k_cfl(const double *Q, const double *g, size_t n3c, size_t fs, double DX, double DY, double DZ,
                       double *out) {
     const double kmax = 2.478, khug = 2.199;   // src/header:237-240
+    const size_t n3 = fs, c0 = (size_t)blockIdx.y * n3c, end = c0 + n3c;
+    out += (size_t)blockIdx.y * kScal;
     double m1 = 0.0, m2 = 0.0;
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
+    for (size_t p = c0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < end; p += (size_t)gridDim.x * blockDim.x) {
         double fac = g[p] * (g[p] - 1.0);
         double tmp1 = 1.0 / Q[3 * n3 + p];
         double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p];
@@ -975,10 +996,12 @@ __global__ void k_cfl(const double *Q, const double *g, size_t n3, double DX, do
 // Compute_Tstep hyperviscous limits src/lddrk4_nonperiodic_mf.f:100-145 -> out[2..5] minima
 template <class R>
 __global__ void k_tstep(const double *Q, const double *Y, const double *g, const R *vh, const R *bh,
-                        const R *kh, const R *Dh, size_t n3, double del, double g1, double g2,
+                        const R *kh, const R *Dh, size_t n3c, size_t fs, double del, double g1, double g2,
                         double eps, double *out) {
+    const size_t n3 = fs, c0 = (size_t)blockIdx.y * n3c, end = c0 + n3c;
+    out += (size_t)blockIdx.y * kScal;
     double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY, m6 = INFINITY;
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
+    for (size_t p = c0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < end; p += (size_t)gridDim.x * blockDim.x) {
         double fac = g[p] * (g[p] - 1.0);
         float fac1 = (float)(Y[p] + (eps * (g1 - 1.0) / (g2 - 1.0)) * (1.0 - Y[p]));   // implicit REAL
         double tmp1 = 1.0 / Q[3 * n3 + p];
@@ -1008,11 +1031,13 @@ __global__ void k_tstep(const double *Q, const double *Y, const double *g, const
 // Compute_Tstep of the periodic family, src/lddrk4_periodic_sf.f:105-135:
 // single-fluid temperature, no diffusivity limit (out[5] stays +inf)
 template <class R>
-__global__ void k_tstep_sf(const double *Q, const R *vh, const R *bh, const R *kh, size_t n3,
+__global__ void k_tstep_sf(const double *Q, const R *vh, const R *bh, const R *kh, size_t n3c, size_t fs,
                            double del, double gam, double *out) {
+    const size_t n3 = fs, c0 = (size_t)blockIdx.y * n3c, end = c0 + n3c;
+    out += (size_t)blockIdx.y * kScal;
     double m3 = INFINITY, m4 = INFINITY, m5 = INFINITY;
     const double fac = gam * (gam - 1.0);
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
+    for (size_t p = c0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < end; p += (size_t)gridDim.x * blockDim.x) {
         double tmp1 = 1.0 / Q[3 * n3 + p];
         double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p], q5 = Q[4 * n3 + p];
         double tmp2 = sqrt(fac * tmp1 * (q5 - 5.0e-1 * tmp1 * (q1 * q1 + q2 * q2 + q3 * q3)));
@@ -1034,11 +1059,21 @@ __global__ void k_tstep_sf(const double *Q, const R *vh, const R *bh, const R *k
 // f is 0.2D0 in src/lddrk4_nonperiodic_mf.f:156-157 and the default-REAL
 // literal 0.2 (float32) in src/lddrk4_periodic_sf.f:141-142; out[5] = +inf
 // when a limit is absent.
-__global__ void k_tstep_final(double *out, double cfl_cal, int use_hyper, int resv_dev, double resv_host,
-                              double f) {
+// Thread k: case k.  use_hyper < 0: each case decides from its own step
+// count (out[SC_STEP], advanced here), with the limits from step > hyper_from.
+__global__ void k_tstep_final(double *out, int ncase, double cfl_cal, int use_hyper, int hyper_from, int resv_dev,
+                              double resv_host, double f) {
+    const int k = threadIdx.x;
+    if (k >= ncase) return;
+    out += (size_t)k * kScal;
     double resv = resv_dev ? out[1] : resv_host;
     double t = cfl_cal / resv;
-    if (use_hyper) {
+    bool hyp = use_hyper > 0;
+    if (use_hyper < 0) {
+        hyp = out[SC_STEP] > (double)hyper_from;
+        out[SC_STEP] = out[SC_STEP] + 1.0;
+    }
+    if (hyp) {
         double cand[4] = {f * out[2], f * out[3], f * out[4], f * out[5]};
         for (int q = 0; q < 4; q++) if (cand[q] < t) t = cand[q];
     }
@@ -1051,10 +1086,10 @@ static int grid_blocks(size_t n) {
 }
 
 int dev_compute_cfl(st_ctx *c, const double *Q, bool to_host, double *stab, double *resv) {
-    ST_CUDA(c, cudaMemsetAsync(c->dscal, 0, 2 * sizeof(double), c->stream));
-    int pi = prof_start(c, "k_cfl", 48.0 * c->dm.n3);
-    k_cfl<<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, c->gamma_eff, c->dm.n3, c->DX, c->DY, c->DZ,
-                                                       c->dscal);
+    ST_CUDA(c, cudaMemset2DAsync(c->dscal, kScal * sizeof(double), 0, 2 * sizeof(double), c->na, c->stream));
+    int pi = prof_start(c, "k_cfl", 48.0 * c->ncell());
+    const dim3 grid(grid_blocks(c->dm.n3), c->na);
+    k_cfl<<<grid, 256, 0, c->stream>>>(Q, c->gamma_eff, c->dm.n3, c->fs, c->DX, c->DY, c->DZ, c->dscal);
     prof_stop(c, pi);
     ST_CUDA(c, cudaGetLastError());
     if (to_host) {
@@ -1073,36 +1108,43 @@ int dev_compute_cfl(st_ctx *c, const double *Q, bool to_host, double *stab, doub
 template <class R>
 static int tstep_hyper(st_ctx *c, const double *Q, const double *Y, bool sf) {
     R *const *H = Store<R>::hyp(c);
+    const dim3 grid(grid_blocks(c->dm.n3), c->na);
     if (sf) {
-        int pi = prof_start(c, "k_tstep", (40.0 + 3 * sizeof(R)) * c->dm.n3);
-        k_tstep_sf<R><<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(Q, H[H_VISC], H[H_BETA], H[H_K], c->dm.n3,
-                                                                   c->DX, c->p.gamma1, c->dscal);
+        int pi = prof_start(c, "k_tstep", (40.0 + 3 * sizeof(R)) * c->ncell());
+        k_tstep_sf<R><<<grid, 256, 0, c->stream>>>(Q, H[H_VISC], H[H_BETA], H[H_K], c->dm.n3, c->fs, c->DX,
+                                                   c->p.gamma1, c->dscal);
         prof_stop(c, pi);
     } else {
-        int pi = prof_start(c, "k_tstep", (56.0 + 4 * sizeof(R)) * c->dm.n3);
-        k_tstep<R><<<grid_blocks(c->dm.n3), 256, 0, c->stream>>>(
-            Q, Y, c->gamma_eff, H[H_VISC], H[H_BETA], H[H_K], H[H_D], c->dm.n3, c->DX, c->p.gamma1, c->p.gamma2,
-            c->p.epsilon, c->dscal);
+        int pi = prof_start(c, "k_tstep", (56.0 + 4 * sizeof(R)) * c->ncell());
+        k_tstep<R><<<grid, 256, 0, c->stream>>>(Q, Y, c->gamma_eff, H[H_VISC], H[H_BETA], H[H_K], H[H_D],
+                                                c->dm.n3, c->fs, c->DX, c->p.gamma1, c->p.gamma2, c->p.epsilon,
+                                                c->dscal);
         prof_stop(c, pi);
     }
     ST_CUDA(c, cudaGetLastError());
     return ST_OK;
 }
 
+// step < 0: a batch step, in which each case takes its own step count from
+// its scalars (the limits may apply to some cases and not others).
 int dev_compute_tstep(st_ctx *c, const double *Q, const double *Y, int step, bool resv_on_device,
                       double cfl_resv_host) {
     const bool sf = c->p.family == ST_FAMILY_PERIODIC;
     // hyperviscous limits from the first step on (_mf) or the second (periodic)
-    const bool use_hyper = c->p.hyper_param == 1 && step > (sf ? 1 : 0);
+    const int hyper_from = sf ? 1 : 0;
+    const bool per_case = step < 0;
+    const bool use_hyper = c->p.hyper_param == 1 && (per_case || step > hyper_from);
     if (use_hyper) {
         // minima start at +inf (a device fill, so that the step can be captured in a graph)
-        ST_TRY(dev_fill(c, c->dscal + 2, 4, INFINITY));
+        double *d = c->dscal;
+        PFOR(c, (size_t)c->na * 4, io(d), { d[(p >> 2) * kScal + 2 + (p & 3)] = INFINITY; });
         ST_TRY(fp32_mode(c) ? tstep_hyper<float>(c, Q, Y, sf) : tstep_hyper<double>(c, Q, Y, sf));
     }
     c->launches++;
     const double f = sf ? (double)0.2f : 0.2;
-    k_tstep_final<<<1, 1, 0, c->stream>>>(c->dscal, c->p.cfl_cal, use_hyper ? 1 : 0, resv_on_device ? 1 : 0,
-                                          cfl_resv_host, f);
+    const int mode = !use_hyper ? 0 : (per_case ? -1 : 1);
+    k_tstep_final<<<1, ((c->na + 31) / 32) * 32, 0, c->stream>>>(c->dscal, c->na, c->p.cfl_cal, mode, hyper_from,
+                                                                 resv_on_device ? 1 : 0, cfl_resv_host, f);
     ST_CUDA(c, cudaGetLastError());
     return ST_OK;
 }
@@ -1138,9 +1180,9 @@ template <> struct StateCopy<float> {
 template <class R>
 static int refresh(st_ctx *c, StateCopy<R> &sc, const double *Q, const double *Y, bool with_y) {
     if constexpr (!is_fp64<R>()) {
-        const size_t n3 = c->dm.n3;
+        const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
         float *qs = sc.qs, *ys = sc.ys;
-        PFOR(c, n3, 5 * io(Q, qs) + (with_y ? io(Y, ys) : 0.0), {
+        PFOR(c, nc, 5 * io(Q, qs) + (with_y ? io(Y, ys) : 0.0), {
             for (int l = 0; l < 5; l++) qs[l * n3 + p] = (float)Q[l * n3 + p];
             if (with_y) ys[p] = (float)Y[p];
         });
@@ -1160,13 +1202,15 @@ static int lddrk4_sf(st_ctx *c) {
     static const double beta2[6] = {1.1584888181285561688e-1, 3.7287699051652864918e-1,
                                     7.3795368921435295698e-1, 5.7981109366311039538e-1,
                                     1.031284991300145194e0, 1.5e-1};
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     Scratch Qfs(c, 5);
     double *Qf = Qfs;
     StateCopy<R> sc(c);
     bool fresh = false;   // the float state copy holds the current state
-    const double *dtp = c->dscal + 6;
-    double *timep = c->dscal + 7;
+    const double *dtp = c->dscal + SC_DT;     // time step and time of case k at k*kScal
+    double *timep = c->dscal + SC_TIME;
+    const size_t n3c = c->dm.n3;
+    const bool one = c->na == 1;
     for (int loop = 0; loop < 2; loop++) {
         const int ns = loop == 0 ? 5 : 6;
         for (int K = 0; K < ns; K++) {
@@ -1180,8 +1224,8 @@ static int lddrk4_sf(st_ctx *c) {
             if (!fresh) ST_TRY(refresh<R>(c, sc, Q, c->Y, false));
             ST_TRY(rhs_t<R>(c, Q, sc.q(Q), dQ, c->Y));
             ST_TRY(hyper_rhs_t<R>(c, Q, dQ, c->Y, sc.y(c->Y)));
-            PFOR(c, n3, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)), {
-                double dt = *dtp;
+            PFOR(c, nc, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)), {
+                double dt = dtp[(one ? 0 : p / n3c) * kScal];
                 for (int l = 0; l < 5; l++) {
                     size_t q = l * n3 + p;
                     double qw = first ? dt * dQ[q] : al * QW[q] + dt * dQ[q];
@@ -1201,7 +1245,7 @@ static int lddrk4_sf(st_ctx *c) {
                 fresh = true;
             }
         }
-        PFOR(c, 1, io(timep, timep), { timep[0] = timep[0] + dtp[0]; });
+        PFOR(c, (size_t)c->na, io(timep, timep), { timep[p * kScal] = timep[p * kScal] + dtp[p * kScal]; });
     }
     return ST_OK;
 }
@@ -1212,13 +1256,15 @@ static int lddrk4_mf(st_ctx *c) {
                                      -2.016477077503357e+00, -1.056444269767207e+00};
     static const double beta1[5] = {1.028639988104959e-01, 7.408540575766301e-01, 7.426530946683799e-01,
                                     4.694937902357905e-01, 1.881733382887932e-01};
-    const size_t n3 = c->dm.n3;
+    const size_t n3 = c->fs, nc = c->ncell();   // field stride; cells processed
     Scratch rYs(c), Qfs(c, 5);
     double *rY = rYs, *Qf = Qfs;
     StateCopy<R> sc(c);
     bool fresh = false;   // the float state copy holds the current state
-    const double *dtp = c->dscal + 6;
-    double *timep = c->dscal + 7;
+    const double *dtp = c->dscal + SC_DT;     // time step and time of case k at k*kScal
+    double *timep = c->dscal + SC_TIME;
+    const size_t n3c = c->dm.n3;
+    const bool one = c->na == 1;
     for (int loop = 0; loop < 2; loop++) {
         for (int K = 0; K < 5; K++) {
             const bool real = loop == 0 || c->p.rk_mode == 1;
@@ -1233,8 +1279,8 @@ static int lddrk4_mf(st_ctx *c) {
             ST_TRY(species_rhs_t<R>(c, Q, sc.q(Q), dQ, Y, sc.y(Y), drYi));
             ST_TRY(bc_rhs_t<R>(c, Q, dQ, Y, drYi));
             ST_TRY(sponge_t<R>(c, Q, dQ, Y, drYi));
-            PFOR(c, n3, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)) + io(Y, drYi, rYW, rY) + (first ? 0.0 : io(rYW)), {
-                double dt = *dtp;
+            PFOR(c, nc, 5 * io(dQ, Q, Q, QW) + (first ? 0.0 : 5 * io(QW)) + io(Y, drYi, rYW, rY) + (first ? 0.0 : io(rYW)), {
+                double dt = dtp[(one ? 0 : p / n3c) * kScal];
                 double ry = Q[3 * n3 + p] * Y[p];
                 for (int l = 0; l < 5; l++) {
                     size_t q = l * n3 + p;
@@ -1260,7 +1306,7 @@ static int lddrk4_mf(st_ctx *c) {
             const double *g = c->gamma_eff;
             float *qs = nullptr, *ys = nullptr;
             if constexpr (!is_fp64<R>()) { qs = sc.qs; ys = sc.ys; fresh = true; }
-            PFOR(c, n3, 5 * io(Q) + io(rY, g, Y, Q) + (qs ? 5 * io(qs) + io(ys) : 0.0), {
+            PFOR(c, nc, 5 * io(Q) + io(rY, g, Y, Q) + (qs ? 5 * io(qs) + io(ys) : 0.0), {
                 double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p];
                 double y = rY[p] / q4;
                 Y[p] = y;
@@ -1277,7 +1323,7 @@ static int lddrk4_mf(st_ctx *c) {
                 }
             });
         }
-        PFOR(c, 1, io(timep, timep), { timep[0] = timep[0] + dtp[0]; });
+        PFOR(c, (size_t)c->na, io(timep, timep), { timep[p * kScal] = timep[p * kScal] + dtp[p * kScal]; });
     }
     return ST_OK;
 }
@@ -1291,9 +1337,10 @@ int dev_lddrk4(st_ctx *c, bool) {
 // monitoring sums (Compute_Mom/KE/Mass/Energy/Entropy), two-pass block sums
 // sf: periodic family, whose Compute_Entropy (src/lddrk4_periodic_sf.f:268-300)
 // holds gamma - 1 in an undeclared (float32) local and skips Entropy2
-__global__ void k_monitor_partial(const double *Q, const double *g, size_t n3, double *part, int sf) {
+__global__ void k_monitor_partial(const double *Q, const double *g, size_t n3c, size_t fs, double *part, int sf) {
+    const size_t n3 = fs;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3; p += (size_t)gridDim.x * blockDim.x) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n3c; p += (size_t)gridDim.x * blockDim.x) {
         double q1 = Q[p], q2 = Q[n3 + p], q3 = Q[2 * n3 + p], q4 = Q[3 * n3 + p], q5 = Q[4 * n3 + p];
         double t = 1.0 / q4;
         double ke = 0.0;
@@ -1326,7 +1373,7 @@ int dev_monitors(st_ctx *c) {
     Scratch parts(c);   // >= 8*nb doubles for every supported grid (n3 >= 32^3)
     double *part = parts;
     c->launches++;
-    k_monitor_partial<<<nb, 256, 0, c->stream>>>(c->Q, c->gamma_eff, c->dm.n3, part,
+    k_monitor_partial<<<nb, 256, 0, c->stream>>>(c->Q, c->gamma_eff, c->dm.n3, c->fs, part,
                                                  c->p.family == ST_FAMILY_PERIODIC ? 1 : 0);
     ST_CUDA(c, cudaGetLastError());
     std::vector<double> h(8 * nb);

@@ -3,21 +3,29 @@
 Requests arrive over time (each one a full case: initial state, grid size,
 number of LDDRK4 steps).  The server
 
-  - admits a request when a solver slot of its grid size is free, or when a
-    new slot fits in the HBM budget (first come, first served, with later
+  - keeps one batch context per grid size (st_create_batch): its cases share
+    every kernel launch of a step, so k same-size cases cost one launch per
+    operator instead of k, and cases of different sizes overlap on the GPU
+    through their batches' streams;
+  - admits a request when its size's batch has a free case slot, or when a
+    new batch fits in the HBM budget (first come, first served, with later
     requests allowed to start ahead of a head request that does not fit yet);
-  - keeps every admitted case resident on the device in its own solver
-    context (own CUDA stream), uploads its state once and reads back only the
-    final state;
-  - advances all admitted cases concurrently: each step is enqueued without
-    waiting (from the third step on it is one CUDA-graph launch), so the
-    cases' kernels overlap on the GPU, and a case that finishes frees its
-    slot for the next request of that size while the others keep running;
+    a case joins a running batch between steps, at its own step 0, while the
+    others continue (each case has its own time step, time and step count);
+  - keeps every admitted case resident on the device, uploads its state once
+    and reads back only its final state; a finished case's slot is refilled
+    by moving the batch's last active case into it, so the active cases stay
+    in front and every launch covers active cases only;
+  - enqueues the steps of each batch without waiting (one CUDA-graph launch
+    per step, one graph per active count), never past the first case to
+    finish;
   - records arrival, admission and completion times, from which p50/p99
     time-to-solution and aggregate cell-steps/s follow.
 
-Slots are reused across requests of the same size (st_set_state resets a
-context), so the scratch memory and captured step graph of a slot stay warm.
+A batch's capacity is the number of cases of its size that fit in
+``batch_cells`` cells (at least one, at most ``max_batch``).  A case gives
+the same bytes in a batch as alone: same kernels, same arithmetic per cell,
+its own reductions and time step.
 """
 import collections
 import dataclasses
@@ -25,7 +33,7 @@ import time
 
 import numpy as np
 
-BYTES_PER_FIELD_ESTIMATE = 96       # fields of n^3 doubles per context before measurement
+BYTES_PER_FIELD_ESTIMATE = 96       # fields of n^3 doubles per case before measurement
 
 
 @dataclasses.dataclass
@@ -55,91 +63,97 @@ class Result:
         return self.done - self.arrival
 
 
-class _Slot:
-    def __init__(self, n, solver, nbytes):
-        self.n, self.solver, self.nbytes = n, solver, nbytes
-        self.req = None
+class _Case:
+    def __init__(self, req, admitted):
+        self.req = req
         self.step = 0
-        self.admitted = 0.0
+        self.admitted = admitted
+
+
+class _Group:
+    """One batch context of grid size n and its cases (slot k <-> cases[k])."""
+
+    def __init__(self, n, batch, capacity, nbytes):
+        self.n, self.batch, self.capacity, self.nbytes = n, batch, capacity, nbytes
+        self.cases = []
+
+    @property
+    def cells(self):
+        return len(self.cases) * self.n ** 3
 
 
 class Server:
-    """make_solver(n) returns an object with set_state(Q, Y), set_time(t),
-    setup(Q, Y) (the set-up before the main loop), step_async(step), done(),
-    get_state() -> (Q, Y), get_time(), close() and memory_bytes(); the default
-    builds a GPU solver context (Solver)."""
+    """make_batch(n, capacity) returns an object with start(k, Q, Y),
+    set_active(na), get(k) -> (Q, Y, time, step), move(src, dst),
+    step_async(), done(), memory_bytes() and close(); the default builds a
+    GPU batch context (Batch)."""
 
-    def __init__(self, hbm_budget=150e9, make_solver=None, steps_ahead=2, clock=time.perf_counter, estimate=None,
-                 max_active_cells=24e6):
+    def __init__(self, hbm_budget=150e9, make_batch=None, steps_ahead=2, clock=time.perf_counter, estimate=None,
+                 max_active_cells=24e6, batch_cells=16e6, max_batch=16):
         self.budget = float(hbm_budget)
         # cells of the cases stepped concurrently: enough to keep the GPU busy
         # with small cases, few enough that cases finish roughly in arrival
         # order instead of all sharing the GPU until the end
         self.max_active_cells = float(max_active_cells)
-        self.make_solver = make_solver or _gpu_solver_factory()
-        # bytes of one slot of grid n before a slot of that size has been measured
+        self.batch_cells = float(batch_cells)
+        self.max_batch = int(max_batch)
+        self.make_batch = make_batch or _gpu_batch_factory()
+        # bytes of one case of grid n before a batch of that size has been measured
         self.estimate = estimate or (lambda n: BYTES_PER_FIELD_ESTIMATE * 8.0 * n ** 3)
         self.steps_ahead = max(1, int(steps_ahead))
         self.clock = clock
-        self.slots = []                              # every context created
-        self.free = collections.defaultdict(list)    # n -> idle slots
-        self.footprint = {}                          # n -> measured bytes of one slot
+        self.groups = {}                             # n -> _Group
+        self.footprint = {}                          # n -> measured bytes per case
         self.used = 0.0
 
-    # -- memory accounting ------------------------------------------------------
-    def _estimate(self, n):
+    # -- batches and memory ------------------------------------------------------
+    def capacity(self, n):
+        return int(max(1, min(self.max_batch, self.batch_cells // n ** 3)))
+
+    def _per_case(self, n):
         return self.footprint.get(n, self.estimate(n))
 
     def _evict_idle(self, keep_n, need):
-        """Close idle slots of other sizes until `need` more bytes fit (only
+        """Close empty batches of other sizes until `need` more bytes fit (only
         when closing them is enough)."""
-        reclaimable = sum(sl.nbytes for n, lst in self.free.items() if n != keep_n for sl in lst)
-        if self.used - reclaimable + need > self.budget:
+        idle = [g for n, g in self.groups.items() if n != keep_n and not g.cases]
+        if self.used - sum(g.nbytes for g in idle) + need > self.budget:
             return
-        for n in list(self.free):
-            if n == keep_n:
-                continue
-            while self.free[n] and self.used + need > self.budget:
-                slot = self.free[n].pop()
-                slot.solver.close()
-                self.slots.remove(slot)
-                self.used -= slot.nbytes
+        for g in idle:
+            if self.used + need <= self.budget:
+                break
+            g.batch.close()
+            self.used -= g.nbytes
+            del self.groups[g.n]
 
-    def _new_slot(self, n):
-        solver = self.make_solver(n)
-        nbytes = float(solver.memory_bytes())
-        slot = _Slot(n, solver, nbytes)
-        self.slots.append(slot)
-        self.used += nbytes
-        return slot
+    def _group(self, n):
+        g = self.groups.get(n)
+        if g is not None:
+            return g
+        per = self._per_case(n)
+        cap = self.capacity(n)
+        if self.used + per * cap > self.budget:
+            self._evict_idle(n, per)
+        # as many case slots as the budget leaves room for, up to the capacity
+        cap = min(cap, int((self.budget - self.used) // per)) if per > 0 else cap
+        if cap < 1:
+            busy = any(gr.cases for gr in self.groups.values())
+            if not busy and per > self.budget:
+                raise ValueError(f"a {n}^3 case needs about {per:.3g} B, more than the HBM budget")
+            return None
+        b = self.make_batch(n, cap)
+        g = _Group(n, b, cap, float(b.memory_bytes()))
+        self.groups[n] = g
+        self.used += g.nbytes
+        return g
 
-    def _try_admit(self, req, now):
-        if self.free[req.n]:
-            slot = self.free[req.n].pop()
-        else:
-            need = self._estimate(req.n)
-            if self.used + need > self.budget:
-                self._evict_idle(req.n, need)
-            if self.used + need > self.budget:
-                if not any(s.req is not None for s in self.slots) and need > self.budget:
-                    raise ValueError(f"a {req.n}^3 case needs about {need:.3g} B, more than the HBM budget")
-                return None
-            slot = self._new_slot(req.n)
-        slot.req = req
-        slot.step = 0
-        slot.admitted = now
-        slot.solver.set_state(req.Q, req.Y)
-        slot.solver.set_time(0.0)
-        slot.solver.setup(req.Q, req.Y)
-        return slot
-
-    def _refresh_footprint(self, slot):
+    def _refresh_footprint(self, g):
         # the scratch pool of a context grows during its first steps
-        nb = float(slot.solver.memory_bytes())
-        if nb > slot.nbytes:
-            self.used += nb - slot.nbytes
-            slot.nbytes = nb
-        self.footprint[slot.n] = max(self.footprint.get(slot.n, 0.0), slot.nbytes)
+        nb = float(g.batch.memory_bytes())
+        if nb > g.nbytes:
+            self.used += nb - g.nbytes
+            g.nbytes = nb
+        self.footprint[g.n] = max(self.footprint.get(g.n, 0.0), g.nbytes / g.capacity)
 
     # -- main loop -------------------------------------------------------------
     def run(self, requests, idle_sleep=2e-4):
@@ -147,61 +161,94 @@ class Server:
         results in completion order."""
         pending = collections.deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         waiting = []
-        active = []
         results = []
         t0 = self.clock()
-        while pending or waiting or active:
+        while pending or waiting or any(g.cases for g in self.groups.values()):
             now = self.clock() - t0
             while pending and pending[0].arrival <= now:
                 waiting.append(pending.popleft())
-            # admission: FIFO, later requests may pass a head that does not fit
-            still = []
-            active_cells = float(sum(sl.n ** 3 for sl in active))
-            for req in waiting:
-                if active and active_cells + req.n ** 3 > self.max_active_cells:
-                    still.append(req)
-                    continue
-                slot = self._try_admit(req, now)
-                if slot is not None:
-                    active_cells += req.n ** 3
-                if slot is None:
-                    still.append(req)
-                else:
-                    active.append(slot)
-            waiting = still
             progressed = False
-            for slot in list(active):
-                if not slot.solver.done():
+            # finished cases leave their batch (only between steps)
+            for g in list(self.groups.values()):
+                if not g.cases or not g.batch.done():
                     continue
-                progressed = True
-                if slot.step > 0:
-                    self._refresh_footprint(slot)
-                if slot.step >= slot.req.steps:
-                    Q, Y = slot.solver.get_state()
-                    tsim = slot.solver.get_time()
+                if any(cs.step > 0 for cs in g.cases):
+                    self._refresh_footprint(g)
+                k = 0
+                while k < len(g.cases):
+                    cs = g.cases[k]
+                    if cs.step < cs.req.steps:
+                        k += 1
+                        continue
+                    Q, Y, tsim, _ = g.batch.get(k)
                     done = self.clock() - t0
-                    results.append(Result(slot.req.rid, slot.n, slot.req.steps, Q, Y, tsim, slot.req.arrival,
-                                          slot.admitted, done))
-                    slot.req = None
-                    active.remove(slot)
-                    self.free[slot.n].append(slot)
+                    results.append(Result(cs.req.rid, g.n, cs.req.steps, Q, Y, tsim, cs.req.arrival,
+                                          cs.admitted, done))
+                    last = len(g.cases) - 1
+                    if k != last:
+                        g.batch.move(last, k)
+                        g.cases[k] = g.cases[last]
+                    g.cases.pop()
+                    progressed = True
+                if g.cases:
+                    g.batch.set_active(len(g.cases))
+            # admission: FIFO, later requests may pass a head that does not fit
+            active_cells = float(sum(g.cells for g in self.groups.values()))
+            still = []
+            for req in waiting:
+                if active_cells > 0 and active_cells + req.n ** 3 > self.max_active_cells:
+                    still.append(req)
                     continue
-                for _ in range(min(self.steps_ahead, slot.req.steps - slot.step)):
-                    slot.solver.step_async(slot.step)
-                    slot.step += 1
+                g = self._group(req.n)
+                if g is None or len(g.cases) >= g.capacity or (g.cases and not g.batch.done()):
+                    still.append(req)
+                    continue
+                k = len(g.cases)
+                g.batch.start(k, req.Q, req.Y)
+                g.cases.append(_Case(req, self.clock() - t0))
+                g.batch.set_active(len(g.cases))
+                active_cells += req.n ** 3
+                progressed = True
+            waiting = still
+            # enqueue steps of every idle batch, never past its first finisher
+            for g in self.groups.values():
+                if not g.cases or not g.batch.done():
+                    continue
+                todo = min(self.steps_ahead, min(cs.req.steps - cs.step for cs in g.cases))
+                for _ in range(todo):
+                    g.batch.step_async()
+                for cs in g.cases:
+                    cs.step += todo
+                progressed = progressed or todo > 0
             if not progressed and (not pending or pending[0].arrival > self.clock() - t0):
                 time.sleep(idle_sleep)
         return results
 
+    @property
+    def slots(self):
+        """Batch contexts currently held (one per grid size)."""
+        return list(self.groups.values())
+
     def close(self):
-        for slot in self.slots:
-            slot.solver.close()
-        self.slots.clear()
-        self.free.clear()
+        for g in self.groups.values():
+            g.batch.close()
+        self.groups.clear()
         self.used = 0.0
 
 
+def _gpu_batch_factory(**param_kw):
+    from . import Batch, default_params
+
+    def make(n, capacity):
+        kw = dict(re=100.0, re1=100.0, re2=100.0, pr=0.7, hyper_param=1, cfl_cal=0.5, c_beta_scale=1.75)
+        kw.update(param_kw)
+        return Batch(default_params(n, **kw), capacity)
+
+    return make
+
+
 def _gpu_solver_factory(**param_kw):
+    """A single-grid solver with the serving parameters (for running a case alone)."""
     from . import Solver, default_params
 
     class _GpuSolver(Solver):
@@ -215,9 +262,6 @@ def _gpu_solver_factory(**param_kw):
             # the calls before the main loop, src/main_mf.f:100-104
             self.Compute_gamma(Y)
             self.Compute_hyper(Q, Y)
-
-        def get_state(self, Q=None, Y=None):
-            return Solver.get_state(self, Q, Y)
 
     def make(n):
         kw = dict(re=100.0, re1=100.0, re2=100.0, pr=0.7, hyper_param=1, cfl_cal=0.5, c_beta_scale=1.75)
