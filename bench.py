@@ -132,17 +132,17 @@ def oracle_rate(n, steps, warm, threads):
     return n ** 3 * steps / el / 1e6, el
 
 
-def traffic_per_launch(kernel, n):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
-    to an n^3 grid (traffic grows with the cells a launch processes)."""
+def traffic_ratio(kernel):
+    """DRAM read+write bytes over algorithmic bytes per launch of `kernel`, from
+    the committed ncu capture (profiles/ncu_traffic.txt, a small grid): the
+    launch's traffic at any grid is this ratio times its algorithmic bytes."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         parts = line.split()
-        if len(parts) >= 3 and parts[0] == kernel and not line.startswith("#"):
-            ncap, b = int(parts[1]), float(parts[2])
-            return b * (n ** 3) / (ncap ** 3)
+        if len(parts) >= 6 and parts[0] == kernel and not line.startswith("#"):
+            return float(parts[5])
     return None
 
 
@@ -465,6 +465,41 @@ def run_precision(args, rank, world, local, dist):
         "clocks": clk}), flush=True)
 
 
+# ---------------------------------------------------------------- kernel timing
+def kernel_profile(s):
+    """Per-kernel launches, device ms and algorithmic bytes recorded while the
+    context's profiling was on; pointwise launches are folded into one entry
+    and also returned per source site."""
+    import ctypes
+    buf = ctypes.create_string_buffer(1 << 16)
+    s._check(s.lib.st_profile_report(s._h, buf, len(buf)), "st_profile_report")
+    prof, sites = {}, {}
+    for k, v in json.loads(buf.value.decode()).items():
+        key = "k_pointwise" if k.startswith("k_pointwise@") else k
+        if key != k:
+            sites[k.split("@")[1]] = v
+        a = prof.setdefault(key, {"launches": 0, "ms": 0.0, "bytes": 0.0})
+        for f in ("launches", "ms", "bytes"):
+            a[f] += v[f]
+    return prof, sites
+
+
+def kernel_table(prof, ms_total, steps):
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = float(json.load(open(peaks_path))["hbm_gbs"]) if os.path.exists(peaks_path) else 6650.0
+    tot = sum(v["ms"] for v in prof.values()) or 1.0
+    out = {}
+    for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"]):
+        gbs = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["bytes"] and v["ms"] else None
+        out[k] = {"launches": v["launches"], "ms_per_step": round(v["ms"] / steps, 3), "share": round(v["ms"] / tot, 4),
+                  "GB/s": gbs, "frac": round(gbs / peak, 3) if gbs else None}
+    return out
+
+
+def top_sites(sites, n=12):
+    return {"st_physics.cu:" + k: round(v["ms"], 2) for k, v in sorted(sites.items(), key=lambda kv: -kv[1]["ms"])[:n]}
+
+
 # ---------------------------------------------------------------- extensions
 def fp32_extension(args, local, Q0, Y0, ref_state, fp64_value):
     """The FP32 mode on the same 384^3 blast: the same warm-up and timed steps
@@ -486,6 +521,7 @@ def fp32_extension(args, local, Q0, Y0, ref_state, fp64_value):
         t, st = s.step(t, st)
     torch.cuda.synchronize()
     clocks = ClockSampler(gpu_smi_id(local))
+    s.lib.st_profile(s._h, 1)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -494,7 +530,9 @@ def fp32_extension(args, local, Q0, Y0, ref_state, fp64_value):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    s.lib.st_profile(s._h, 0)
     ms = e0.elapsed_time(e1)
+    prof, sites = kernel_profile(s)
     Q32, Y32 = s.get_state()
     s.close()
     errs = field_errors(Q32, ref_state[0], Y32, ref_state[1])
@@ -505,7 +543,8 @@ def fp32_extension(args, local, Q0, Y0, ref_state, fp64_value):
             "dtype": "f32 intermediates / f64 state, accumulators, state filter, pressure recovery",
             "errors_vs_fp64_after_steps": args.warmup + args.steps,
             "errors": {k: {"l2_rel": v[0], "linf_rel": v[1]} for k, v in errs.items()},
-            "worst_l2_rel": l2, "worst_linf_rel": linf, "clocks": clk}
+            "worst_l2_rel": l2, "worst_linf_rel": linf, "clocks": clk,
+            "kernels": kernel_table(prof, ms, args.steps), "pointwise_sites_ms": top_sites(sites)}
 
 
 def serving_extension(args, local, fp64_value):
@@ -692,7 +731,9 @@ def main():
     step_ms_all = sum(v["ms"] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src,
-                "traffic": traffic_per_launch(dom, args.n),
+                "traffic": (traffic_ratio(dom) * d["bytes"] / d["launches"]) if traffic_ratio(dom) else None,
+                "traffic_basis": "ncu dram read+write / algorithmic bytes of a 256^3 plain k_dfd capture "
+                                 "(profiles/ncu_traffic.txt) times the algorithmic bytes per launch",
                 "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
                 "avg_launch_ms": d["ms"] / d["launches"],
                 "share_of_kernel_time": d["ms"] / step_ms_all if step_ms_all else None,

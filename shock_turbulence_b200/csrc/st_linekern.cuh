@@ -6,10 +6,7 @@
 // (st_kernels.cu, st_kernels_cyc.cu) so that the bounded-line kernels keep
 // their register allocation.
 #pragma once
-#include <algorithm>
 #include <cfloat>
-#include <cstdlib>
-#include <cstring>
 #include "st_line.cuh"
 
 namespace st {
@@ -33,10 +30,6 @@ struct LineArgsT {
 };
 using LineArgs = LineArgsT<double>;
 using LineArgsF = LineArgsT<float>;
-
-}  // namespace st
-#include "st_line2.cuh"
-namespace st {
 
 // Every line kernel is instantiated for x/z lines (YT = false: direct
 // coalesced row accesses) and for y lines (YT = true: staged through a
@@ -193,79 +186,6 @@ static void set_smem(size_t bytes) {
     }
 }
 
-// The persistent whole-line kernels (st_line2.cuh) serve the bounded-line
-// operators on lines of 32 segments of S >= 4 rows (n = 32 S, 128 <= n <=
-// 512) whose tile ring fits in shared memory: 16 warps (16 FP64 or 32 FP32
-// lines per tile), or 8 when the input fields of a producer need the room.
-// The periodic family and the other sizes keep the segmented kernels below.
-// ST_LINE_KERNEL=segmented selects those for every operator (for
-// comparisons).
-inline bool whole_line_kernels_enabled() {
-    static const int on = [] {
-        const char *e = std::getenv("ST_LINE_KERNEL");
-        return (e && std::strcmp(e, "segmented") == 0) ? 0 : 1;
-    }();
-    return on != 0;
-}
-
-template <int S, int KIND, int OP, int KW, class T>
-static void launch_whole(st_ctx *c, const LineArgsT<T> &a0, cudaStream_t st) {
-    using RG = lk2::Ring<S, KIND, OP, KW, T>;
-    constexpr int NL = KW * lk2::Elt<T>::LPW;
-    LineArgsT<T> a = a0;
-    a.geo.cblk = (unsigned)(c->dm.n3 / (size_t)a.geo.n / NL);       // tiles per case
-    a.geo.cstride = c->dm.n3;
-    const unsigned ntiles = a.geo.cblk * (unsigned)c->na;
-    set_smem<lk2::k_line2<S, KIND, OP, KW, T>>(RG::kSmem);
-    static int per_sm = 0;     // resident CTAs per SM of this instantiation
-    if (!per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lk2::k_line2<S, KIND, OP, KW, T>, KW * 32, RG::kSmem);
-        if (per_sm < 1) per_sm = 1;
-    }
-    const unsigned ctas = std::min<unsigned>(ntiles, (unsigned)(per_sm * lk2::persistent_ctas(c->dev)));
-    lk2::k_line2<S, KIND, OP, KW, T><<<ctas, KW * 32, RG::kSmem, st>>>(a, ntiles);
-}
-
-// the widest tile whose ring fits
-template <int S, int KIND, int OP, class T>
-static bool launch_whole_fit(st_ctx *c, const LineArgsT<T> &a, cudaStream_t st) {
-    if constexpr (lk2::Ring<S, KIND, OP, 16, T>::kFits) {
-        launch_whole<S, KIND, OP, 16, T>(c, a, st);
-        return true;
-    } else if constexpr (lk2::Ring<S, KIND, OP, 8, T>::kFits) {
-        launch_whole<S, KIND, OP, 8, T>(c, a, st);
-        return true;
-    } else {
-        return false;
-    }
-}
-
-template <int S, bool CYC, class T>
-static bool try_whole(st_ctx *c, OpKind op, const LineArgsT<T> &a, cudaStream_t st) {
-    if constexpr (CYC || S < 4) {
-        return false;
-    } else {
-        if (!whole_line_kernels_enabled() || a.geo.n != 32 * S || a.P != 32) return false;
-        switch (op) {
-            case OP_D1:
-                switch (a.F.op) {
-                    case PR_A: return launch_whole_fit<S, lk2::K2_D1, PR_A, T>(c, a, st);
-                    case PR_MUL: return launch_whole_fit<S, lk2::K2_D1, PR_MUL, T>(c, a, st);
-                    case PR_ADDMUL: return launch_whole_fit<S, lk2::K2_D1, PR_ADDMUL, T>(c, a, st);
-                    case PR_MULMUL: return launch_whole_fit<S, lk2::K2_D1, PR_MULMUL, T>(c, a, st);
-                    case PR_SPEC: return launch_whole_fit<S, lk2::K2_D1, PR_SPEC, T>(c, a, st);
-                    case PR_SPECT: return launch_whole_fit<S, lk2::K2_D1, PR_SPECT, T>(c, a, st);
-                    default: return false;
-                }
-            case OP_D2: return launch_whole_fit<S, lk2::K2_D2, PR_A, T>(c, a, st);
-            case OP_FILTER:
-                if constexpr (sizeof(T) == 8) return launch_whole_fit<S, lk2::K2_FILTER, PR_A, T>(c, a, st);
-                return false;
-            default: return false;
-        }
-    }
-}
-
 template <int S, bool YT, bool CYC, class T>
 static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a0, cudaStream_t st) {
     const size_t nlines = c->dm.n3 / (size_t)a0.geo.n;     // lines of one case
@@ -286,10 +206,6 @@ static void launch_SY(st_ctx *c, OpKind op, const LineArgsT<T> &a0, cudaStream_t
     if (a.E1) b += 2 * es;                         // epilogue addends
     static const char *names[4] = {"k_dfd", "k_d2fd2", "k_filter", "k_gauss"};
     int pi = prof_start(c, names[op], b * n3);
-    if (try_whole<S, CYC, T>(c, op, a, st)) {
-        prof_stop(c, pi);
-        return;
-    }
     switch (op) {
         case OP_D1:
             switch (a.F.op) {
