@@ -132,6 +132,14 @@ def oracle_rate(n, steps, warm, threads):
     return n ** 3 * steps / el / 1e6, el
 
 
+def single_core_rate(n=64, steps=2):
+    """The CPU oracle on one host thread: a 64^3 sample of the same workload,
+    1 warm-up + 2 timed steps (about 15 s)."""
+    rate, el = oracle_rate(n, steps, 1, 1)
+    return {"value": rate, "unit": UNIT, "cores": 1,
+            "sample": f"CPU oracle, {n}^3 sample, 1 warm-up + {steps} timed steps ({el:.1f} s), 1 thread"}
+
+
 def traffic_ratio(kernel):
     """DRAM read+write bytes over algorithmic bytes per launch of `kernel`, from
     the committed ncu capture (profiles/ncu_traffic.txt, a small grid): the
@@ -763,6 +771,7 @@ def main():
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 3 timed steps "
                          f"({el:.1f} s), {threads} OpenMP threads"}
+        cpu["single_core"] = single_core_rate()
 
     ext = None
     if want_ext:

@@ -1,16 +1,13 @@
 """Builds the sm_100a CUDA library ``libst_b200.so`` in-tree with nvcc.
 
-The physics (pointwise) code is compiled with ``--fmad=false`` so that every
-product and sum rounds as the reference source writes it.  The line-kernel
-translation units (compact derivatives, filters, their segmented solves) are
-compiled with ``--fmad=true``: their stencil sums and LU recurrences contract
-to fused multiply-adds, which cuts their FP64 instruction count by about a
-quarter (the FP64 pipe limits the second-derivative and filter kernels); the
-segmented solves do not follow the reference's serial operation order in any
-case, and the results stay within the per-call parity bound.  Each source
-compiles to its own object in ``_build/`` (in parallel; the line-kernel
-translation units hold most of the template instantiations), then nvcc links
-the shared library.
+Everything is compiled with ``--fmad=false`` so that every product and sum
+rounds as the reference source writes it.  (Contracting the line kernels'
+multiply-adds was measured: 1.5-4 % faster operators, but the artificial
+viscosity coefficients, which take high-order derivatives of nearly constant
+fields, then moved by up to 17 % on a periodic test case against the
+oracle.)  Each source compiles to its own object in ``_build/`` (in parallel;
+the line-kernel translation units hold most of the template instantiations),
+then nvcc links the shared library.
 """
 import os
 import subprocess
@@ -24,8 +21,6 @@ SOURCES = ["st_kernels.cu", "st_kernels_cyc.cu", "st_kernels_f32.cu", "st_kernel
            "st_radial.cu", "st_noalloc.cu", "st_diag.cu", "st_tables.cpp", "st_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--extended-lambda", "-std=c++17", "-Xcompiler", "-fPIC"]
-# translation units of the line kernels: contracted multiply-adds
-FMAD_SOURCES = {"st_kernels.cu", "st_kernels_cyc.cu", "st_kernels_f32.cu", "st_kernels_cyc_f32.cu"}
 
 
 def _newest_source_mtime():
@@ -37,8 +32,7 @@ def _newest_source_mtime():
 
 def _compile(src, verbose):
     obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
-    fmad = "--fmad=true" if src in FMAD_SOURCES else "--fmad=false"
-    cmd = ["nvcc", *NVCC_FLAGS, fmad, "-c", "-o", obj, os.path.join(CSRC, src)]
+    cmd = ["nvcc", *NVCC_FLAGS, "--fmad=false", "-c", "-o", obj, os.path.join(CSRC, src)]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
