@@ -30,6 +30,7 @@ module st_b200
   public :: st_bc_rhs, st_sponge_forcing, st_fix_pressure
   public :: st_compute_cfl, st_compute_tstep, st_lddrk4, st_step, st_get_monitors, st_sync
   public :: st_compute_grad, st_shell_count, st_compute_srm_stats, st_generate_shock_surface
+  public :: st_make_padded_arrays, st_write_visual
 
   ! st_params of include/st_b200.h, field for field
   type, bind(c) :: st_params_t
@@ -466,6 +467,24 @@ module st_b200
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: ctx
        real(c_double), intent(out) :: rad_avg, rad_skew_rms
+     end function
+     ! Grad: c_loc of the 4 Compute_Grad fields, or c_null_ptr
+     integer(c_int) function st_make_padded_arrays(ctx, Grad, W, xx, yy, zz) &
+          bind(c, name='st_make_padded_arrays')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       type(c_ptr), value :: Grad
+       real(c_double), intent(out) :: W(*), xx(*), yy(*), zz(*)
+     end function
+     integer(c_int) function st_write_visual(ctx, Grad, vis_path, prefix, cue_vis, time, step) &
+          bind(c, name='st_write_visual')
+       import :: c_int, c_ptr, c_char, c_double
+       type(c_ptr), value :: ctx
+       type(c_ptr), value :: Grad
+       character(kind=c_char), intent(in) :: vis_path(*), prefix(*)
+       integer(c_int), value :: cue_vis
+       real(c_double), value :: time
+       integer(c_int), value :: step
      end function
 
      ! C library strlen, for the error message of st_last_error

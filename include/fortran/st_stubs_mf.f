@@ -702,3 +702,56 @@
       CLOSE(7)
       Return
       End
+
+************************************************************************
+*  MakePaddedArrays src/vis_silo_mf.f:440 (nfields = 11) and
+*  Write_Visual_Silo src/vis_silo_mf.f:7 on /RKWORK/ Q and Grad (filled
+*  by Compute_Grad), the context's gamma_eff and /SPECIES/ Y.  The
+*  visual file is a binary legacy VTK rectilinear grid with the Silo
+*  file's mesh, variables, cycle and time (no Silo library in this
+*  build), written to vis_path/ddd/prefix.000.vtk, ddd the three digits
+*  of cue_vis; Output advances cue_vis as before.
+************************************************************************
+      Subroutine MakePaddedArrays(W, xx, yy, zz, nfields)
+      Use iso_c_binding, only: c_loc
+      Use st_b200
+      Include 'header'
+      Integer nfields
+      Real*8  W(My+1,Mz+1,Mx+1,nfields)
+      Real*8  xx(Mx+1), yy(My+1), zz(Mz+1)
+      Real*8  Q(My,Mz,Mx,5)
+      Real*8, Target :: Grad(My,Mz,Mx,4)
+      Common /RKWORK/ Q, Grad
+      Real*8, Target :: Y(My,Mz,Mx,1)
+      Real*8  drYi(My,Mz,Mx,1), rYW(My,Mz,Mx,1)
+      Common /SPECIES/ Y, drYi, rYW
+      If (nfields .NE. 11) Stop 'libst_b200: nfields is not 11'
+      Call st_b200_init
+      Call st_check(st_set_state(st_ctx, Q, c_loc(Y)),
+     .              'MakePaddedArrays')
+      Call st_check(st_make_padded_arrays(st_ctx, c_loc(Grad), W,
+     .              xx, yy, zz), 'MakePaddedArrays')
+      Return
+      End
+
+      Subroutine Write_Visual_Silo(time, step)
+      Use iso_c_binding, only: c_loc, c_null_char
+      Use st_b200
+      Include 'header'
+      Real*8  time
+      Integer step
+      Real*8  Q(My,Mz,Mx,5)
+      Real*8, Target :: Grad(My,Mz,Mx,4)
+      Common /RKWORK/ Q, Grad
+      Real*8, Target :: Y(My,Mz,Mx,1)
+      Real*8  drYi(My,Mz,Mx,1), rYW(My,Mz,Mx,1)
+      Common /SPECIES/ Y, drYi, rYW
+      Call st_b200_init
+      Call st_check(st_set_state(st_ctx, Q, c_loc(Y)),
+     .              'Write_Visual_Silo')
+      Call st_check(st_write_visual(st_ctx, c_loc(Grad),
+     .              trim(vis_path)//c_null_char,
+     .              trim(prefix)//c_null_char, cue_vis, time, step),
+     .              'Write_Visual_Silo')
+      Return
+      End

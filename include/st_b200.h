@@ -294,6 +294,24 @@ int  st_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur
  * (mean distance of the cells with beta_hyper > 0.1*max from their centroid,
  * and sqrt(sum of squared deviations)/(n*mean)). */
 int  st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms);
+/* MakePaddedArrays src/vis_silo_mf.f:440-689 (one rank): W =
+ * W(My+1,Mz+1,Mx+1,11), the fields u, v, w, rho, P (:494-510), the four
+ * Grad fields, gamma_eff and Y at the nodes of the grid padded by one node
+ * per direction (each padding node a copy of the last node of its
+ * direction, :640-686); xx/yy/zz (Mx+1, My+1, Mz+1, each may be NULL) the
+ * node coordinates plus one spacing (:486-491).  Grad: the 4 fields of
+ * st_compute_grad (/RKWORK/ Grad), or NULL to compute them first. */
+int  st_make_padded_arrays(st_ctx *c, const double *Grad, double *W, double *xx, double *yy, double *zz);
+/* Write_Visual_Silo src/vis_silo_mf.f:7-277 (one rank).  The same mesh
+ * (collinear, axes y, z, x of sizes My+1, Mz+1, Mx+1), the eleven
+ * node-centred variables rho, U, V, W, P, omx, omy, omz, dil, gamma, Y of
+ * st_make_padded_arrays, the cycle (step) and the time, written as one
+ * binary legacy VTK rectilinear-grid file (the Silo library is not part of
+ * this build) to <vis_path>/<ddd>/<prefix>.000.vtk, ddd the three digits of
+ * cue_vis (0..999); the directory is created as make_dir_ (src/dirs.c)
+ * creates it.  Grad as for st_make_padded_arrays. */
+int  st_write_visual(st_ctx *c, const double *Grad, const char *vis_path, const char *prefix, int cue_vis,
+                     double time, int step);
 
 /* ---- 1-D spherical-radial family, batched ---------------------------------
  * Many independent problems, each one run of the reference's radial program

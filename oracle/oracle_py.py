@@ -66,6 +66,7 @@ def _load():
     lib.orc_shell_count.argtypes = [ctypes.c_void_p]
     lib.orc_compute_srm_stats.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
     lib.orc_shock_surface.argtypes = [ctypes.c_void_p, _dp, _dp]
+    lib.orc_make_padded_arrays.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
     rp = ctypes.POINTER(StRadialParams)
     ci, cd = ctypes.c_int, ctypes.c_double
     lib.orc_rad_radius.argtypes = [ci, cd, _dp]
@@ -234,6 +235,16 @@ class Oracle:
         a, b = np.zeros(1), np.zeros(1)
         lib().orc_compute_grad(ctypes.c_void_p(self._c), _p(G), _p(a), _p(b))
         return G, float(a[0]), float(b[0])
+
+    def make_padded_arrays(self, Grad):
+        """MakePaddedArrays (src/vis_silo_mf.f:440-689): W (11, Mx+1, Mz+1,
+        My+1) and the padded coordinates xx, yy, zz."""
+        nx, nz, ny = self.shape
+        G = np.ascontiguousarray(Grad, dtype=np.float64)
+        W = np.zeros((11, nx + 1, nz + 1, ny + 1))
+        xx, yy, zz = np.zeros(nx + 1), np.zeros(ny + 1), np.zeros(nz + 1)
+        lib().orc_make_padded_arrays(ctypes.c_void_p(self._c), _p(G), _p(W), _p(xx), _p(yy), _p(zz))
+        return W, xx, yy, zz
 
     def compute_srm_stats(self):
         na = lib().orc_shell_count(ctypes.c_void_p(self._c))

@@ -2097,3 +2097,44 @@ void orc_shock_surface(orc *c, double *rad_avg, double *rad_skew_rms) {
     *rad_avg = ra;
     *rad_skew_rms = sqrt(sk) / (n * ra);
 }
+
+/* MakePaddedArrays, src/vis_silo_mf.f:440-689, on one rank (Px = Py = Pz = 1).
+ * W(My+1, Mz+1, Mx+1, 11): the primitive variables of :494-510 (u, v, w =
+ * Q1..Q3 / Q4, rho = Q4, P = fac1 (Q5 - 0.5 Vs (Q1^2 + Q2^2 + Q3^2)) with
+ * fac1 = gamma_eff - 1, Vs = 1/Q4), the four Grad fields (w_x, w_y, w_z,
+ * dilatation), gamma_eff and Y.  Without neighbour ranks every padding node
+ * copies the last node of its direction: faces :640-666, edges :668-684,
+ * corner :686.  xx/yy/zz (Mx+1, My+1, Mz+1): the coordinates of Setup_Grid
+ * (src/grid.f:28-40, Uniform_X :116-128), the extra node one spacing
+ * (gxcor(2) - gxcor(1)) beyond the last (:486-491). */
+void orc_make_padded_arrays(orc *c, const double *Grad, double *W, double *xx, double *yy, double *zz) {
+    const int Mx = c->M[0], My = c->M[1], Mz = c->M[2];
+    const size_t n3 = c->n3, Pj = (size_t)My + 1, Pk = (size_t)Mz + 1;
+    const size_t np = Pj * Pk * ((size_t)Mx + 1);
+    const double *Q = c->Q;
+    for (int i = 0; i <= Mx; i++)
+        for (int k = 0; k <= Mz; k++)
+            for (int j = 0; j <= My; j++) {
+                const size_t p = (size_t)j + Pj * ((size_t)k + Pk * (size_t)i);
+                const size_t q = IX(c, j < My ? j : My - 1, k < Mz ? k : Mz - 1, i < Mx ? i : Mx - 1);
+                const double q1 = Q[q], q2 = Q[n3 + q], q3 = Q[2 * n3 + q], q4 = Q[3 * n3 + q], q5 = Q[4 * n3 + q];
+                const double fac1 = c->gamma_eff[q] - 1.0;
+                const double vs = 1.0 / q4;
+                W[p] = q1 / q4;
+                W[np + p] = q2 / q4;
+                W[2 * np + p] = q3 / q4;
+                W[3 * np + p] = q4;
+                W[4 * np + p] = fac1 * (q5 - 5.0e-1 * vs * (q1 * q1 + q2 * q2 + q3 * q3));
+                for (int f = 0; f < 4; f++) W[(5 + f) * np + p] = Grad[f * n3 + q];
+                W[9 * np + p] = c->gamma_eff[q];
+                W[10 * np + p] = c->Y[q];
+            }
+    const st_params *pp = &c->p;
+    const double st[3] = {pp->x_start, pp->y_start, pp->z_start}, ln[3] = {pp->x_leng, pp->y_leng, pp->z_leng};
+    double *cor[3] = {xx, yy, zz};
+    for (int d = 0; d < 3; d++) {
+        const int n = c->M[d];
+        for (int i = 0; i < n; i++) cor[d][i] = st[d] + ln[d] * (double)i / (double)(n - 1);
+        cor[d][n] = cor[d][n - 1] + (cor[d][1] - cor[d][0]);
+    }
+}

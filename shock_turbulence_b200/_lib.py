@@ -48,6 +48,8 @@ SIGNATURES = {
     "st_shell_count": [_ctx, ctypes.POINTER(ctypes.c_int)],
     "st_compute_srm_stats": [_ctx] + [ctypes.POINTER(ctypes.c_double)] * 4,
     "st_generate_shock_surface": [_ctx] + [ctypes.POINTER(ctypes.c_double)] * 2,
+    "st_make_padded_arrays": [_ctx, _dp, _dp, _dp, _dp, _dp],
+    "st_write_visual": [_ctx, _dp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int],
     "st_sync": [_ctx],
     "st_step_async": [_ctx, ctypes.c_int],
     "st_get_time": [_ctx, ctypes.POINTER(ctypes.c_double)],

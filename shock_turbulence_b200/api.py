@@ -8,11 +8,13 @@ CUDA) in the reference layout F(My,Mz,Mx[,n]), i.e. C-order shape
 Every failure raises :class:`StError`; nothing falls back to the CPU.
 """
 import ctypes
+import os
 
 import numpy as np
 
 from . import _lib
 from .params import StParams, default_params
+from .visual import visual_path
 
 
 class StError(RuntimeError):
@@ -226,6 +228,29 @@ class Solver:
         self._check(self.lib.st_generate_shock_surface(self._h, ctypes.byref(a), ctypes.byref(b)),
                     "Generate_Shock_Surface")
         return a.value, b.value
+
+    def MakePaddedArrays(self, Grad=None):
+        """MakePaddedArrays (src/vis_silo_mf.f:440): returns (W, xx, yy, zz),
+        W (11, Mx+1, Mz+1, My+1) = u, v, w, rho, P, w_x, w_y, w_z,
+        dilatation, gamma_eff, Y at the nodes of the grid padded by one node
+        per direction.  Grad: the 4 fields of Compute_Grad, or None to
+        compute them first."""
+        nx, nz, ny = self.shape
+        W = np.zeros((11, nx + 1, nz + 1, ny + 1))
+        xx, yy, zz = np.zeros(nx + 1), np.zeros(ny + 1), np.zeros(nz + 1)
+        g = None if Grad is None else self._a(Grad, 4)
+        self._check(self.lib.st_make_padded_arrays(self._h, g, W.ctypes.data, xx.ctypes.data, yy.ctypes.data,
+                                                   zz.ctypes.data), "MakePaddedArrays")
+        return W, xx, yy, zz
+
+    def Write_Visual_Silo(self, time, step, vis_path, prefix, cue_vis, Grad=None):
+        """Write_Visual_Silo (src/vis_silo_mf.f:7): the visual fields as one
+        legacy VTK rectilinear-grid file (the Silo library is not part of
+        this build); returns its path, <vis_path>/<ddd>/<prefix>.000.vtk."""
+        g = None if Grad is None else self._a(Grad, 4)
+        self._check(self.lib.st_write_visual(self._h, g, os.fsencode(vis_path), os.fsencode(prefix), int(cue_vis),
+                                             float(time), int(step)), "Write_Visual_Silo")
+        return visual_path(vis_path, prefix, cue_vis)
 
     def monitors(self):
         out = np.zeros(10)

@@ -1,6 +1,10 @@
 // st_api.cpp - C ABI (include/st_b200.h): context life cycle, COMMON-block
 // mirrors, host/device argument staging and the reference-named entry points.
+#include <sys/stat.h>
+#include <algorithm>
+#include <cerrno>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -132,6 +136,88 @@ class Args {
     bool err_ = false;
 };
 
+
+// device memory of the context's device (used in place) or not (staged)
+static bool on_device(const st_ctx *c, const void *p) {
+    cudaPointerAttributes at{};
+    bool dev = false;
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+        (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged))
+        dev = at.device == c->dev;
+    cudaGetLastError();
+    return dev;
+}
+
+// ---- visual file: legacy VTK rectilinear grid ------------------------------
+// The reference writes its visual fields with the LLNL Silo library
+// (src/vis_silo_mf.f:7-277: a quad mesh with collinear coordinates "yc",
+// "zc", "xc" of sizes My+1, Mz+1, Mx+1, eleven node-centred double
+// variables, cycle and time options).  Silo is not available here; the same
+// mesh, variables, names, centring, cycle and time go into one legacy VTK
+// file (binary, big-endian), which VisIt and ParaView read: the VTK x axis is
+// the reference's first mesh axis (y), then z, then x.
+static const char *kVisNames[11] = {"rho", "U", "V", "W", "P", "omx", "omy", "omz", "dil", "gamma", "Y"};
+static const int kVisField[11] = {3, 0, 1, 2, 4, 5, 6, 7, 8, 9, 10};   // W(..., f) of each name, 0-based
+
+static bool put_be(FILE *f, const double *v, size_t n) {
+    std::vector<uint64_t> b(std::min<size_t>(n, 1 << 20));
+    for (size_t o = 0; o < n; o += b.size()) {
+        const size_t m = std::min(b.size(), n - o);
+        for (size_t q = 0; q < m; q++) {
+            uint64_t u;
+            std::memcpy(&u, v + o + q, 8);
+            b[q] = __builtin_bswap64(u);
+        }
+        if (std::fwrite(b.data(), 8, m, f) != m) return false;
+    }
+    return std::fputc('\n', f) != EOF;
+}
+
+// <vis_path>/<ddd>/<prefix>.000.vtk, ddd the three digits of cue_vis (the
+// directory make_dir_ creates, src/dirs.c, and the group file name of
+// src/vis_silo_mf.f:97-106 for group 0)
+static std::string visual_path(const char *vis_path, const char *prefix, int cue_vis, std::string *dir) {
+    char d[16];
+    std::snprintf(d, sizeof d, "/%d%d%d", (cue_vis / 100) % 10, (cue_vis % 100) / 10, cue_vis % 10);
+    *dir = std::string(vis_path) + d;
+    return *dir + "/" + prefix + ".000.vtk";
+}
+
+static int write_vtk(st_ctx *c, const std::string &path, const double *Wd, const double *cor[3], double time,
+                     int step) {
+    const int Mx = c->dm.n[0], My = c->dm.n[1], Mz = c->dm.n[2];
+    const size_t np = padded_nodes(c);
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return fail(c, ST_E_ARG, "cannot create " + path + ": " + std::strerror(errno));
+    bool ok = true;
+    std::vector<double> h(np);
+    ok = ok && std::fprintf(f, "# vtk DataFile Version 3.0\nshock-turbulence visual fields, time %.17g, step %d\n"
+                                "BINARY\nDATASET RECTILINEAR_GRID\nFIELD FieldData 2\nTIME 1 1 double\n",
+                            time, step) > 0;
+    ok = ok && put_be(f, &time, 1);
+    ok = ok && std::fprintf(f, "CYCLE 1 1 int\n") > 0;
+    const uint32_t cyc = __builtin_bswap32((uint32_t)step);
+    ok = ok && std::fwrite(&cyc, 4, 1, f) == 1 && std::fputc('\n', f) != EOF;
+    ok = ok && std::fprintf(f, "DIMENSIONS %d %d %d\n", My + 1, Mz + 1, Mx + 1) > 0;
+    const char *axis[3] = {"X", "Y", "Z"};
+    const int order[3] = {1, 2, 0}, len[3] = {My + 1, Mz + 1, Mx + 1};
+    for (int a = 0; a < 3 && ok; a++) {
+        ok = std::fprintf(f, "%s_COORDINATES %d double\n", axis[a], len[a]) > 0;
+        ok = ok && put_be(f, cor[order[a]], (size_t)len[a]);
+    }
+    ok = ok && std::fprintf(f, "POINT_DATA %zu\n", np) > 0;
+    for (int v = 0; v < 11 && ok; v++) {
+        if (cudaMemcpy(h.data(), Wd + (size_t)kVisField[v] * np, np * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::fclose(f);
+            return fail(c, ST_E_CUDA, "visual field copy");
+        }
+        ok = std::fprintf(f, "SCALARS %s double 1\nLOOKUP_TABLE default\n", kVisNames[v]) > 0;
+        ok = ok && put_be(f, h.data(), np);
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (!ok) return fail(c, ST_E_ARG, "write error on " + path);
+    return ST_OK;
+}
 
 }  // namespace st
 
@@ -1082,6 +1168,57 @@ int st_generate_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms) 
     API_BEGIN(c)
     ST_TRY(dev_shock_surface(c, rad_avg, rad_skew_rms));
     return ST_OK;
+    API_END(c)
+}
+
+int st_make_padded_arrays(st_ctx *c, const double *Grad, double *W, double *xx, double *yy, double *zz) {
+    SINGLE_CASE(c);
+    if (!W) return ST_E_ARG;
+    MF_ONLY(c, "MakePaddedArrays");
+    API_BEGIN(c)
+    Args a(c);
+    const double *Gd = Grad ? a.map(Grad, 4, true, false) : nullptr;
+    const size_t np = padded_nodes(c), wbytes = 11 * np * sizeof(double);
+    const bool wdev = on_device(c, W);
+    // staged: whole scratch fields covering the 11 padded fields
+    Scratch ws(c, wdev ? 1 : (int)((11 * np + c->fs - 1) / c->fs));
+    double *Wd = wdev ? W : (double *)ws;
+    ST_TRY(dev_make_padded_arrays(c, Gd, Wd));
+    if (!wdev) ST_CUDA(c, cudaMemcpyAsync(W, Wd, wbytes, cudaMemcpyDeviceToHost, c->stream));
+    ST_TRY(a.finish());
+    double *out[3] = {xx, yy, zz};
+    std::vector<double> cor[3];
+    double *cp[3];
+    for (int d = 0; d < 3; d++) { cor[d].resize(c->dm.n[d] + 1); cp[d] = cor[d].data(); }
+    padded_coords(c, cp);
+    for (int d = 0; d < 3; d++)
+        if (out[d]) ST_CUDA(c, cudaMemcpy(out[d], cp[d], cor[d].size() * sizeof(double), cudaMemcpyDefault));
+    return ST_OK;
+    API_END(c)
+}
+
+int st_write_visual(st_ctx *c, const double *Grad, const char *vis_path, const char *prefix, int cue_vis,
+                    double time, int step) {
+    SINGLE_CASE(c);
+    if (!vis_path || !prefix || cue_vis < 0 || cue_vis > 999) return ST_E_ARG;
+    MF_ONLY(c, "Write_Visual_Silo");
+    API_BEGIN(c)
+    Args a(c);
+    const double *Gd = Grad ? a.map(Grad, 4, true, false) : nullptr;
+    const size_t np = padded_nodes(c);
+    Scratch ws(c, (int)((11 * np + c->fs - 1) / c->fs));
+    ST_TRY(dev_make_padded_arrays(c, Gd, ws));
+    ST_TRY(a.finish());
+    std::vector<double> cor[3];
+    double *cp[3];
+    for (int d = 0; d < 3; d++) { cor[d].resize(c->dm.n[d] + 1); cp[d] = cor[d].data(); }
+    padded_coords(c, cp);
+    std::string dir;
+    const std::string path = visual_path(vis_path, prefix, cue_vis, &dir);
+    if (mkdir(dir.c_str(), S_IRWXU | S_IRWXG) != 0 && errno != EEXIST)
+        return fail(c, ST_E_ARG, "cannot create directory " + dir + ": " + std::strerror(errno));
+    const double *ccp[3] = {cp[0], cp[1], cp[2]};
+    return write_vtk(c, path, ws, ccp, time, step);
     API_END(c)
 }
 

@@ -387,4 +387,74 @@ int dev_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms) {
     return ST_OK;
 }
 
+// ---- MakePaddedArrays -----------------------------------------------------------
+// src/vis_silo_mf.f:440-689 on one rank (Px = Py = Pz = 1): the eleven visual
+// fields at the nodes of the grid padded by one node per direction,
+// W(My+1, Mz+1, Mx+1, 11) = (u, v, w, rho, P, w_x, w_y, w_z, dilatation,
+// gamma_eff, Y), with the primitive variables of :494-510 (u = Q1/Q4, ...,
+// P = fac1 (Q5 - 0.5 Vs (Q1^2 + Q2^2 + Q3^2)), fac1 = gamma_eff - 1,
+// Vs = 1/Q4).  With no neighbour rank each padding node copies the last node
+// of its direction (faces :640-666, edges :668-684, corner :686), so the
+// source cell is the node index clamped to the grid.  One thread per padded
+// node: 11 fields read, 11 written.
+__global__ void k_padded(const double *__restrict__ Q, const double *__restrict__ Grad,
+                         const double *__restrict__ gam, const double *__restrict__ Y, double *__restrict__ W,
+                         int My, int Mz, int Mx, size_t n3) {
+    const size_t Pj = (size_t)My + 1, Pk = (size_t)Mz + 1, np = Pj * Pk * ((size_t)Mx + 1);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < np; p += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = p / Pj, j = p - r * Pj, i = r / Pk, k = r - i * Pk;
+        const size_t q = (j < (size_t)My ? j : My - 1) +
+                         (size_t)My * ((k < (size_t)Mz ? k : Mz - 1) + (size_t)Mz * (i < (size_t)Mx ? i : Mx - 1));
+        const double q1 = Q[q], q2 = Q[n3 + q], q3 = Q[2 * n3 + q], q4 = Q[3 * n3 + q], q5 = Q[4 * n3 + q];
+        const double g = gam[q];
+        const double fac1 = g - 1.0;
+        const double vs = 1.0 / q4;
+        W[p] = q1 / q4;
+        W[np + p] = q2 / q4;
+        W[2 * np + p] = q3 / q4;
+        W[3 * np + p] = q4;
+        W[4 * np + p] = fac1 * (q5 - 5.0e-1 * vs * (q1 * q1 + q2 * q2 + q3 * q3));
+#pragma unroll
+        for (int f = 0; f < 4; f++) W[(5 + f) * np + p] = Grad[f * n3 + q];
+        W[9 * np + p] = g;
+        W[10 * np + p] = Y[q];
+    }
+}
+
+size_t padded_nodes(const st_ctx *c) {
+    return ((size_t)c->dm.n[0] + 1) * ((size_t)c->dm.n[1] + 1) * ((size_t)c->dm.n[2] + 1);
+}
+
+// W (device, 11 padded fields) from the context's state; Grad (device, the
+// 4 fields of Compute_Grad) or NULL: then Compute_Grad runs first, as Output
+// calls it before the visual file is written (src/out_mf.f:681-698)
+static int launch_padded(st_ctx *c, const double *Grad, double *W) {
+    const size_t np = padded_nodes(c);
+    const int blocks = (int)std::min<size_t>((np + kRB - 1) / kRB, (size_t)148 * 16);
+    c->launches++;
+    k_padded<<<blocks, kRB, 0, c->stream>>>(c->Q, Grad, c->gamma_eff, c->Y, W, c->dm.n[1], c->dm.n[2], c->dm.n[0],
+                                            c->dm.n3);
+    ST_CUDA(c, cudaGetLastError());
+    return ST_OK;
+}
+
+int dev_make_padded_arrays(st_ctx *c, const double *Grad, double *W) {
+    if (Grad) return launch_padded(c, Grad, W);
+    Scratch gs(c, 4);
+    double maxdil, enstrophy;
+    ST_TRY(dev_compute_grad(c, gs, &maxdil, &enstrophy));
+    return launch_padded(c, gs, W);
+}
+
+// the padded coordinates (src/vis_silo_mf.f:486-491): Setup_Grid's nodes
+// (src/grid.f:28-40, Uniform_X :116-128) and one spacing beyond the last
+void padded_coords(const st_ctx *c, double *cor[3]) {
+    const Grid g = grid_of(c);
+    for (int d = 0; d < 3; d++) {
+        const int n = g.n[d];
+        for (int i = 0; i < n; i++) cor[d][i] = g.start[d] + g.leng[d] * (double)i / (double)(n - 1);
+        cor[d][n] = cor[d][n - 1] + (cor[d][1] - cor[d][0]);
+    }
+}
+
 }  // namespace st

@@ -287,6 +287,9 @@ int dev_monitors(st_ctx *c);
 int shell_count(const st_ctx *c);
 int dev_compute_grad(st_ctx *c, double *Grad, double *maxdil, double *enstrophy);
 int dev_compute_srm_stats(st_ctx *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg);
+size_t padded_nodes(const st_ctx *c);
+int dev_make_padded_arrays(st_ctx *c, const double *Grad, double *W);
+void padded_coords(const st_ctx *c, double *cor[3]);
 int dev_shock_surface(st_ctx *c, double *rad_avg, double *rad_skew_rms);
 
 }  // namespace st

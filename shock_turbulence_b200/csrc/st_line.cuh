@@ -229,7 +229,9 @@ __device__ __forceinline__ void cyc_fix(V (&r)[N], const A *__restrict__ Kt, int
 // products of 2^k consecutive transfer factors in [kScanSteps][kMaxSeg]
 // tables.  Lane s of a warp takes segment s and reads the others by
 // shuffles (no CTA barrier); the arithmetic and its order are those of a
-// Hillis-Steele scan over shared memory.  Warps take lines w, w + nwarps, ...
+// Hillis-Steele scan over shared memory.  The full warps take lines w,
+// w + nwarps, ... (a CTA has 16 P threads: with P odd its last warp is a half
+// warp, which takes none; every full warp has 32 >= P lanes).
 __device__ __forceinline__ double shfl_seg(bool up, double v, int d) {
     return up ? __shfl_up_sync(0xffffffffu, v, d) : __shfl_down_sync(0xffffffffu, v, d);
 }
@@ -240,6 +242,7 @@ __device__ __forceinline__ F2 shfl_seg(bool up, F2 v, int d) {
 template <bool FWD, class V, class A>
 __device__ __forceinline__ void seg_scan1_warp(V *buf, const A *__restrict__ tab, int P) {
     const int l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if ((int)(threadIdx.x >> 5) >= nw) return;     // the half warp of an odd P takes no line
     for (int ln = threadIdx.x >> 5; ln < kLanes; ln += nw) {
         V *row = buf + ln * (kMaxSeg + 1);
         V f = l < P ? row[l] : V(0.0);
@@ -331,11 +334,12 @@ __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s,
 // ([kScanSteps][kMaxSeg][4] tables).  Lane s of a warp takes segment s; the
 // values of the other segments come by shuffles, so the scan needs no CTA
 // barrier.  The arithmetic and its order are those of a Hillis-Steele scan
-// over shared memory.  Warps take lines w, w + nwarps, ... (P/2 warps for
-// the 16 lines; lanes >= P idle).
+// over shared memory.  The full warps take lines w, w + nwarps, ... (the
+// half warp of an odd P takes none; lanes >= P idle).
 template <bool FWD>
 __device__ __forceinline__ void seg_scan_warp(double2 *buf, const double *__restrict__ tab, int P) {
     const int l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if ((int)(threadIdx.x >> 5) >= nw) return;     // the half warp of an odd P takes no line
     for (int ln = threadIdx.x >> 5; ln < kLanes; ln += nw) {
         double2 *row = buf + ln * (kMaxSeg + 1);
         double f1 = 0.0, f2 = 0.0;

@@ -81,6 +81,8 @@ REF_MF = [
     ("Compute_Grad", [], "src/grad_sym.f:13"),
     ("Compute_SRM_Stats", ["step"], "pproc/pproc_mf.f:4"),
     ("Generate_Shock_Surface", [], "src/shock.f:163"),
+    ("MakePaddedArrays", ["W", "xx", "yy", "zz", "nfields"], "src/vis_silo_mf.f:440"),
+    ("Write_Visual_Silo", ["time", "step"], "src/vis_silo_mf.f:7"),
 ]
 REF_PERIODIC = [
     ("Setup_Derivatives", [], "src/derivCDopt6_periodic.f:9"),
