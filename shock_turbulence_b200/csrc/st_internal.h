@@ -16,6 +16,8 @@ namespace st {
 
 constexpr int kMaxSeg = 32;       // max segments per line (warps per CTA)
 constexpr int kLanes = 16;        // lines per CTA (half a warp; a warp holds two segments)
+constexpr int kLineThreads = kLanes * kMaxSeg;     // threads of a line-kernel CTA at most
+constexpr int kLineCtasPerSm = 32 / kLanes;        // resident CTAs per SM at 64 registers a thread
 constexpr int kScanSteps = 5;     // log2(kMaxSeg): steps of a scan over the segments
 
 // A line of n rows is split into P = n/S segments of S rows; thread t of a CTA

@@ -183,12 +183,10 @@ __device__ __forceinline__ void store_rows(const V (&r)[N], T *__restrict__ O, c
 
 // shared buffers for the segment end values of one solve, and the corner
 // values of a periodic line (rows 0, 1, n-2, n-1 of the banded solution)
-// (a and b have one spare segment row: the pentadiagonal solve views each as
-// [kLanes][kMaxSeg + 1] pairs)
 template <class V>
 struct CarryBufT {
-    alignas(16) V a[kMaxSeg + 1][kLanes][2];
-    alignas(16) V b[kMaxSeg + 1][kLanes][2];
+    V a[kMaxSeg][kLanes][2];
+    V b[kMaxSeg][kLanes][2];
     V cy[kLanes][4];
 };
 using CarryBuf = CarryBufT<double>;
@@ -260,6 +258,20 @@ __device__ __forceinline__ void seg_scan1_warp(V *buf, const A *__restrict__ tab
 // (src/tridiagonal.f90:274-284) per segment with zero carries, then the
 // carry corrections.  Caller guarantees cb is free (synchronised).
 template <int S, int N, class V, class A>
+__device__ __forceinline__ void tri_back(V (&r)[N], const TriTabT<A> &T, int a, bool flat) {
+    if (flat) {
+        const A up = T.cup, id = T.cid;
+        r[S - 1] = r[S - 1] * id;
+#pragma unroll
+        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - up * r[t + 1]) * id;
+    } else {
+        r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
+#pragma unroll
+        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
+    }
+}
+
+template <int S, int N, class V, class A>
 __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s, int P, int lane,
                                           CarryBufT<V> &cb) {
     const int a = s * S;
@@ -274,87 +286,49 @@ __device__ __forceinline__ void tri_solve(V (&r)[N], const TriTabT<A> &T, int s,
     }
     // Carries reaching more than twice as many segments as a scan has steps
     // (short segments: small grids, n <= 128) come from a log2(P)-step warp
-    // scan, f(s) = a(s) + B_s f(s-1), carry into s = f(s-1); otherwise from
-    // the sum over the kf segments before s (measured faster for n >= 256).
-    // The choice is uniform over the CTA.
+    // scan per direction, f(s) = a(s) + B_s f(s-1), carry into s = f(s-1);
+    // otherwise from the sum over the kf segments before s (kb after s for
+    // the right carry; measured faster for n >= 256).  The choice is uniform
+    // over the CTA.
     const bool scan = T.kf > 2 * kScanSteps || T.kb > 2 * kScanSteps;
-    constexpr int LS = kMaxSeg + 1;
-    V cin = V(0.0);
     if (scan) {
+        constexpr int LS = kMaxSeg + 1;
+        V cin = V(0.0);
         V *fa = &cb.a[0][0][0];          // [kLanes][kMaxSeg + 1]
         fa[lane * LS + s] = r[S - 1];
         __syncthreads();
         seg_scan1_warp<true>(fa, T.sf, P);
         __syncthreads();
         if (s > 0) cin = fa[lane * LS + s - 1];
-    } else {
-        cb.a[s][lane][0] = r[S - 1];
-        __syncthreads();
-#pragma unroll 4
-        for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
-    }
 #pragma unroll
-    for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
-    if (flat) {
-        const A up = T.cup, id = T.cid;
-        r[S - 1] = r[S - 1] * id;
-#pragma unroll
-        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - up * r[t + 1]) * id;
-    } else {
-        r[S - 1] = r[S - 1] * __ldg(T.id + a + S - 1);
-#pragma unroll
-        for (int t = S - 2; t >= 0; t--) r[t] = (r[t] - __ldg(T.up + a + t) * r[t + 1]) * __ldg(T.id + a + t);
-    }
-    V ein = V(0.0);
-    if (scan) {
+        for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
+        tri_back<S>(r, T, a, flat);
         // the second buffer: the first is still read until the barrier below
+        V ein = V(0.0);
         V *fb = &cb.b[0][0][0];
         fb[lane * LS + s] = r[0];
         __syncthreads();
         seg_scan1_warp<false>(fb, T.sb, P);
         __syncthreads();
         if (s + 1 < P) ein = fb[lane * LS + s + 1];
+#pragma unroll
+        for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.h + a + t), ein, r[t]);
     } else {
+        V cin = V(0.0), ein = V(0.0);
+        cb.a[s][lane][0] = r[S - 1];
+        __syncthreads();
+#pragma unroll 4
+        for (int sp = max(0, s - T.kf); sp < s; sp++) cin = vfma(__ldg(T.wf + sp * P + s), cb.a[sp][lane][0], cin);
+#pragma unroll
+        for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.g + a + t), cin, r[t]);
+        tri_back<S>(r, T, a, flat);
         cb.b[s][lane][0] = r[0];
         __syncthreads();
 #pragma unroll 4
         for (int sp = s + 1, se = min(P, s + 1 + T.kb); sp < se; sp++)
             ein = vfma(__ldg(T.wb + sp * P + s), cb.b[sp][lane][0], ein);
-    }
 #pragma unroll
-    for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.h + a + t), ein, r[t]);
-}
-
-// ---- scan of 2-vector carries over the segments, one warp per line --------
-// buf[ln*(kMaxSeg+1) + s] holds segment s's pair of line ln on entry and the
-// inclusive scan value on exit:
-//   FWD:  f(s) = a(s) + T_k(s) f(s - 2^k)   for k = 0, 1, ... while 2^k < P
-//   back: g(s) = b(s) + U_k(s) g(s + 2^k)
-// with T_k/U_k the products of 2^k consecutive segment transfer matrices
-// ([kScanSteps][kMaxSeg][4] tables).  Lane s of a warp takes segment s; the
-// values of the other segments come by shuffles, so the scan needs no CTA
-// barrier.  The arithmetic and its order are those of a Hillis-Steele scan
-// over shared memory.  The full warps take lines w, w + nwarps, ... (the
-// half warp of an odd P takes none; lanes >= P idle).
-template <bool FWD>
-__device__ __forceinline__ void seg_scan_warp(double2 *buf, const double *__restrict__ tab, int P) {
-    const int l = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if ((int)(threadIdx.x >> 5) >= nw) return;     // the half warp of an odd P takes no line
-    for (int ln = threadIdx.x >> 5; ln < kLanes; ln += nw) {
-        double2 *row = buf + ln * (kMaxSeg + 1);
-        double f1 = 0.0, f2 = 0.0;
-        if (l < P) { const double2 v = row[l]; f1 = v.x; f2 = v.y; }
-        for (int k = 0, d = 1; d < P; k++, d <<= 1) {
-            const double o1 = FWD ? __shfl_up_sync(0xffffffffu, f1, d) : __shfl_down_sync(0xffffffffu, f1, d);
-            const double o2 = FWD ? __shfl_up_sync(0xffffffffu, f2, d) : __shfl_down_sync(0xffffffffu, f2, d);
-            if (FWD ? (l >= d && l < P) : (l + d < P)) {
-                const double2 *m = reinterpret_cast<const double2 *>(tab + ((size_t)k * kMaxSeg + l) * 4);
-                const double2 m01 = __ldg(m), m23 = __ldg(m + 1);
-                f1 = fma(m01.x, o1, fma(m01.y, o2, f1));
-                f2 = fma(m23.x, o1, fma(m23.y, o2, f2));
-            }
-        }
-        if (l < P) row[l] = make_double2(f1, f2);
+        for (int t = 0; t < S; t++) r[t] = vfma(__ldg(T.h + a + t), ein, r[t]);
     }
 }
 
@@ -386,17 +360,29 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
         }
     }
     // carry into segment s: c(s) = f(s-1) of the inclusive scan
-    // f(s) = a(s) + M_s f(s-1) over the segments' end values a(s) (the reach
-    // of the carries, up to the whole line for this nearly singular system,
-    // costs every segment the same); one warp scans one line
-    constexpr int LS = kMaxSeg + 1;
-    double2 *fa = reinterpret_cast<double2 *>(&cb.a[0][0][0]);
-    fa[lane * LS + s] = make_double2(r[S - 1], (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0);
+    // f(s) = a(s) + M_s f(s-1) over the segments' end values a(s), in
+    // log2(P) steps over a double buffer (the reach of the carries, up to the
+    // whole line for this nearly singular system, costs every segment the
+    // same)
+    double f1 = r[S - 1], f2 = (S >= 2) ? r[S >= 2 ? S - 2 : 0] : 0.0;
+    double(*cur)[kLanes][2] = cb.a;
+    double(*nxt)[kLanes][2] = cb.b;
+    cur[s][lane][0] = f1;
+    cur[s][lane][1] = f2;
     __syncthreads();
-    seg_scan_warp<true>(fa, T.sf, P);
-    __syncthreads();
-    double c1 = 0.0, c2 = 0.0;
-    if (s > 0) { const double2 cv = fa[lane * LS + s - 1]; c1 = cv.x; c2 = cv.y; }
+    for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+        if (s >= d) {
+            const double *m = T.sf + ((size_t)k * kMaxSeg + s) * 4;
+            const double o1 = cur[s - d][lane][0], o2 = cur[s - d][lane][1];
+            f1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, f1));
+            f2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, f2));
+        }
+        nxt[s][lane][0] = f1;
+        nxt[s][lane][1] = f2;
+        __syncthreads();
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+    }
+    const double c1 = s > 0 ? cur[s - 1][lane][0] : 0.0, c2 = s > 0 ? cur[s - 1][lane][1] : 0.0;
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.g1 + a + t), c1, fma(__ldg(T.g2 + a + t), c2, r[t]));
     if (flat) {
@@ -417,15 +403,28 @@ __device__ __forceinline__ void pen_solve(double (&r)[N], const PenTab &T, int s
             r[t] = v * __ldg(T.id + a + t);
         }
     }
-    // carry from the right: e(s) = g(s+1) of g(s) = b(s) + N_s g(s+1), in the
-    // second buffer (the first is still read until the barrier below)
-    double2 *fb = reinterpret_cast<double2 *>(&cb.b[0][0][0]);
-    fb[lane * LS + s] = make_double2(r[0], (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0);
+    // carry from the right: e(s) = g(s+1) of g(s) = b(s) + N_s g(s+1); the
+    // first write goes to the buffer nobody reads after the forward scan
+    double g1 = r[0], g2 = (S >= 2) ? r[S >= 2 ? 1 : 0] : 0.0;
+    nxt[s][lane][0] = g1;
+    nxt[s][lane][1] = g2;
+    {
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+    }
     __syncthreads();
-    seg_scan_warp<false>(fb, T.sb, P);
-    __syncthreads();
-    double e1 = 0.0, e2 = 0.0;
-    if (s + 1 < P) { const double2 ev = fb[lane * LS + s + 1]; e1 = ev.x; e2 = ev.y; }
+    for (int k = 0, d = 1; d < P; k++, d <<= 1) {
+        if (s + d < P) {
+            const double *m = T.sb + ((size_t)k * kMaxSeg + s) * 4;
+            const double o1 = cur[s + d][lane][0], o2 = cur[s + d][lane][1];
+            g1 = fma(__ldg(m + 0), o1, fma(__ldg(m + 1), o2, g1));
+            g2 = fma(__ldg(m + 2), o1, fma(__ldg(m + 3), o2, g2));
+        }
+        nxt[s][lane][0] = g1;
+        nxt[s][lane][1] = g2;
+        __syncthreads();
+        double(*t)[kLanes][2] = cur; cur = nxt; nxt = t;
+    }
+    const double e1 = s + 1 < P ? cur[s + 1][lane][0] : 0.0, e2 = s + 1 < P ? cur[s + 1][lane][1] : 0.0;
 #pragma unroll
     for (int t = 0; t < S; t++) r[t] = fma(__ldg(T.h1 + a + t), e1, fma(__ldg(T.h2 + a + t), e2, r[t]));
 }

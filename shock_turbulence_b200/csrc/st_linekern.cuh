@@ -50,7 +50,7 @@ using LineArgsF = LineArgsT<float>;
 // L2 prefetch of the rows the block kAhead blocks later will load (about one
 // wave of resident CTAs ahead: 2 per SM on 148 SMs), so that the next wave's
 // loads find their lines in L2 while this wave solves.
-constexpr unsigned kAhead = 2 * 148;
+constexpr unsigned kAhead = kLineCtasPerSm * 148;
 __device__ __forceinline__ void pf_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 template <int S, bool YT, int OP, class T>
@@ -83,12 +83,13 @@ __device__ __forceinline__ void get_rows(V (&v)[S + 2 * H], const A *tile, const
     if (YT) ytile_rows<S, H>(v, tile, lane, a, n, cyc);
     else load_rows<S, H, OP>(v, F, m, lane, a, n, cyc);
 }
-template <int S, bool YT, int N, class T, class V, class A>
+// SYNCED: a barrier since the last read of the tile (the solves' exchange)
+template <int S, bool YT, bool SYNCED, int N, class T, class V, class A>
 __device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const ColMap &m,
                                          int lane, int a, int n, int add, const T *E1 = nullptr,
                                          const T *E2 = nullptr) {
     if (YT) {
-        __syncthreads();                 // every thread has finished reading the tile
+        if (!SYNCED) __syncthreads();    // every thread has finished reading the tile
         ytile_put<S>(tile, v, lane, a, n);
         __syncthreads();
         ytile_store<T>(tile, O, m.base, n, add);
@@ -99,7 +100,7 @@ __device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const C
 
 // DF*_sym/_asym and the periodic DF*: O1 (=|+=) cadd * dF/ds
 template <int S, bool YT, int OP, bool CYC, class T>
-__global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_dfd(LineArgsT<T> a) {
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
     V v[S + 4];
@@ -108,14 +109,14 @@ __global__ void __launch_bounds__(512, 2) k_dfd(LineArgsT<T> a) {
     rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
-    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, a.iadd, a.E1, a.E2);
+    put_rows<S, YT, true>(v, tile, a.O1, m, lane, row0, n, a.iadd, a.E1, a.E2);
 }
 
 // D2F*2_sym/_asym and the periodic D2F*2: O2 = d2F/ds2; if iadd, O1 = dF/ds
 // (cadd = 1).  The first
 // derivative re-reads the rows (the CTA's lines are still in L2).
 template <int S, bool YT, bool CYC, class T>
-__global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_d2fd2(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
         rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
         if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t2.cyc, s, a.P, lane, cb);
-        put_rows<S, YT>(v, tile, a.O2, m, lane, row0, n, 0, a.E1, a.E2);
+        put_rows<S, YT, true>(v, tile, a.O2, m, lane, row0, n, 0, a.E1, a.E2);
     }
     if (a.iadd) {
         __syncthreads();   // carry buffers and tile are reused
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
         rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
         tri_solve<S>(v, a.t1, s, a.P, lane, cb);
         if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
-        put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+        put_rows<S, YT, true>(v, tile, a.O1, m, lane, row0, n, 0);
     }
 }
 
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(512, 2) k_d2fd2(LineArgsT<T> a) {
 // F (including the boundary re-reads) happens before the solve's first
 // barrier and every write after its last one.
 template <int S, bool YT, bool CYC, class T>
-__global__ void __launch_bounds__(512, 2) k_filter(LineArgsT<T> a) {
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_filter(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
@@ -155,13 +156,13 @@ __global__ void __launch_bounds__(512, 2) k_filter(LineArgsT<T> a) {
     rhs_filter<S, 4>(v, row0, n, a.asym, CYC, a.K, rd);
     pen_solve<S>(v, a.p, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 8, 4>(v, a.p.cyc, s, a.P, lane, cb);
-    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+    put_rows<S, YT, true>(v, tile, a.O1, m, lane, row0, n, 0);
 }
 
 // Gaussian_Filter_X/Y/Z (both families): O1 = explicit 9-point Gaussian of F
 // (O1 != F)
 template <int S, bool YT, bool CYC, class T>
-__global__ void __launch_bounds__(512, 2) k_gauss(LineArgsT<T> a) {
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_gauss(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(512, 2) k_gauss(LineArgsT<T> a) {
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
     if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
     rhs_gauss<S, 4>(v, row0, n, CYC, a.K, rd);
-    put_rows<S, YT>(v, tile, a.O1, m, lane, row0, n, 0);
+    put_rows<S, YT, false>(v, tile, a.O1, m, lane, row0, n, 0);
 }
 
 enum OpKind { OP_D1, OP_D2, OP_FILTER, OP_GAUSS };

@@ -2,8 +2,8 @@
 
 A line of n points is cut into P = n/S segments (S the smallest of 2, 3, 4,
 6, 8, 12, 16 with n/S <= 32) and a CTA runs 16 lines x P segments, 16 P
-threads.  The segment carries of the compact filter (always) and of the
-tridiagonal solves of short segments are scanned one line per warp.  With P
+threads.  The compact filter scans its segment carries across the CTA; the
+tridiagonal solves of short segments scan theirs one line per warp.  With P
 odd (n = 272: S = 16, P = 17) the CTA ends in a half warp, which takes no
 line; with P < 32 the warps take more than one line each (n = 48: P = 24,
 12 warps for 16 lines; n = 80: P = 20).  Both families (_mf symmetric octant
