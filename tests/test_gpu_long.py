@@ -11,8 +11,7 @@ step tests hold after 3, and the same for the simulated time (the sum of the
 differences of the segmented line solves (~1e-14) must not grow through a
 shocked flow; the test records the difference at steps 1, 10, 25, 50 and
 100 so a failure shows how it grew.  The cases use the reference build's
-second RK loop (rk_mode 0); the other RK option is covered over 3 steps in
-test_gpu_physics.py."""
+RK option (rk_mode 0), and one case the other option (rk_mode 1)."""
 import numpy as np
 import pytest
 
@@ -73,12 +72,19 @@ def march(s, o, with_y):
 # the same way (3e-12 at step 50, 2e-8 at step 100).  No implementation
 # that does not repeat the reference's operation order bit for bit can
 # meet 1e-10 there.
-@pytest.mark.parametrize("grid,p_ratio", [((32, 64, 32), 100.0), ((64, 64, 64), 20.0)], ids=["32x64x32", "64^3"])
-def test_mf_blast_100_steps(oracle_mod, grid, p_ratio):
+#
+# The other RK option (rk_mode 1: the second five-stage loop reuses
+# alpha1/beta1, so both loops of a step advance the state by a time step)
+# is less robust on these blasts: on 32x64x32 the oracle itself overflows to
+# NaN at step 72 with pressure ratio 100 and at step 99 with 20, so its
+# 100-step case uses pressure ratio 5, which the oracle runs stably.
+@pytest.mark.parametrize("grid,p_ratio,rk", [((32, 64, 32), 100.0, 0), ((64, 64, 64), 20.0, 0),
+                                             ((32, 64, 32), 5.0, 1)], ids=["32x64x32", "64^3", "32x64x32-rk1"])
+def test_mf_blast_100_steps(oracle_mod, grid, p_ratio, rk):
     """_mf octant: symmetry planes, sponge and outflow faces, two species,
     molecular viscosity on (Re 100), artificial viscosity with C_beta 1.75."""
     from shock_turbulence_b200 import Solver
-    p = default_params(*grid, re=100.0, rk_mode=0, c_beta_scale=1.75)
+    p = default_params(*grid, re=100.0, rk_mode=rk, c_beta_scale=1.75)
     s, o = Solver(p), oracle_mod.Oracle(p)
     Q, Y = mf_state(p, seed=11, p_ratio=p_ratio)
     for h in (s, o):
