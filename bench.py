@@ -132,6 +132,17 @@ def oracle_rate(n, steps, warm, threads):
     return n ** 3 * steps / el / 1e6, el
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the baseline record."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def single_core_rate(n=64, steps=2):
     """The CPU oracle on one host thread: a 64^3 sample of the same workload,
     1 warm-up + 2 timed steps (about 15 s)."""
@@ -169,7 +180,8 @@ def run_reference(args, rank):
         "data": "synthetic (seeded blast-in-turbulence)",
         "config": {"workload": f"blast wave in isotropic turbulence, octant, sample {n}^3 of 384^3",
                    "grid": n, "parallelism": "host OpenMP"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -286,7 +298,7 @@ def run_radial(args, rank, world, local, dist):
         rate, el, pts = radial_oracle_rate(512, 10, threads, seed=3)
         cpu = {"value": rate, "unit": RAD_UNIT, "cores": threads, "kind": "port",
                "sample": f"CPU oracle, 512 problems of the same distribution ({pts} points), 1 warm-up + 10 timed "
-                         f"steps ({el:.1f} s), {threads} OpenMP threads"}
+                         f"steps ({el:.1f} s), {threads} OpenMP threads", "cpu_model": cpu_model()}
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = float(json.load(open(peaks_path))["hbm_gbs"]) if os.path.exists(peaks_path) else 6650.0
     alg = RAD_OPS * 16.0 * npts * args.steps          # every line operator: one field in, one out
@@ -301,7 +313,8 @@ def run_radial(args, rank, world, local, dist):
                        "points": npts, "kernel_config": {"short": cfg[0], "long": cfg[1]},
                        "tune_ms": tune_ms, "parallelism": f"replicas x{world}",
                        "l2": "state 207 MB per field set, larger than L2", "finite": finite,
-                       "steps_done_min": int(st.min())},
+                       "steps_done_min": int(st.min()),
+                       "rk_stages_per_step": 11, "mpoint_stages_per_s": value * 11},
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_rad_steps", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -772,6 +785,7 @@ def main():
                "sample": f"CPU oracle, {args.cpu_n}^3 sample of the same workload, 1 warm-up + 3 timed steps "
                          f"({el:.1f} s), {threads} OpenMP threads"}
         cpu["single_core"] = single_core_rate()
+        cpu["cpu_model"] = cpu_model()
 
     ext = None
     if want_ext:
@@ -791,7 +805,9 @@ def main():
                                    "physics (Y=1), Re=100 viscous term on, artificial viscosity on, CFL 0.5",
                        "grid": args.n, "cells": cells, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (one field is %.0f MB)" % (cells * 8 / 1e6),
-                       "finite": finite},
+                       "finite": finite,
+                       # stages per step differ between the families (10 here, 11 for the sf ones)
+                       "rk_stages_per_step": 10, "mcell_stages_per_s": value * 10},
             "e2e": ({"value": e2e, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
                      "steps": args.e2e_steps} if e2e is not None else None),
             "gpu_launches": int(c1.value - c0.value),
