@@ -38,6 +38,12 @@ def make_params(n, device=0, precision=0):
                           c_beta_scale=1.75, device=device, precision=precision)
 
 
+# Interface bytes per cell and RK stage of the reference's operator graph for
+# the _mf blast step (Re > 0, artificial viscosity on): DF*/D2F*2 at 16 or 24
+# B, filter and Gaussian passes at 16 B, the stage update at 40 B per
+# variable.  Counted by the instrumented CPU oracle; tests/test_graph_bytes.py
+# keeps this figure equal to that count.
+GRAPH_BYTES_PER_CELL_STAGE = 2848.0
 METRIC_FP32 = "Mcell-steps/s (FP32-mode RHS+LDDRK4 step, 10 RK stages/step)"
 
 
@@ -773,6 +779,17 @@ def main():
                             "bytes_per_step": step_bytes / args.steps,
                             "kernel_ms_per_step": step_ms_all / args.steps,
                             "bytes_per_cell_per_stage": step_bytes / args.steps / cells / 10}
+    if not fp32:
+        # the reference's operator graph (derivative, filter and Gaussian
+        # passes and stage updates at their interface bytes; pointwise passes
+        # not counted) moved in the measured step time: how near the step is
+        # to the bound an ideal fusion of this graph would have
+        g_bytes = GRAPH_BYTES_PER_CELL_STAGE * 10 * cells
+        g_gbs = g_bytes / (ms / args.steps / 1e3) / 1e9
+        roofline["graph"] = {"bytes_per_cell_per_stage": GRAPH_BYTES_PER_CELL_STAGE, "bytes_per_step": g_bytes,
+                             "achieved": g_gbs, "frac": g_gbs / peak,
+                             "basis": "interface bytes of the reference operator calls of one step (count of the "
+                                      "instrumented CPU oracle, tests/test_graph_bytes.py) / ms_per_step"}
     for k, v in prof.items():
         if v["bytes"] and v["ms"]:
             roofline["kernels"][k]["frac"] = round(v["bytes"] / (v["ms"] / 1e3) / 1e9 / peak, 3)

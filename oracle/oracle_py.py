@@ -67,6 +67,9 @@ def _load():
     lib.orc_compute_srm_stats.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
     lib.orc_shock_surface.argtypes = [ctypes.c_void_p, _dp, _dp]
     lib.orc_make_padded_arrays.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+    lib.orc_graph_bytes.restype = ctypes.c_double
+    lib.orc_graph_bytes.argtypes = []
+    lib.orc_graph_bytes_reset.argtypes = []
     rp = ctypes.POINTER(StRadialParams)
     ci, cd = ctypes.c_int, ctypes.c_double
     lib.orc_rad_radius.argtypes = [ci, cd, _dp]
@@ -101,6 +104,15 @@ def _p(a):
         return None
     assert a.dtype == np.float64 and a.flags.c_contiguous, "oracle needs C-contiguous float64"
     return a.ctypes.data_as(_dp)
+
+
+def graph_bytes(reset=False):
+    """Interface bytes of the reference operator calls made since the last
+    reset (DF*, D2F*2, filter and Gaussian passes, stage updates)."""
+    v = lib().orc_graph_bytes()
+    if reset:
+        lib().orc_graph_bytes_reset()
+    return v
 
 
 def set_threads(n):

@@ -484,11 +484,28 @@ static void per_line_op(orc *c, int d, int kind, const double *F, double *O, int
     }
 }
 
+/* ---- operator-graph byte count ------------------------------------------- */
+/* Interface bytes of the reference's operator graph, counted as its operator
+ * calls happen (test infrastructure: the per-cell figure a GPU step is
+ * compared with).  Per call and cell: DF* 16 B (read F, write dF), 24 B with
+ * iadd (dF read too); D2F*2 16 B, 24 B with iadd (dF written as well, the
+ * nested DF* call not counted again); one compact or Gaussian filter pass
+ * 16 B; the LDDRK4 stage update 40 B per variable (read Q, QW, dQ; write Q,
+ * QW).  Pointwise passes are not part of the graph. */
+static double g_graph_bytes = 0.0;
+static int g_graph_nested = 0;
+void orc_graph_bytes_reset(void) { g_graph_bytes = 0.0; }
+double orc_graph_bytes(void) { return g_graph_bytes; }
+static void graph_count(const orc *c, double per_cell) {
+    if (!g_graph_nested) g_graph_bytes += per_cell * (double)c->n3;
+}
+
 /* ---- derivatives ---------------------------------------------------------- */
 /* DFDX_sym src/derivCDopt6_sym_tri.f:409-535 / DFDX_asym
  * src/derivCDopt6_asym_tri.f:412-537 and their y/z twins (the one-rank
  * branches xrank==0 and xrank==Px-1 both apply). */
 void orc_dfd(orc *c, int d, int asym, const double *F, double *dF, int iadd, double cadd) {
+    graph_count(c, iadd ? 24.0 : 16.0);
     if (is_per(c)) { per_line_op(c, d, PER_D1, F, dF, iadd, cadd); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
@@ -527,7 +544,15 @@ void orc_dfd(orc *c, int d, int asym, const double *F, double *dF, int iadd, dou
 
 /* D2FDX2_sym src/derivCDopt6_sym_tri.f:538-669 / D2FDX2_asym
  * src/derivCDopt6_asym_tri.f:540-667 and y/z twins */
+static void orc_d2fd2_body(orc *c, int d, int asym, const double *F, double *dF, double *d2F, int iadd);
 void orc_d2fd2(orc *c, int d, int asym, const double *F, double *dF, double *d2F, int iadd) {
+    graph_count(c, iadd == 1 ? 24.0 : 16.0);
+    g_graph_nested++;
+    orc_d2fd2_body(c, d, asym, F, dF, d2F, iadd);
+    g_graph_nested--;
+}
+
+static void orc_d2fd2_body(orc *c, int d, int asym, const double *F, double *dF, double *d2F, int iadd) {
     if (is_per(c)) {
         /* D2FDX2 src/derivCDopt6_periodic.f:270-392: dF by DFDX when iadd = 1 */
         if (iadd == 1) per_line_op(c, d, PER_D1, F, dF, 0, 1.0);
@@ -573,6 +598,7 @@ void orc_d2fd2(orc *c, int d, int asym, const double *F, double *dF, double *d2F
 /* Compact_Filter_X_sym src/filters_sym.f:436-634 / Compact_Filter_X_asym
  * src/filters_asym.f:388-583 and y/z twins */
 void orc_filter(orc *c, int d, int asym, const double *F, double *F0) {
+    graph_count(c, 16.0);
     if (is_per(c)) { per_line_op(c, d, PER_FILT, F, F0, 0, 1.0); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
@@ -637,6 +663,7 @@ void orc_compact_filter(orc *c, const double *F, double *F0, int nvar) {
 
 /* Gaussian_Filter_X src/filters_sym.f:1076-1219 and Y/Z :1222-1554 */
 void orc_gauss(orc *c, int d, const double *F, double *Fg) {
+    graph_count(c, 16.0);
     if (is_per(c)) { per_line_op(c, d, PER_GAUSS, F, Fg, 0, 1.0); return; }
     int n; size_t st, lot;
     line_geom(c, d, &n, &st, &lot);
@@ -1810,6 +1837,7 @@ static void lddrk4_sf(orc *c, double *time, int *step) {
             else { al = 0.0; be = 0.0; }
             orc_rhs(c, Q, dQ, c->Y);
             orc_hyper_rhs(c, Q, dQ, c->Y);
+            graph_count(c, 5 * 40.0);
             PAR for (size_t q = 0; q < 5 * n3; q++) QW[q] = al * QW[q] + dt * dQ[q];
             PAR for (size_t q = 0; q < 5 * n3; q++) Q[q] = Q[q] + be * QW[q];
             orc_compact_filter(c, Q, Qf, 5);
@@ -1845,6 +1873,7 @@ void orc_lddrk4(orc *c, double *time, int *step) {
             orc_bc_rhs(c, Q, dQ, Y, drYi, tstage);
             orc_sponge_forcing(c, Q, dQ, Y, drYi);
             PAR FOR_P rY[p] = Q[3 * n3 + p] * Y[p];
+            graph_count(c, 6 * 40.0);       /* Q (5 fields) and rY */
             PAR for (size_t q = 0; q < 5 * n3; q++) QW[q] = al * QW[q] + dt * dQ[q];
             PAR for (size_t q = 0; q < 5 * n3; q++) Q[q] = Q[q] + be * QW[q];
             PAR FOR_P rYW[p] = al * rYW[p] + dt * drYi[p];

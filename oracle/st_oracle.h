@@ -72,6 +72,8 @@ void orc_compute_grad(orc *c, double *Grad, double *maxdil, double *enstrophy);
 int  orc_shell_count(const orc *c);
 void orc_compute_srm_stats(orc *c, double *hmix, double *tke_total, double *ur_avg, double *y_avg);
 void orc_shock_surface(orc *c, double *rad_avg, double *rad_skew_rms);
+void orc_graph_bytes_reset(void);
+double orc_graph_bytes(void);
 void orc_make_padded_arrays(orc *c, const double *Grad, double *W, double *xx, double *yy, double *zz);
 
 /* 1-D spherical-radial family (st_oracle_radial.c).  Q = (u_r, rho, s)
