@@ -245,6 +245,18 @@ inline bool fp32_mode(const st_ctx *c) { return c->p.precision == ST_PRECISION_F
 // line operators on device arrays (st_kernels.cu)
 int dev_dfd(st_ctx *c, int dir, int asym, const double *F, double *dF, int iadd, double cadd);
 int dev_dfd_prod(st_ctx *c, int dir, int asym, const Prod &F, double *dF, int iadd, double cadd);
+// two first derivatives along one direction (DFD*_sym/_asym with iadd and
+// cadd each), in order, one launch when the second operand set contains the
+// first
+template <class T>
+struct D1SpecT {
+    ProdT<T> F;
+    T *dF;
+    int asym, iadd;
+    double cadd;
+};
+int dev_dfd_pair(st_ctx *c, int dir, const D1SpecT<double> *ops);
+int dev_dfd_pair_f(st_ctx *c, int dir, const D1SpecT<float> *ops);
 // FP32-field variants (FP32 mode): same operators, float inputs and outputs
 int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd, double cadd);
 int dev_dfd_prod_f(st_ctx *c, int dir, int asym, const ProdF &F, float *dF, int iadd, double cadd);

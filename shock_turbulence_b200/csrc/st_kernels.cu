@@ -120,6 +120,55 @@ int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd,
     return dev_dfd_prod_f(c, dir, asym, plain_f(F), dF, iadd, cadd);
 }
 
+// ---- two first derivatives along one direction, one launch ---------------------
+int launch_pair_f32(st_ctx *c, const D1PairT<float> &g, double bytes);
+
+// Producers (a, a*b), (a*b, c*(a*b)) or (species flux, its energy
+// counterpart) of the bounded lines run as one launch (the second operand set
+// contains the first); the periodic family and any other pair run as two
+// launches, with the same results.
+template <class T>
+static int dfd_pair_t(st_ctx *c, int dir, const D1SpecT<T> *ops) {
+    const int o0 = ops[0].F.op, o1 = ops[1].F.op;
+    const ProdT<T> &f0 = ops[0].F, &f1 = ops[1].F;
+    bool fuse = c->p.family != ST_FAMILY_PERIODIC &&
+                ((o0 == PR_A && o1 == PR_MUL && f1.b == f0.a) ||
+                 (o0 == PR_MUL && o1 == PR_MULMUL && f1.a == f0.a && f1.b == f0.b) ||
+                 (o0 == PR_SPEC && o1 == PR_SPECT && f1.a == f0.a && f1.b == f0.b && f1.c == f0.c &&
+                  f1.k0 == f0.k0 && f1.k1 == f0.k1));
+    if (!fuse) {
+        for (int i = 0; i < 2; i++) {
+            if constexpr (sizeof(T) == 8)
+                ST_TRY(dev_dfd_prod(c, dir, ops[i].asym, ops[i].F, ops[i].dF, ops[i].iadd, ops[i].cadd));
+            else
+                ST_TRY(dev_dfd_prod_f(c, dir, ops[i].asym, ops[i].F, ops[i].dF, ops[i].iadd, ops[i].cadd));
+        }
+        return ST_OK;
+    }
+    D1PairT<T> g{};
+    g.a = make_args<T>(c, dir);
+    for (int i = 0; i < 2; i++) {
+        const D1SpecT<T> &o = ops[i];
+        if constexpr (sizeof(T) == 4) ST_TRY(check_f2(c, o.F, o.dF, nullptr));
+        D1OpT<T> &d = g.op[i];
+        d.F = o.F; d.O1 = o.dF; d.asym = o.asym; d.iadd = o.iadd;
+        d.fac1 = o.cadd * c->s1[dir] * (double)(g.a.geo.n - 1);           // src/derivCDopt6_sym_tri.f:424
+        if constexpr (sizeof(T) == 8) d.t1 = c->tri[dir][o.asym ? K_D1A : K_D1S];
+        else d.t1 = c->trif[dir][o.asym ? K_D1A : K_D1S];
+    }
+    // algorithmic bytes per cell: the second operation's operands (they
+    // contain the first's), each accumulated output read, each output written
+    const double nin = o1 == PR_MUL ? 2.0 : o1 == PR_MULMUL ? 3.0 : 4.0;
+    const double nacc = (double)(ops[0].iadd + ops[1].iadd);
+    const double nout = ops[0].dF == ops[1].dF ? 1.0 : 2.0;
+    const double bytes = (double)sizeof(T) * (nin + nacc + nout);
+    if constexpr (sizeof(T) == 8) return launch_pair_t<double>(c, g, bytes);
+    else return launch_pair_f32(c, g, bytes);
+}
+
+int dev_dfd_pair(st_ctx *c, int dir, const D1SpecT<double> *ops) { return dfd_pair_t(c, dir, ops); }
+int dev_dfd_pair_f(st_ctx *c, int dir, const D1SpecT<float> *ops) { return dfd_pair_t(c, dir, ops); }
+
 int dev_d2fd2_f(st_ctx *c, int dir, int asym, const float *F, float *dF, float *d2F, int iadd) {
     LineArgsF a = make_args<float>(c, dir);
     a.F = plain_f(F); a.O1 = dF; a.O2 = d2F; a.asym = asym; a.iadd = iadd;

@@ -6,5 +6,6 @@
 namespace st {
 
 int launch_line_f32(st_ctx *c, OpKind op, const LineArgsF &a) { return launch_line_t<false, float>(c, op, a); }
+int launch_pair_f32(st_ctx *c, const D1PairT<float> &g, double bytes) { return launch_pair_t<float>(c, g, bytes); }
 
 }  // namespace st

@@ -54,16 +54,16 @@ constexpr unsigned kAhead = kLineCtasPerSm * 148;
 __device__ __forceinline__ void pf_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 template <int S, bool YT, int OP, class T>
-__device__ __forceinline__ void prefetch_next(const LineArgsT<T> &a, int lane, int row0) {
+__device__ __forceinline__ void prefetch_next(const LineGeo &geo, const ProdT<T> &F, int lane, int row0) {
     const unsigned nb = blockIdx.x + kAhead;
     if (nb >= gridDim.x) return;
     constexpr int W = Val<T>::W;
     constexpr int NI = OP == PR_A ? 1 : OP == PR_MUL ? 2 : OP == PR_SPECT ? 4 : 3;   // fields the producer reads
-    const ColMap m = a.geo.template map<W>(nb);
-    const T *f[4] = {a.F.a, a.F.b, a.F.c, a.F.d};
+    const ColMap m = geo.template map<W>(nb);
+    const T *f[4] = {F.a, F.b, F.c, F.d};
     if (YT) {
         // the block's lines are one contiguous range: one 128-byte line per thread and pass
-        const size_t bytes = (size_t)kLanes * W * a.geo.n * sizeof(T);
+        const size_t bytes = (size_t)kLanes * W * geo.n * sizeof(T);
         for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)
 #pragma unroll
             for (int k = 0; k < NI; k++) pf_l2(reinterpret_cast<const char *>(f[k] + m.base) + off);
@@ -102,10 +102,10 @@ __device__ __forceinline__ void put_rows(const V (&v)[N], A *tile, T *O, const C
 template <int S, bool YT, int OP, bool CYC, class T>
 __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_dfd(LineArgsT<T> a) {
     LINE_PROLOGUE
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0); __syncthreads(); }
     V v[S + 4];
     get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
-    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
+    if (!YT) prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0);
     rhs_d1<S, 2>(v, row0, n, a.asym, CYC, a.fac1, a.K, rd);
     tri_solve<S>(v, a.t1, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t1.cyc, s, a.P, lane, cb);
@@ -120,10 +120,10 @@ __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_d2fd2(LineArgs
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     {
-        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
+        if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0); __syncthreads(); }
         V v[S + 4];
         get_rows<S, 2, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
-        if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
+        if (!YT) prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0);
         rhs_d2<S, 2>(v, row0, n, a.asym, CYC, a.fac2, a.K, rd);
         tri_solve<S>(v, a.t2, s, a.P, lane, cb);
         if constexpr (CYC) cyc_fix<S, S + 4, 2>(v, a.t2.cyc, s, a.P, lane, cb);
@@ -149,10 +149,10 @@ template <int S, bool YT, bool CYC, class T>
 __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_filter(LineArgsT<T> a) {
     constexpr int OP = PR_A;
     LINE_PROLOGUE
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0); __syncthreads(); }
     double v[S + 8];
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
-    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
+    if (!YT) prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0);
     rhs_filter<S, 4>(v, row0, n, a.asym, CYC, a.K, rd);
     pen_solve<S>(v, a.p, s, a.P, lane, cb);
     if constexpr (CYC) cyc_fix<S, S + 8, 4>(v, a.p.cyc, s, a.P, lane, cb);
@@ -166,12 +166,87 @@ __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_gauss(LineArgs
     constexpr int OP = PR_A;
     LINE_PROLOGUE
     (void)cb;
-    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a, lane, row0); __syncthreads(); }
+    if (YT) { ytile_load<OP>(tile, a.F, m.base, n); prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0); __syncthreads(); }
     V v[S + 8];
     get_rows<S, 4, YT, OP>(v, tile, a.F, m, lane, row0, n, CYC);
-    if (!YT) prefetch_next<S, YT, OP>(a, lane, row0);
+    if (!YT) prefetch_next<S, YT, OP>(a.geo, a.F, lane, row0);
     rhs_gauss<S, 4>(v, row0, n, CYC, a.K, rd);
     put_rows<S, YT, false>(v, tile, a.O1, m, lane, row0, n, 0);
+}
+
+// ---- two first derivatives along one direction in one launch ------------
+// Hyper_RHS (src/hyper_rhs_sym_mf.f) differentiates, in each direction, a
+// viscous flux and then its product with a velocity component (v_h S_12 and
+// then v_h S_12 u, or tau_xx and then u tau_xx); Species_RHS
+// (src/species_rhs_sym.f) the diffusive flux of Y and then its energy
+// counterpart, and Y and then rho u_i Y.  The second operand set contains
+// the first, so one CTA runs both on its own lines: the second
+// operation finds the shared rows in L2, as the first derivative of
+// D2F*2 with iadd does.  Each operation is exactly the k_dfd of its
+// arguments, so the results are bitwise those of two launches.
+template <class T>
+struct D1OpT {
+    ProdT<T> F;
+    T *O1;
+    double fac1;
+    int asym, iadd;
+    TriTabT<T> t1;
+};
+template <class T>
+struct D1PairT {
+    LineArgsT<T> a;      // geometry, segmentation and scheme constants (its F, O1, t1 unused)
+    D1OpT<T> op[2];
+};
+
+// block and thread index read so that the compiler keeps nothing derived
+// from them live from the first operation to the second
+__device__ __forceinline__ unsigned opaque_ctaid() {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(v));
+    return v;
+}
+__device__ __forceinline__ unsigned opaque_tid() {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(v));
+    return v;
+}
+
+// one operation; PF: the L2 prefetch of the next wave's rows of the first
+// operation (OPF, producer FN), issued with the second operation
+template <int S, bool YT, int OP, bool PF, int OPF, class T>
+__device__ __forceinline__ void pair_d1(const LineArgsT<T> &a, const D1OpT<T> &o, const ProdT<T> &FN,
+                                        CarryBufT<typename Val<T>::V> &cb, typename Val<T>::A *tile) {
+    using V = typename Val<T>::V;
+    constexpr int W = Val<T>::W;
+    const unsigned tid = opaque_tid();
+    const int lane = tid & (kLanes - 1), s = tid / kLanes, row0 = s * S, n = a.geo.n;
+    const ColMap m = a.geo.template map<W>(opaque_ctaid());
+    const RowReader<OP, T, V> rd = YT ? RowReader<OP, T, V>{tile + W * lane * (n + 1), nullptr, 0, 0, n + 1}
+                                      : RowReader<OP, T, V>{nullptr, &o.F, m.base + (size_t)lane * W * m.lstride,
+                                                            m.rstride, 0};
+    if (YT) {
+        ytile_load<OP>(tile, o.F, m.base, n);
+        if (PF) prefetch_next<S, YT, OPF>(a.geo, FN, lane, row0);
+        __syncthreads();
+    }
+    V v[S + 4];
+    get_rows<S, 2, YT, OP>(v, tile, o.F, m, lane, row0, n, 0);
+    if (!YT && PF) prefetch_next<S, YT, OPF>(a.geo, FN, lane, row0);
+    rhs_d1<S, 2>(v, row0, n, o.asym, 0, o.fac1, a.K, rd);
+    tri_solve<S>(v, o.t1, s, a.P, lane, cb);
+    put_rows<S, YT, true>(v, tile, o.O1, m, lane, row0, n, o.iadd);
+}
+
+template <int S, bool YT, class T, int OP0, int OP1>
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_dfd_pair(D1PairT<T> g) {
+    using V = typename Val<T>::V;
+    using A = typename Val<T>::A;
+    __shared__ CarryBufT<V> cb;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A *tile = reinterpret_cast<A *>(smem_raw);
+    pair_d1<S, YT, OP0, false, OP0>(g.a, g.op[0], g.op[0].F, cb, tile);
+    __syncthreads();                     // tile and carry buffers are reused
+    pair_d1<S, YT, OP1, true, OP0>(g.a, g.op[1], g.op[0].F, cb, tile);
 }
 
 enum OpKind { OP_D1, OP_D2, OP_FILTER, OP_GAUSS };
@@ -245,6 +320,47 @@ static int launch_line_t(st_ctx *c, OpKind op, const LineArgsT<T> &a) {
     return ST_OK;
 }
 
+
+// one launch of a pair (bounded lines): producers (a, a*b), (a*b, c*(a*b))
+// or the species flux and its energy counterpart;
+// bytes: algorithmic bytes per cell (every distinct field read or written once)
+template <int S, bool YT, class T, int OP0, int OP1>
+static void launch_pair_SY(st_ctx *c, const D1PairT<T> &g0, double bytes, cudaStream_t st) {
+    const size_t nlines = c->dm.n3 / (size_t)g0.a.geo.n;   // lines of one case
+    constexpr int NL = kLanes * Val<T>::W;
+    D1PairT<T> g = g0;
+    g.a.geo.cblk = (unsigned)(nlines / NL);                  // CTAs per case
+    g.a.geo.cstride = c->dm.n3;
+    dim3 grid(g.a.geo.cblk * (unsigned)c->na), block(kLanes * g.a.P);
+    const size_t smem = YT ? (size_t)NL * (g.a.geo.n + 1) * sizeof(T) : 0;
+    int pi = prof_start(c, "k_dfd_pair", bytes * (double)c->ncell());
+    set_smem<k_dfd_pair<S, YT, T, OP0, OP1>>(smem);
+    k_dfd_pair<S, YT, T, OP0, OP1><<<grid, block, smem, st>>>(g);
+    prof_stop(c, pi);
+}
+
+template <int S, bool YT, class T>
+static void launch_pair_SYT(st_ctx *c, const D1PairT<T> &g, double bytes) {
+    if (g.op[0].F.op == PR_A) launch_pair_SY<S, YT, T, PR_A, PR_MUL>(c, g, bytes, c->stream);
+    else if (g.op[0].F.op == PR_MUL) launch_pair_SY<S, YT, T, PR_MUL, PR_MULMUL>(c, g, bytes, c->stream);
+    else launch_pair_SY<S, YT, T, PR_SPEC, PR_SPECT>(c, g, bytes, c->stream);
+}
+
+template <class T>
+static int launch_pair_t(st_ctx *c, const D1PairT<T> &g, double bytes) {
+    switch (g.a.S) {
+#define CASE(s_)                                                       \
+    case s_:                                                           \
+        if (g.a.geo.dir == 1) launch_pair_SYT<s_, true, T>(c, g, bytes); \
+        else launch_pair_SYT<s_, false, T>(c, g, bytes);                 \
+        break;
+        CASE(2) CASE(3) CASE(4) CASE(6) CASE(8) CASE(12) CASE(16)
+#undef CASE
+        default: return fail(c, ST_E_UNSUPPORTED, "unsupported line segmentation");
+    }
+    ST_CUDA(c, cudaGetLastError());
+    return ST_OK;
+}
 
 // launches of the other instantiations, each in its own translation unit:
 // periodic lines (st_kernels_cyc.cu), FP32 fields (st_kernels_f32.cu) and

@@ -44,6 +44,8 @@ static constexpr double io(const P *...) { return (0.0 + ... + (double)sizeof(P)
 
 // producer expressions evaluated by the derivative kernels while loading
 template <class R>
+static ProdT<R> pr_one(const R *a) { ProdT<R> p{}; p.op = PR_A; p.a = a; return p; }
+template <class R>
 static ProdT<R> pr_mul(const R *a, const R *b) { ProdT<R> p{}; p.op = PR_MUL; p.a = a; p.b = b; return p; }
 template <class R>
 static ProdT<R> pr_addmul(const R *a, const R *b, const R *c) {
@@ -88,6 +90,15 @@ static int d2fd2_sum(st_ctx *c, int dir, int asym, const double *F, double *d2F,
 static int d2fd2_sum(st_ctx *c, int dir, int asym, const float *F, float *d2F, const float *E1,
                      const float *E2) {
     return dev_d2fd2_sum_f(c, dir, asym, F, d2F, E1, E2);
+}
+// two first derivatives of one direction in order (D1SpecT: producer, output,
+// asym, iadd, cadd), one launch when the second reads what the first reads
+template <class R>
+static int dfd_pair(st_ctx *c, int dir, ProdT<R> F0, R *O0, int asym0, int iadd0, ProdT<R> F1, R *O1, int asym1,
+                    int iadd1) {
+    const D1SpecT<R> ops[2] = {{F0, O0, asym0, iadd0, 1.0}, {F1, O1, asym1, iadd1, 1.0}};
+    if constexpr (sizeof(R) == 8) return dev_dfd_pair(c, dir, ops);
+    else return dev_dfd_pair_f(c, dir, ops);
 }
 static int gauss(st_ctx *c, int dir, const double *F, double *Fg) { return dev_gauss(c, dir, F, Fg); }
 static int gauss(st_ctx *c, int dir, const float *F, float *Fg) { return dev_gauss_f(c, dir, F, Fg); }
@@ -644,27 +655,21 @@ static int hyper_rhs_t(st_ctx *c, const double *Q, R *Qrhs, const double *Y, con
         Flux2[p] = 2.0 * vh[p] * G4[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p];
     });
     // x momentum: Qh1 = dFx + dFy + dFz, Qh5 = dEx + dEy + dEz
-    ST_TRY(dfd(c, 0, 0, Flux, h1, 0, 1.0));
-    ST_TRY(dfd(c, 0, 1, pr_mul(U1, Flux), h5, 0, 1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mul(vh, S1), h1, 1, 1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mulmul(vh, S1, U1), h5, 1, 1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mul(vh, S2), h1, 1, 1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S2, U1), h5, 1, 1.0));
+    // (each line pair: a flux and its product with a velocity component, the
+    // second reading what the first reads; one launch per pair)
+    const R *cF = Flux, *cF2 = Flux2;
+    ST_TRY(dfd_pair<R>(c, 0, pr_one(cF), h1, 0, 0, pr_mul(U1, cF), h5, 1, 0));
+    ST_TRY(dfd_pair<R>(c, 1, pr_mul(vh, S1), h1, 1, 1, pr_mulmul(vh, S1, U1), h5, 1, 1));
+    ST_TRY(dfd_pair<R>(c, 2, pr_mul(vh, S2), h1, 1, 1, pr_mulmul(vh, S2, U1), h5, 1, 1));
     // y momentum (x, y, z accumulation order)
-    ST_TRY(dfd(c, 0, 1, pr_mul(vh, S1), h2, 0, 1.0));
-    ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S1, U2), h5, 1, 1.0));
-    ST_TRY(dfd(c, 1, 0, Flux2, h2, 1, 1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mul(U2, Flux2), h5, 1, 1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mul(vh, S3), h2, 1, 1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mulmul(vh, S3, U2), h5, 1, 1.0));
+    ST_TRY(dfd_pair<R>(c, 0, pr_mul(vh, S1), h2, 1, 0, pr_mulmul(vh, S1, U2), h5, 1, 1));
+    ST_TRY(dfd_pair<R>(c, 1, pr_one(cF2), h2, 0, 1, pr_mul(U2, cF2), h5, 1, 1));
+    ST_TRY(dfd_pair<R>(c, 2, pr_mul(vh, S3), h2, 1, 1, pr_mulmul(vh, S3, U2), h5, 1, 1));
     // z momentum
     PFOR(c, nc, io(vh, G8, bh, dila, Flux), { Flux[p] = 2.0 * vh[p] * G8[p] + (bh[p] - (2.0 / 3.0) * vh[p]) * dila[p]; });
-    ST_TRY(dfd(c, 0, 1, pr_mul(vh, S2), h3, 0, 1.0));
-    ST_TRY(dfd(c, 0, 1, pr_mulmul(vh, S2, U3), h5, 1, 1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mul(vh, S3), h3, 1, 1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mulmul(vh, S3, U3), h5, 1, 1.0));
-    ST_TRY(dfd(c, 2, 0, Flux, h3, 1, 1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mul(U3, Flux), h5, 1, 1.0));
+    ST_TRY(dfd_pair<R>(c, 0, pr_mul(vh, S2), h3, 1, 0, pr_mulmul(vh, S2, U3), h5, 1, 1));
+    ST_TRY(dfd_pair<R>(c, 1, pr_mul(vh, S3), h3, 1, 1, pr_mulmul(vh, S3, U3), h5, 1, 1));
+    ST_TRY(dfd_pair<R>(c, 2, pr_one(cF), h3, 0, 1, pr_mul(U3, cF), h5, 1, 1));
     // artificial heat flux
     ST_TRY(dfd(c, 0, 0, pr_mul(kh, GTx), h5, 1, 1.0));
     ST_TRY(dfd(c, 1, 0, pr_mul(kh, GTy), h5, 1, 1.0));
@@ -697,20 +702,22 @@ static int species_rhs_t(st_ctx *c, const double *Q, const R *Qr, R *Qrhs, const
         thermo(f, g[p], Y[p], Q1[p], Q2[p], Q3[p], Q4[p], Q5[p], Vs, P, Tt);
         T[p] = Tt;
     });
-    ST_TRY(dfd(c, 0, 0, Yr, dYd[0], 0, 1.0));
-    ST_TRY(dfd(c, 1, 0, Yr, dYd[1], 0, 1.0));
-    ST_TRY(dfd(c, 2, 0, Yr, dYd[2], 0, 1.0));
-    ST_TRY(dfd(c, 0, 1, pr_mul(q1r, Yr), Yrhs, 0, -1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mul(q2r, Yr), Yrhs, 1, -1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mul(q3r, Yr), Yrhs, 1, -1.0));
+    // dY/dx_i and d(rho u_i Y)/dx_i per direction, one launch each (the
+    // gradient and the flux are independent; the flux keeps its x, y, z order)
+    const R *qr[3] = {q1r, q2r, q3r};
+    for (int d = 0; d < 3; d++) {
+        const D1SpecT<R> ops[2] = {{pr_one(Yr), dYd[d], 0, 0, 1.0},
+                                   {pr_mul(qr[d], Yr), Yrhs, 1, d == 0 ? 0 : 1, -1.0}};
+        if constexpr (sizeof(R) == 8) ST_TRY(dev_dfd_pair(c, d, ops));
+        else ST_TRY(dev_dfd_pair_f(c, d, ops));
+    }
     const double cst = 1.0 - f.eps * f.g2 * (f.g1 - 1.0) / (f.g1 * (f.g2 - 1.0));
     for (int d = 0; d < 3; d++) {
         ProdT<R> fl{};
         fl.op = PR_SPEC; fl.a = q4r; fl.b = Dh; fl.c = dYd[d]; fl.k0 = f.Re1_inv; fl.k1 = f.Sc_inv;
         ProdT<R> ft = fl;
         ft.op = PR_SPECT; ft.d = T; ft.k2 = cst;
-        ST_TRY(dfd(c, d, 1, fl, Yd, d == 0 ? 0 : 1, 1.0));
-        ST_TRY(dfd(c, d, 1, ft, Qrhs + 4 * n3, 1, 1.0));
+        ST_TRY(dfd_pair<R>(c, d, fl, Yd, 1, d == 0 ? 0 : 1, ft, Qrhs + 4 * n3, 1, 1));
     }
     PFOR(c, nc, io(Yrhs, Yrhs, Yd), { Yrhs[p] = Yrhs[p] + Yd[p]; });
     return ST_OK;
