@@ -123,19 +123,14 @@ int dev_dfd_f(st_ctx *c, int dir, int asym, const float *F, float *dF, int iadd,
 // ---- two first derivatives along one direction, one launch ---------------------
 int launch_pair_f32(st_ctx *c, const D1PairT<float> &g, double bytes);
 
-// Producers (a, a*b), (a*b, c*(a*b)) or (species flux, its energy
-// counterpart) of the bounded lines run as one launch (the second operand set
-// contains the first); the periodic family and any other pair run as two
-// launches, with the same results.
+// Two first derivatives of the bounded lines whose producers form a compiled
+// pair (kPairOps) run as one launch, in order; the periodic family and any
+// other pair run as two launches, with the same results.  The callers pair
+// operations that share fields (the second reads what the first reads, or
+// adds to what it wrote), which is where one launch saves DRAM traffic.
 template <class T>
 static int dfd_pair_t(st_ctx *c, int dir, const D1SpecT<T> *ops) {
-    const int o0 = ops[0].F.op, o1 = ops[1].F.op;
-    const ProdT<T> &f0 = ops[0].F, &f1 = ops[1].F;
-    bool fuse = c->p.family != ST_FAMILY_PERIODIC &&
-                ((o0 == PR_A && o1 == PR_MUL && f1.b == f0.a) ||
-                 (o0 == PR_MUL && o1 == PR_MULMUL && f1.a == f0.a && f1.b == f0.b) ||
-                 (o0 == PR_SPEC && o1 == PR_SPECT && f1.a == f0.a && f1.b == f0.b && f1.c == f0.c &&
-                  f1.k0 == f0.k0 && f1.k1 == f0.k1));
+    const bool fuse = c->p.family != ST_FAMILY_PERIODIC && pair_kind(ops[0].F.op, ops[1].F.op) >= 0;
     if (!fuse) {
         for (int i = 0; i < 2; i++) {
             if constexpr (sizeof(T) == 8)
@@ -147,6 +142,14 @@ static int dfd_pair_t(st_ctx *c, int dir, const D1SpecT<T> *ops) {
     }
     D1PairT<T> g{};
     g.a = make_args<T>(c, dir);
+    // algorithmic bytes per cell: each distinct field once (the producers'
+    // operands and accumulated outputs read, the outputs written)
+    const void *rd[10], *wr[2];
+    int nr = 0, nw = 0;
+    auto add_once = [](const void **v, int &n, const void *p) {
+        for (int k = 0; k < n; k++) if (v[k] == p) return;
+        v[n++] = p;
+    };
     for (int i = 0; i < 2; i++) {
         const D1SpecT<T> &o = ops[i];
         if constexpr (sizeof(T) == 4) ST_TRY(check_f2(c, o.F, o.dF, nullptr));
@@ -155,13 +158,14 @@ static int dfd_pair_t(st_ctx *c, int dir, const D1SpecT<T> *ops) {
         d.fac1 = o.cadd * c->s1[dir] * (double)(g.a.geo.n - 1);           // src/derivCDopt6_sym_tri.f:424
         if constexpr (sizeof(T) == 8) d.t1 = c->tri[dir][o.asym ? K_D1A : K_D1S];
         else d.t1 = c->trif[dir][o.asym ? K_D1A : K_D1S];
+        const int op = o.F.op, ni = op == PR_A ? 1 : op == PR_MUL ? 2 : op == PR_SPECT ? 4 : 3;
+        const T *in[4] = {o.F.a, o.F.b, o.F.c, o.F.d};
+        for (int k = 0; k < ni; k++) add_once(rd, nr, in[k]);
+        // an accumulated output is read, unless the first operation wrote it
+        if (o.iadd && !(i == 1 && o.dF == ops[0].dF)) add_once(rd, nr, o.dF);
+        add_once(wr, nw, o.dF);
     }
-    // algorithmic bytes per cell: the second operation's operands (they
-    // contain the first's), each accumulated output read, each output written
-    const double nin = o1 == PR_MUL ? 2.0 : o1 == PR_MULMUL ? 3.0 : 4.0;
-    const double nacc = (double)(ops[0].iadd + ops[1].iadd);
-    const double nout = ops[0].dF == ops[1].dF ? 1.0 : 2.0;
-    const double bytes = (double)sizeof(T) * (nin + nacc + nout);
+    const double bytes = (double)sizeof(T) * (double)(nr + nw);
     if constexpr (sizeof(T) == 8) return launch_pair_t<double>(c, g, bytes);
     else return launch_pair_f32(c, g, bytes);
 }

@@ -182,8 +182,11 @@ __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_gauss(LineArgs
 // counterpart, and Y and then rho u_i Y.  The second operand set contains
 // the first, so one CTA runs both on its own lines: the second
 // operation finds the shared rows in L2, as the first derivative of
-// D2F*2 with iadd does.  Each operation is exactly the k_dfd of its
-// arguments, so the results are bitwise those of two launches.
+// D2F*2 with iadd does.  The convective fluxes of RHS pair up the same way
+// where two adjacent ones share the velocity factor, or where the second
+// adds the pressure gradient to what the first wrote.  Each operation is
+// exactly the k_dfd of its arguments, so the results are bitwise those of
+// two launches.
 template <class T>
 struct D1OpT {
     ProdT<T> F;
@@ -321,8 +324,7 @@ static int launch_line_t(st_ctx *c, OpKind op, const LineArgsT<T> &a) {
 }
 
 
-// one launch of a pair (bounded lines): producers (a, a*b), (a*b, c*(a*b))
-// or the species flux and its energy counterpart;
+// one launch of a pair (bounded lines), producers as in kPairOps;
 // bytes: algorithmic bytes per cell (every distinct field read or written once)
 template <int S, bool YT, class T, int OP0, int OP1>
 static void launch_pair_SY(st_ctx *c, const D1PairT<T> &g0, double bytes, cudaStream_t st) {
@@ -339,11 +341,25 @@ static void launch_pair_SY(st_ctx *c, const D1PairT<T> &g0, double bytes, cudaSt
     prof_stop(c, pi);
 }
 
+// the producer pairs compiled (first, second); pair_kind gives the index
+constexpr int kPairOps[][2] = {{PR_A, PR_MUL},   {PR_MUL, PR_MULMUL}, {PR_SPEC, PR_SPECT},
+                               {PR_MUL, PR_ADDMUL}, {PR_MUL, PR_A},    {PR_MUL, PR_MUL}};
+inline int pair_kind(int op0, int op1) {
+    for (int k = 0; k < (int)(sizeof(kPairOps) / sizeof(kPairOps[0])); k++)
+        if (kPairOps[k][0] == op0 && kPairOps[k][1] == op1) return k;
+    return -1;
+}
+
 template <int S, bool YT, class T>
 static void launch_pair_SYT(st_ctx *c, const D1PairT<T> &g, double bytes) {
-    if (g.op[0].F.op == PR_A) launch_pair_SY<S, YT, T, PR_A, PR_MUL>(c, g, bytes, c->stream);
-    else if (g.op[0].F.op == PR_MUL) launch_pair_SY<S, YT, T, PR_MUL, PR_MULMUL>(c, g, bytes, c->stream);
-    else launch_pair_SY<S, YT, T, PR_SPEC, PR_SPECT>(c, g, bytes, c->stream);
+    switch (pair_kind(g.op[0].F.op, g.op[1].F.op)) {
+        case 0: launch_pair_SY<S, YT, T, PR_A, PR_MUL>(c, g, bytes, c->stream); break;
+        case 1: launch_pair_SY<S, YT, T, PR_MUL, PR_MULMUL>(c, g, bytes, c->stream); break;
+        case 2: launch_pair_SY<S, YT, T, PR_SPEC, PR_SPECT>(c, g, bytes, c->stream); break;
+        case 3: launch_pair_SY<S, YT, T, PR_MUL, PR_ADDMUL>(c, g, bytes, c->stream); break;
+        case 4: launch_pair_SY<S, YT, T, PR_MUL, PR_A>(c, g, bytes, c->stream); break;
+        default: launch_pair_SY<S, YT, T, PR_MUL, PR_MUL>(c, g, bytes, c->stream); break;
+    }
 }
 
 template <class T>

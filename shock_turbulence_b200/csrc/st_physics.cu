@@ -91,14 +91,20 @@ static int d2fd2_sum(st_ctx *c, int dir, int asym, const float *F, float *d2F, c
                      const float *E2) {
     return dev_d2fd2_sum_f(c, dir, asym, F, d2F, E1, E2);
 }
-// two first derivatives of one direction in order (D1SpecT: producer, output,
-// asym, iadd, cadd), one launch when the second reads what the first reads
+// two first derivatives of one direction in order (producer, output, asym,
+// iadd[, cadd] of each; cadd 1 where not given), one launch where they share
+// fields
+template <class R>
+static int dfd_pair(st_ctx *c, int dir, ProdT<R> F0, R *O0, int asym0, int iadd0, double cadd0, ProdT<R> F1, R *O1,
+                    int asym1, int iadd1, double cadd1) {
+    const D1SpecT<R> ops[2] = {{F0, O0, asym0, iadd0, cadd0}, {F1, O1, asym1, iadd1, cadd1}};
+    if constexpr (sizeof(R) == 8) return dev_dfd_pair(c, dir, ops);
+    else return dev_dfd_pair_f(c, dir, ops);
+}
 template <class R>
 static int dfd_pair(st_ctx *c, int dir, ProdT<R> F0, R *O0, int asym0, int iadd0, ProdT<R> F1, R *O1, int asym1,
                     int iadd1) {
-    const D1SpecT<R> ops[2] = {{F0, O0, asym0, iadd0, 1.0}, {F1, O1, asym1, iadd1, 1.0}};
-    if constexpr (sizeof(R) == 8) return dev_dfd_pair(c, dir, ops);
-    else return dev_dfd_pair_f(c, dir, ops);
+    return dfd_pair<R>(c, dir, F0, O0, asym0, iadd0, 1.0, F1, O1, asym1, iadd1, 1.0);
 }
 static int gauss(st_ctx *c, int dir, const double *F, double *Fg) { return dev_gauss(c, dir, F, Fg); }
 static int gauss(st_ctx *c, int dir, const float *F, float *Fg) { return dev_gauss_f(c, dir, F, Fg); }
@@ -242,12 +248,14 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
         mu[p] = m;
         dmu[p] = dm;
     });
-    ST_TRY(dfd(c, 0, 1, pr_mul(q4r, u), Qcx + 3 * n3, 0, -1.0));
-    ST_TRY(dfd(c, 0, 1, pr_addmul(q5r, P, u), Qcx + 4 * n3, 0, -1.0));
-    ST_TRY(dfd(c, 0, 0, pr_mul(q1r, u), Qcx, 0, -5.0e-1));
-    ST_TRY(dfd(c, 0, 0, P, Qcx, 1, -1.0));
-    ST_TRY(dfd(c, 0, 1, pr_mul(q2r, u), Qcx + n3, 0, -5.0e-1));
-    ST_TRY(dfd(c, 0, 1, pr_mul(q3r, u), Qcx + 2 * n3, 0, -5.0e-1));
+    // adjacent fluxes sharing u (or the second adding dP/dx to what the first
+    // wrote) run as pairs, in the reference's order
+    const R *cu = u, *cv = v, *cw = w, *cP = P;
+    ST_TRY(dfd_pair<R>(c, 0, pr_mul(q4r, cu), Qcx + 3 * n3, 1, 0, -1.0, pr_addmul(q5r, cP, cu), Qcx + 4 * n3, 1, 0,
+                       -1.0));
+    ST_TRY(dfd_pair<R>(c, 0, pr_mul(q1r, cu), Qcx, 0, 0, -5.0e-1, pr_one(cP), Qcx, 0, 1, -1.0));
+    ST_TRY(dfd_pair<R>(c, 0, pr_mul(q2r, cu), Qcx + n3, 1, 0, -5.0e-1, pr_mul(q3r, cu), Qcx + 2 * n3, 1, 0,
+                       -5.0e-1));
     ST_TRY(dfd(c, 0, 1, q1r, FF, 0, 1.0));
     R *dTx = dd[0], *duxx = dd[1], *dvxx = dd[2], *dwxx = dd[3];
     if (visc) {
@@ -294,15 +302,12 @@ static int rhs_t(st_ctx *c, double *Q, const R *Qr, R *Qrhs, const double *Y) {
     // d(rho v)/dy and d(rho w)/dz with iadd=0, cadd=-1: Qconv(4) = 0 - d(.) exactly
     ST_TRY(dfd(c, 1, 1, q2r, Qcy + 3 * n3, 0, -1.0));
     ST_TRY(dfd(c, 1, 1, pr_mul(q1r, v), Qcy, 0, -5.0e-1));
-    ST_TRY(dfd(c, 1, 0, pr_mul(q2r, v), Qcy + n3, 0, -5.0e-1));
-    ST_TRY(dfd(c, 1, 0, P, Qcy + n3, 1, -1.0));
-    ST_TRY(dfd(c, 1, 1, pr_mul(q3r, v), Qcy + 2 * n3, 0, -5.0e-1));
-    ST_TRY(dfd(c, 1, 1, pr_addmul(q5r, P, v), Qcy + 4 * n3, 0, -1.0));
+    ST_TRY(dfd_pair<R>(c, 1, pr_mul(q2r, cv), Qcy + n3, 0, 0, -5.0e-1, pr_one(cP), Qcy + n3, 0, 1, -1.0));
+    ST_TRY(dfd_pair<R>(c, 1, pr_mul(q3r, cv), Qcy + 2 * n3, 1, 0, -5.0e-1, pr_addmul(q5r, cP, cv), Qcy + 4 * n3, 1,
+                       0, -1.0));
     ST_TRY(dfd(c, 2, 1, q3r, Qcz + 3 * n3, 0, -1.0));
-    ST_TRY(dfd(c, 2, 1, pr_mul(q1r, w), Qcz, 0, -5.0e-1));
-    ST_TRY(dfd(c, 2, 1, pr_mul(q2r, w), Qcz + n3, 0, -5.0e-1));
-    ST_TRY(dfd(c, 2, 0, pr_mul(q3r, w), Qcz + 2 * n3, 0, -5.0e-1));
-    ST_TRY(dfd(c, 2, 0, P, Qcz + 2 * n3, 1, -1.0));
+    ST_TRY(dfd_pair<R>(c, 2, pr_mul(q1r, cw), Qcz, 1, 0, -5.0e-1, pr_mul(q2r, cw), Qcz + n3, 1, 0, -5.0e-1));
+    ST_TRY(dfd_pair<R>(c, 2, pr_mul(q3r, cw), Qcz + 2 * n3, 0, 0, -5.0e-1, pr_one(cP), Qcz + 2 * n3, 0, 1, -1.0));
     ST_TRY(dfd(c, 2, 1, pr_addmul(q5r, P, w), Qcz + 4 * n3, 0, -1.0));
     R *d2Ty = dd[0], *d2Tz = dd[1], *d2uy = dd[2], *d2vy = dd[3], *d2wy = dd[4], *d2wz = dd[5];
     R *dGzz_y = dd[6], *d2uz = dd[7], *d2vz = dd[8], *dGxx_y = dd[9], *dGxx_z = dd[10], *dGyx_y = dd[11];
