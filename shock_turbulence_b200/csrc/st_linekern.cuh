@@ -182,7 +182,9 @@ __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm) k_gauss(LineArgs
 // counterpart, and Y and then rho u_i Y.  The second operand set contains
 // the first, so one CTA runs both on its own lines: the second
 // operation finds the shared rows in L2, as the first derivative of
-// D2F*2 with iadd does.  The convective fluxes of RHS pair up the same way
+// D2F*2 with iadd does.  (An accumulated output, the pressure-gradient case
+// below, is re-read by the thread that wrote it, with plain loads, so it is
+// coherent without a barrier.)  The convective fluxes of RHS pair up the same way
 // where two adjacent ones share the velocity factor, or where the second
 // adds the pressure gradient to what the first wrote.  Each operation is
 // exactly the k_dfd of its arguments, so the results are bitwise those of
