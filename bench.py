@@ -759,8 +759,9 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": (traffic_ratio(dom) * d["bytes"] / d["launches"]) if traffic_ratio(dom) else None,
-                "traffic_basis": "ncu dram read+write / algorithmic bytes of a 256^3 plain k_dfd capture "
-                                 "(profiles/ncu_traffic.txt) times the algorithmic bytes per launch",
+                "traffic_basis": (f"ncu dram read+write / algorithmic bytes of a 256^3 capture of {dom} "
+                                  "(profiles/ncu_traffic.txt) times the algorithmic bytes per launch")
+                                 if traffic_ratio(dom) else f"no ncu DRAM capture of {dom}",
                 "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
                 "avg_launch_ms": d["ms"] / d["launches"],
                 "share_of_kernel_time": d["ms"] / step_ms_all if step_ms_all else None,
